@@ -1,0 +1,188 @@
+/*
+ * sp2b - B200-native SP2 density-matrix purification (C ABI).
+ *
+ * Raw-pointer core API.  Every entry point returns an int status (SP2B_OK = 0)
+ * instead of terminating the process the way the reference's Fortran `stop` does
+ * (src/prg_sp2_mod.F90:118,362).  Matrices are dense FP64, n x n, column-major
+ * (the Fortran / BML dense convention), and symmetric (a Hamiltonian): the library
+ * relies on H = H^T and returns an exactly symmetric density matrix.  rho is the
+ * spin-summed density, 2x the idempotent projector (src/prg_sp2_mod.F90:375).
+ *
+ * Pointers are host pointers unless sp2b_opts.device_ptrs = 1, in which case they
+ * are device pointers on the current CUDA device and the call is asynchronous on
+ * sp2b_opts.stream up to its final status read.
+ *
+ * The PROGRESS-named exports (prg_sp2_alg2, ...) with the reference's exact C
+ * signatures are declared in prg_sp2b.h.
+ */
+#ifndef SP2B_H
+#define SP2B_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define SP2B_OK 0
+#define SP2B_NOT_CONVERGED 1 /* reference: "SP2 purification is not converging: STOP!" */
+#define SP2B_BAD_ARG 2
+#define SP2B_CUDA_ERROR 3
+#define SP2B_TIMEOUT 4       /* a bounded device-side wait ran out */
+#define SP2B_BAD_INPUT 5     /* NaN / Inf in the input or during the iteration */
+#define SP2B_NO_DEVICE 6
+
+/* Arithmetic of the SP2 squarings. */
+#define SP2B_PREC_FP64 0        /* FP64 products and sums: parity form (1e-10) */
+#define SP2B_PREC_MIXED_FP16 1  /* FP16 hi+lo split products on tcgen05, FP32 accumulate,
+                                   FP64 traces, final FP64 McWeeny step */
+#define SP2B_PREC_MIXED_BF16 2  /* same with BF16 hi+lo operands */
+
+typedef struct sp2b_opts {
+  int precision;     /* SP2B_PREC_* (default FP64) */
+  int mcweeny;       /* mixed only: FP64 McWeeny steps after the loop (default 1) */
+  double mixed_tol;  /* mixed only: stop once Tr(X - X^2) < mixed_tol (default 1e-3) */
+  int device_ptrs;   /* 1: matrix arguments are device pointers */
+  void* stream;      /* cudaStream_t to run on (NULL: the per-library stream) */
+  int verbose;
+} sp2b_opts;
+
+/* Fill opts with defaults (FP64, host pointers). */
+int sp2b_opts_default(sp2b_opts* opts);
+
+/* Options used by the PROGRESS-named exports (prg_sp2b.h).  Initialised from the
+ * environment variable SP2B_PRECISION ("fp64", "mixed", "mixed_bf16") on first use. */
+int sp2b_set_default_opts(const sp2b_opts* opts);
+int sp2b_get_default_opts(sp2b_opts* opts);
+
+/* Message describing the last non-OK status of this thread. */
+const char* sp2b_last_error(void);
+
+/* ---- dense SP2 (replaces src/prg_sp2_mod.F90) --------------------------------------- */
+
+/* prg_sp2_alg2, src/prg_sp2_mod.F90:263-380.  iters_out (may be NULL) = SP2 steps taken.
+ * `threshold` is accepted for signature parity; dense products are not thresholded. */
+int sp2b_sp2_alg2(const double* h, double* rho, int n, double threshold, double bndfil,
+                  int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                  int verbose, const sp2b_opts* opts, int* iters_out);
+
+/* prg_sp2_alg2_genseq, src/prg_sp2_mod.F90:395-533.  pp, vv: length >= maxsp2iter. */
+int sp2b_sp2_alg2_genseq(const double* h, double* rho, int n, double threshold, double bndfil,
+                         int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                         int* pp, int* icount, double* vv, int verbose, const sp2b_opts* opts);
+
+/* prg_sp2_alg2_seq, src/prg_sp2_mod.F90:543-627: replay pp(1:icount). */
+int sp2b_sp2_alg2_seq(const double* h, double* rho, int n, double threshold, const int* pp,
+                      int icount, double* vv, int verbose, const sp2b_opts* opts);
+
+/* prg_prg_sp2_alg2_seq_inplace, src/prg_sp2_mod.F90:638-722: rho holds H on entry. */
+int sp2b_sp2_alg2_seq_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                              double* vv, double mineval, double maxeval, int verbose,
+                              const sp2b_opts* opts);
+
+/* prg_sp2_alg1, src/prg_sp2_mod.F90:734-864. */
+int sp2b_sp2_alg1(const double* h, double* rho, int n, double threshold, double bndfil,
+                  int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                  int verbose, const sp2b_opts* opts, int* iters_out);
+
+/* prg_sp2_alg1_genseq, src/prg_sp2_mod.F90:879-1000. */
+int sp2b_sp2_alg1_genseq(const double* h, double* rho, int n, double threshold, double bndfil,
+                         int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                         int* pp, int* icount, double* vv, const sp2b_opts* opts);
+
+/* prg_sp2_alg1_seq, src/prg_sp2_mod.F90:1010-1089. */
+int sp2b_sp2_alg1_seq(const double* h, double* rho, int n, double threshold, const int* pp,
+                      int icount, double* vv, const sp2b_opts* opts);
+
+/* prg_prg_sp2_alg1_seq_inplace, src/prg_sp2_mod.F90:1100-1177. */
+int sp2b_sp2_alg1_seq_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                              double* vv, double mineval, double maxeval, const sp2b_opts* opts);
+
+/* prg_sp2_basic, src/prg_sp2_mod.F90:49-135. */
+int sp2b_sp2_basic(const double* h, double* rho, int n, double threshold, double bndfil,
+                   int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                   int verbose, const sp2b_opts* opts, int* iters_out);
+
+/* prg_sp2_submatrix_inplace, src/prg_sp2_mod.F90:1259-1310: vv(1:icount) is
+ * ACCUMULATED with the sum of squares of (X - X^2) over the first core_size rows. */
+int sp2b_sp2_submatrix_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                               double* vv, double mineval, double maxeval, int core_size,
+                               const sp2b_opts* opts);
+
+/* prg_sp2_submatrix, src/prg_sp2_mod.F90:1190-1246 (separate input H). */
+int sp2b_sp2_submatrix(const double* ham, double* rho, int n, double threshold, const int* pp,
+                       int icount, double* vv, double mineval, double maxeval, int core_size,
+                       const sp2b_opts* opts);
+
+/* ---- normalisation and checks ----------------------------------------------------- */
+
+/* bml_gershgorin as used by prg_normalize (src/prg_normalize_mod.F90:41). */
+int sp2b_gershgorin(const double* h, int n, double* mineval, double* maxeval,
+                    const sp2b_opts* opts);
+
+/* prg_normalize, src/prg_normalize_mod.F90:32-46: h <- (e_max I - h)/(e_max - e_min). */
+int sp2b_normalize(double* h, int n, double* mineval, double* maxeval, const sp2b_opts* opts);
+
+/* prg_check_idempotency, src/prg_densitymatrix_mod.F90:862-880: ||A^2 - A||_F. */
+int sp2b_check_idempotency(const double* a, int n, double threshold, double* idempotency,
+                           const sp2b_opts* opts);
+
+/* ---- host-side graph / sequence logic (no GPU) ------------------------------------ */
+
+/* prg_sp2sequence, src/prg_homolumo_mod.F90:97-147.  pp has room for ppmax (>= 100). */
+int sp2b_sp2sequence(int* pp, int* imax, double mineval, double maxeval, double ehomo,
+                     double elumo, double errlimit, int ppmax);
+
+/* prg_homolumogap, src/prg_homolumo_mod.F90:22-89 (imax is the 1-based count). */
+int sp2b_homolumogap(const double* vv, int imax, const int* pp, double mineval, double maxeval,
+                     double* ehomo, double* elumo, double* egap);
+
+/* prg_equalPartition, src/prg_graph_mod.F90:359-399.  part_ptr has nparts+1 entries,
+ * nodes has nnodes entries (0-based node ids, part i = nodes[part_ptr[i]:part_ptr[i+1]]).
+ * Call with part_ptr = NULL to query nparts. */
+int sp2b_equal_partition(int nodes_per_part, int nnodes, int* nparts, int* part_ptr,
+                         int* nodes);
+
+/* Core+halo index of each part (bml_matrix2submatrix_index as called at
+ * src/prg_subgraphloop_mod.F90:60-63).  Graph and H are CSR (row_ptr n+1 int64,
+ * col int32); h_* may be NULL.  Output: halo_ptr (nparts+1) and halo_idx (capacity
+ * halo_cap; core nodes first), core sizes in llsize, total sizes in lsize.  Returns
+ * SP2B_BAD_ARG with the needed capacity in *halo_needed when halo_cap is too small. */
+int sp2b_subgraph_halos(int n, const long long* g_row_ptr, const int* g_col,
+                        const long long* h_row_ptr, const int* h_col, int nparts,
+                        const int* part_ptr, const int* part_nodes, int double_jump,
+                        long long* halo_ptr, int* halo_idx, long long halo_cap,
+                        long long* halo_needed, int* lsize, int* llsize);
+
+/* ---- graph-partitioned SP2 (replaces prg_subgraphSP2Loop) ------------------------- */
+
+/* prg_subgraphSP2Loop, src/prg_subgraphloop_mod.F90:36-126, flattened (the reference
+ * has no C binding: graph_partitioning_t is not interoperable).
+ *
+ * H is CSR (row_ptr int64 [n+1], col int32, val FP64).  Parts are given by their
+ * core+halo index lists (halo_ptr/halo_idx, core first, llsize[p] core nodes).  All
+ * parts run the same branch sequence pp(1:maxiter) with the global bounds
+ * mineval/maxeval.  Outputs:
+ *   rho_core  packed core rows: part p's llsize[p] x lsize[p] block (row-major, row r
+ *             = node halo_idx[halo_ptr[p]+r], column c = node halo_idx[halo_ptr[p]+c])
+ *             at offset rho_off[p] = sum_{q<p} llsize[q]*lsize[q];
+ *   rho_dense optional dense n x n output (may be NULL), core rows filled, rest zero;
+ *   vv        maxiter sums over all parts' core rows of (X - X^2)^2, already passed
+ *             through sqrt as prg_fnormGraph does (src/prg_graph_mod.F90:933-971).
+ * Host or device pointers per opts.device_ptrs. */
+int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
+                           const double* h_val, int nparts, const long long* halo_ptr,
+                           const int* halo_idx, const int* llsize, const int* pp, int maxiter,
+                           double mineval, double maxeval, double* rho_core,
+                           double* rho_dense, double* vv, const sp2b_opts* opts);
+
+/* ---- device-resident building blocks (used by the torch binding) ------------------ */
+
+/* Split-precision symmetric-operand product on device arrays:
+ * C = A * B with A, B symmetric n x n FP32 (row- or column-major, same thing),
+ * computed as hi/lo FP16 tcgen05 products with FP32 accumulation. */
+int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* c, int n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SP2B_H */

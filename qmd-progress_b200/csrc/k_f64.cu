@@ -1,0 +1,354 @@
+// FP64 kernels: Gershgorin bounds, normalisation, and the symmetric-tile DMMA product
+// with the fused SP2 epilogue.  This is the parity form of the SP2 step (1e-10).
+#include "reduce.cuh"
+
+namespace sp2b {
+
+// ------------------------------------------------------------------------------------
+// Gershgorin bounds (bml_gershgorin as used by prg_normalize, src/prg_normalize_mod.F90:41)
+// H is column-major: H(i, j) = h[i + j*ld]; thread i walks row i, so a warp reads 32
+// consecutive doubles of one column per step (coalesced).
+// ------------------------------------------------------------------------------------
+__global__ void k_gersh_partial(const double* __restrict__ h, int n, int ld, int ncol,
+                                double* __restrict__ rowsum) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int j0 = blockIdx.y * ncol;
+  const int j1 = min(n, j0 + ncol);
+  double s = 0.0;
+  for (int j = j0; j < j1; ++j)
+    if (j != i) s += fabs(h[i + (size_t)j * ld]);
+  rowsum[(size_t)blockIdx.y * n + i] = s;
+}
+
+__global__ void k_gersh_final(const double* __restrict__ h, int n, int ld, int nsplit,
+                              const double* __restrict__ rowsum, double* __restrict__ bounds) {
+  // single block: deterministic min/max over rows
+  __shared__ double smin[1024], smax[1024];
+  double mn = 1e308, mx = -1e308;
+  bool bad = false;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int s = 0; s < nsplit; ++s) r += rowsum[(size_t)s * n + i];
+    const double d = h[i + (size_t)i * ld];
+    if (!(r == r) || !(d == d) || fabs(r) > 1e300 || fabs(d) > 1e300) bad = true;
+    mn = fmin(mn, d - r);
+    mx = fmax(mx, d + r);
+  }
+  if (bad) mn = mx = nan("");
+  smin[threadIdx.x] = mn;
+  smax[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      const double a = smin[threadIdx.x + o], b = smax[threadIdx.x + o];
+      smin[threadIdx.x] = (a != a || smin[threadIdx.x] != smin[threadIdx.x]) ? nan("") : fmin(smin[threadIdx.x], a);
+      smax[threadIdx.x] = (b != b || smax[threadIdx.x] != smax[threadIdx.x]) ? nan("") : fmax(smax[threadIdx.x], b);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    bounds[0] = smin[0];
+    bounds[1] = smax[0];
+  }
+}
+
+int gersh_nsplit(int n) {
+  const int rows_blocks = (n + 255) / 256;
+  int ns = (4 * 148 + rows_blocks - 1) / rows_blocks;
+  if (ns > n) ns = n;
+  if (ns < 1) ns = 1;
+  return ns;
+}
+
+cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsplit,
+                         double* bounds, cudaStream_t st) {
+  const int ncol = (n + nsplit - 1) / nsplit;
+  dim3 grid((n + 255) / 256, nsplit);
+  k_gersh_partial<<<grid, 256, 0, st>>>(h, n, ld, ncol, rowsum);
+  k_gersh_final<<<1, 1024, 0, st>>>(h, n, ld, nsplit, rowsum, bounds);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// Normalisation X0 = alpha H + beta I, alpha = -1/(emax-emin), beta = emax/(emax-emin)
+// (src/prg_normalize_mod.F90:27, in the alpha/beta form of src/prg_response_mod.F90:700)
+// into the zero-padded np x np buffer, with Tr X0 and ||X0||_F^2 for the first SP2 step.
+// ------------------------------------------------------------------------------------
+__global__ void k_normalize_f64(const double* __restrict__ h, int n, int ld, int np,
+                                const double* __restrict__ bounds, double* __restrict__ x,
+                                double* partials, unsigned* counter, SP2Rec* rec0,
+                                double* norm_out) {
+  __shared__ double red[32 * 4];
+  __shared__ int s_last;
+  const double emin = bounds[0], emax = bounds[1];
+  const double mm = emax - emin;
+  const double alpha = -1.0 / mm, beta = emax / mm;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  const size_t total = (size_t)np * np;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / np), c = (int)(idx % np);
+    double v = 0.0;
+    if (r < n && c < n) {
+      v = alpha * h[(size_t)r * ld + c];
+      if (r == c) v += beta;
+    }
+    x[idx] = v;
+    s[0] += v * v;
+    if (r == c) s[1] += v;
+  }
+  block_sum<4>(s, red);
+  if (threadIdx.x == 0) {
+    partials[4 * blockIdx.x] = s[0];
+    partials[4 * blockIdx.x + 1] = s[1];
+    __threadfence();
+    s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double t[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) {
+    t[0] += __ldcg(partials + 4 * j);
+    t[1] += __ldcg(partials + 4 * j + 1);
+  }
+  block_sum<4>(t, red);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    SP2Rec r0;
+    memset(&r0, 0, sizeof(r0));
+    r0.trx = t[1];
+    r0.trx_data = t[1];
+    r0.fro2 = t[0];
+    r0.last_branch = -1;
+    if (!(t[0] == t[0]) || !(mm > 0.0)) {
+      r0.status = SP2B_BAD_INPUT;
+      r0.done = 1;
+    }
+    *rec0 = r0;
+    norm_out[0] = emin;
+    norm_out[1] = emax;
+    norm_out[2] = t[1];
+    norm_out[3] = t[0];
+  }
+}
+
+static int norm_grid(int np) {
+  const size_t total = (size_t)np * np;
+  size_t g = (total + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  return (int)g;
+}
+
+cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const double* bounds,
+                                 double* x, double* partials, unsigned* counter, SP2Rec* rec0,
+                                 double* norm_out, cudaStream_t st) {
+  k_normalize_f64<<<norm_grid(np), 256, 0, st>>>(h, n, ld, np, bounds, x, partials, counter,
+                                                 rec0, norm_out);
+  return cudaGetLastError();
+}
+
+__global__ void k_copy_in(const double* __restrict__ src, int n, int ld, int np,
+                          double* __restrict__ x) {
+  const size_t total = (size_t)np * np;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / np), c = (int)(idx % np);
+    x[idx] = (r < n && c < n) ? src[(size_t)r * ld + c] : 0.0;
+  }
+}
+
+cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,
+                           cudaStream_t st) {
+  k_copy_in<<<norm_grid(np), 256, 0, st>>>(src, n, ld, np, x);
+  return cudaGetLastError();
+}
+
+__global__ void k_finish_f64(const double* __restrict__ x, int np, int n, double scale,
+                             double* __restrict__ rho, int ld) {
+  const size_t total = (size_t)n * n;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / n), c = (int)(idx % n);
+    rho[(size_t)r * ld + c] = scale * x[(size_t)r * np + c];
+  }
+}
+
+cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, double* rho,
+                              int ld, cudaStream_t st) {
+  k_finish_f64<<<norm_grid(np), 256, 0, st>>>(x, np, n, scale, rho, ld);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// Symmetric-tile FP64 product with the SP2 epilogue.
+// One CTA per upper tile (bi <= bj) of BT x BT; WM x WN warps, each owning a
+// (BT/WM) x (BT/WN) block of m8n8k4 DMMA fragments.  Operand tiles are rows of the
+// symmetric inputs: As[k][m] = A[k0+k][i0+m], Bs[k][n] = B[k0+k][j0+n], staged by a
+// 3-deep cp.async pipeline with rows padded to BT+4 doubles (conflict-free fragment loads).
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+template <int BT, int WM, int WN>
+struct F64Cfg {
+  static constexpr int BK = 16;
+  static constexpr int NW = WM * WN;
+  static constexpr int NT = NW * 32;
+  static constexpr int LDS = BT + 4;
+  static constexpr int ST = 3;
+  static constexpr int TM = BT / WM, TN = BT / WN;
+  static constexpr int MI = TM / 8, NI = TN / 8;
+  static constexpr size_t SMEM = (size_t)ST * 2 * BK * LDS * sizeof(double);
+};
+
+template <int BT, int WM, int WN>
+__global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs p) {
+  using C = F64Cfg<BT, WM, WN>;
+  extern __shared__ __align__(16) double sm[];
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+
+  double alpha = p.alpha, beta = p.beta;
+  if (p.control) {
+    const int br = control_prologue(p);
+    if (br < 0) return;
+    if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
+    else { alpha = -1.0; beta = 2.0; }
+  }
+  int bi, bj;
+  upper_tile(blockIdx.x, bi, bj);
+  const int i0 = bi * BT, j0 = bj * BT;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wm = warp / WN, wn = warp % WN;
+  const double* __restrict__ A = (const double*)p.A;
+  const double* __restrict__ B = (const double*)p.B;
+  const int np = p.np;
+
+  double acc[C::MI][C::NI][2];
+#pragma unroll
+  for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < C::NI; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+
+  const int KB = np / C::BK;
+  auto load = [&](int stage, int kb) {
+    double* As = sm + stage * 2 * C::BK * C::LDS;
+    double* Bs = As + C::BK * C::LDS;
+    const int k0 = kb * C::BK;
+    for (int c = tid; c < C::BK * BT / 2; c += C::NT) {
+      const int row = c / (BT / 2), col = (c % (BT / 2)) * 2;
+      cp_async16(As + row * C::LDS + col, A + (size_t)(k0 + row) * np + i0 + col);
+      cp_async16(Bs + row * C::LDS + col, B + (size_t)(k0 + row) * np + j0 + col);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < C::ST - 1; ++s) {
+    if (s < KB) load(s, s);
+    cp_async_commit();
+  }
+  for (int kb = 0; kb < KB; ++kb) {
+    cp_async_wait<C::ST - 2>();
+    __syncthreads();
+    {
+      const int nk = kb + C::ST - 1;
+      if (nk < KB) load(nk % C::ST, nk);
+      cp_async_commit();
+    }
+    const double* As = sm + (kb % C::ST) * 2 * C::BK * C::LDS;
+    const double* Bs = As + C::BK * C::LDS;
+#pragma unroll
+    for (int kk = 0; kk < C::BK; kk += 4) {
+      double a[C::MI], b[C::NI];
+#pragma unroll
+      for (int mi = 0; mi < C::MI; ++mi) a[mi] = As[(kk + t4) * C::LDS + wm * C::TM + mi * 8 + g];
+#pragma unroll
+      for (int ni = 0; ni < C::NI; ++ni) b[ni] = Bs[(kk + t4) * C::LDS + wn * C::TN + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < C::NI; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // ---- epilogue: out = alpha*acc + beta*E, mirrored store, FP64 sums ----
+  const bool diag = (bi == bj);
+  const double* __restrict__ E = (const double*)p.E;
+  double* __restrict__ out = (double*)p.out;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};  // ||out||^2, Tr out, ||E-acc||^2 (core rows), Tr acc
+#pragma unroll
+  for (int mi = 0; mi < C::MI; ++mi) {
+#pragma unroll
+    for (int ni = 0; ni < C::NI; ++ni) {
+      const int r = i0 + wm * C::TM + mi * 8 + g;
+      const int c = j0 + wn * C::TN + ni * 8 + 2 * t4;
+      const double2 e = *reinterpret_cast<const double2*>(E + (size_t)r * np + c);
+      const double a0 = acc[mi][ni][0], a1 = acc[mi][ni][1];
+      const double v0 = alpha * a0 + beta * e.x;
+      const double v1 = alpha * a1 + beta * e.y;
+      const int w0 = sym_weight(diag, r, c), w1 = sym_weight(diag, r, c + 1);
+      const double d0 = e.x - a0, d1 = e.y - a1;
+      s[0] += w0 * v0 * v0 + w1 * v1 * v1;
+      s[2] += core_weight(w0, r, c, p.core) * d0 * d0 + core_weight(w1, r, c + 1, p.core) * d1 * d1;
+      if (r == c) { s[1] += v0; s[3] += a0; }
+      if (r == c + 1) { s[1] += v1; s[3] += a1; }
+      if (out) {
+        if (!diag) {
+          *reinterpret_cast<double2*>(out + (size_t)r * np + c) = make_double2(v0, v1);
+          out[(size_t)c * np + r] = v0;
+          out[(size_t)(c + 1) * np + r] = v1;
+        } else {
+          if (w0) { out[(size_t)r * np + c] = v0; out[(size_t)c * np + r] = v0; }
+          if (w1) { out[(size_t)r * np + c + 1] = v1; out[(size_t)(c + 1) * np + r] = v1; }
+        }
+      }
+    }
+  }
+  publish_and_finalize(p, s, red, &s_flag);
+}
+
+int f64_tile(int np) {
+  const int t128 = np / 128;
+  return (t128 * (t128 + 1) / 2 >= 2 * 148) ? 128 : 64;
+}
+
+int f64_ntiles(int np) {
+  const int t = np / f64_tile(np);
+  return t * (t + 1) / 2;
+}
+
+cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st) {
+  const int bt = f64_tile(a.np);
+  const int t = a.np / bt;
+  const int ntiles = t * (t + 1) / 2;
+  if (bt == 128) {
+    using C = F64Cfg<128, 2, 4>;
+    auto kern = k_sym_gemm_f64<128, 2, 4>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
+  } else {
+    using C = F64Cfg<64, 2, 2>;
+    auto kern = k_sym_gemm_f64<64, 2, 2>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace sp2b

@@ -1,0 +1,564 @@
+// Split-precision symmetric products on the 5th-generation tensor cores (sm_100a).
+//
+// X is held as two 16-bit arrays, X ~= hi + 2^-s lo (s = 11 for FP16, 8 for BF16), and
+//   X*X ~= hi*hi + 2^-s (hi*lo + lo*hi)
+// is accumulated in FP32 in TMEM: one accumulator for hi*hi, one for the two cross
+// terms, merged in FP64 in the epilogue.  Operands are staged by TMA (128-byte swizzle,
+// no multicast) through a 3-deep mbarrier pipeline; one thread issues tcgen05.mma; all
+// four warps read the accumulators back with tcgen05.ld and run the fused SP2 epilogue
+// (branch update, hi/lo re-split of X_{n+1}, mirrored store, FP64 trace and norm sums).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <mutex>
+
+#include "reduce.cuh"
+
+namespace sp2b {
+namespace tc {
+constexpr int BM = 128;  // UMMA M (TMEM lanes)
+constexpr int BN = 128;  // UMMA N
+constexpr int BK = 64;   // 64 x 16-bit = one 128-byte swizzle row
+constexpr int UK = 16;   // K of one kind::f16 MMA
+constexpr int ST = 3;    // pipeline depth
+constexpr int TILE_BYTES = BM * BK * 2;
+constexpr int STAGE_BYTES = 4 * TILE_BYTES;  // A_hi, A_lo, B_hi, B_lo
+constexpr int SMEM_BYTES = ST * STAGE_BYTES + 1024;
+constexpr int TMEM_COLS = 256;               // two 128-column FP32 accumulators
+}  // namespace tc
+
+template <typename T>
+struct SplitTraits;
+template <>
+struct SplitTraits<__half> {
+  static constexpr uint32_t kFmt = 0;  // UMMA F16
+  static constexpr double kScale = 2048.0, kInv = 1.0 / 2048.0;
+  __device__ static double to_d(__half h) { return (double)__half2float(h); }
+  __device__ static __half from_d(double v) { return __double2half(v); }
+};
+template <>
+struct SplitTraits<__nv_bfloat16> {
+  static constexpr uint32_t kFmt = 1;  // UMMA BF16
+  static constexpr double kScale = 256.0, kInv = 1.0 / 256.0;
+  __device__ static double to_d(__nv_bfloat16 h) { return (double)__bfloat162float(h); }
+  __device__ static __nv_bfloat16 from_d(double v) { return __double2bfloat16(v); }
+};
+
+// ---------------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t cnt) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(cnt) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up (returns false and raises the CTA abort flag) after
+// kSpinLimit polls, or early once another thread of the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try(a, parity)) return true;
+    if ((i & 255u) == 255u && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(mbar), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   mbar)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+        "=r"(v[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// K-major operand tile, 128-byte swizzle, 8-row groups 1024 bytes apart (SBO), LBO
+// unused for swizzled K-major (1), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+// kind::f16 instruction descriptor: FP32 accumulate, A/B K-major, M x N.
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, int M, int N) {
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// ---------------------------------------------------------------------------------
+// The kernel.  SYM: one CTA per upper 128x128 tile with the SP2 epilogue.
+//              !SYM: one CTA per tile of a plain product, FP32 output.
+// ---------------------------------------------------------------------------------
+template <typename T, bool SYM>
+__global__ void __launch_bounds__(128, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
+              const __grid_constant__ CUtensorMap tm_bhi, const __grid_constant__ CUtensorMap tm_blo,
+              const StepArgs p, float* plain_out, int plain_n) {
+  using TR = SplitTraits<T>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full[tc::ST];
+  __shared__ __align__(8) uint64_t bar_empty[tc::ST];
+  __shared__ __align__(8) uint64_t bar_done;
+  __shared__ uint32_t tmem_holder;
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+  __shared__ volatile int s_abort;
+
+  double alpha = p.alpha, beta = p.beta;
+  if (SYM && p.control) {
+    const int br = control_prologue(p);
+    if (br < 0) return;
+    if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
+    else { alpha = -1.0; beta = 2.0; }
+  }
+  int bi, bj;
+  if (SYM) upper_tile(blockIdx.x, bi, bj);
+  else { bi = blockIdx.y; bj = blockIdx.x; }
+  const int i0 = bi * tc::BM, j0 = bj * tc::BN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = smem_u32(smem);
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < tc::ST; ++s) {
+      mbar_init(smem_u32(&bar_full[s]), 1);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    mbar_init(smem_u32(&bar_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_holder), tc::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_holder;
+  const int KB = p.np / tc::BK;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer ----------------
+      int issued_phase[tc::ST];
+      for (int s = 0; s < tc::ST; ++s) issued_phase[s] = -1;
+      bool ok = true;
+      for (int kb = 0; kb < KB && ok; ++kb) {
+        const int s = kb % tc::ST, u = kb / tc::ST;
+        if (kb >= tc::ST) ok = mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort);
+        if (!ok) break;
+        const uint32_t fb = smem_u32(&bar_full[s]);
+        const uint32_t st = sbase + s * tc::STAGE_BYTES;
+        mbar_expect_tx(fb, tc::STAGE_BYTES);
+        tma_load_2d(st + 0 * tc::TILE_BYTES, &tm_ahi, fb, kb * tc::BK, i0);
+        tma_load_2d(st + 1 * tc::TILE_BYTES, &tm_alo, fb, kb * tc::BK, i0);
+        tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_bhi, fb, kb * tc::BK, j0);
+        tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_blo, fb, kb * tc::BK, j0);
+        issued_phase[s] = u & 1;
+      }
+      if (!ok) {
+        // Abort: wait (bounded) for this CTA's copies still in flight before leaving.
+        for (int s = 0; s < tc::ST; ++s)
+          if (issued_phase[s] >= 0) {
+            for (uint32_t i = 0; i < kSpinLimit; ++i)
+              if (mbar_try(smem_u32(&bar_full[s]), issued_phase[s])) break;
+          }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer ----------------
+      constexpr uint32_t idesc = make_idesc(TR::kFmt, tc::BM, tc::BN);
+      const uint32_t acc_hh = tmem, acc_x = tmem + tc::BN;
+      bool ok = true;
+      for (int kb = 0; kb < KB; ++kb) {
+        const int s = kb % tc::ST, u = kb / tc::ST;
+        ok = mbar_wait(smem_u32(&bar_full[s]), u & 1, &s_abort);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t st = sbase + s * tc::STAGE_BYTES;
+        const uint64_t d_ahi = sw128_desc(st + 0 * tc::TILE_BYTES);
+        const uint64_t d_alo = sw128_desc(st + 1 * tc::TILE_BYTES);
+        const uint64_t d_bhi = sw128_desc(st + 2 * tc::TILE_BYTES);
+        const uint64_t d_blo = sw128_desc(st + 3 * tc::TILE_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < tc::BK / tc::UK; ++kk) {
+          // advance 16 elements = 32 bytes along K inside the swizzle atom
+          const uint64_t off = (uint64_t)((kk * tc::UK * 2) >> 4);
+          const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+          umma_f16(acc_hh, d_ahi + off, d_bhi + off, idesc, acc);
+          umma_f16(acc_x, d_ahi + off, d_blo + off, idesc, acc);
+          umma_f16(acc_x, d_alo + off, d_bhi + off, idesc, 1u);
+        }
+        umma_commit(smem_u32(&bar_empty[s]));  // stage free once these MMAs retire
+      }
+      umma_commit(smem_u32(&bar_done));        // accumulators complete
+      if (!ok) s_abort = 1;
+    }
+    __syncwarp();
+  }
+
+  // ---------------- epilogue (all 4 warps; warp w owns TMEM lanes 32w..32w+31) ----------
+  const bool good = mbar_wait(smem_u32(&bar_done), 0, &s_abort) && !s_abort;
+  tc_fence_after();
+  double sums[4] = {0.0, 0.0, 0.0, 0.0};
+  if (good) {
+    const int rl = warp * 32 + lane;
+    const int r = i0 + rl;
+    const int np = p.np;
+    const bool diag = SYM && (bi == bj);
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const T* Ehi = (const T*)p.E;
+    const T* Elo = (const T*)p.E_lo;
+    T* Ohi = (T*)p.out;
+    T* Olo = (T*)p.out_lo;
+#pragma unroll 1
+    for (int cc = 0; cc < tc::BN / 32; ++cc) {
+      uint32_t hh[32], xx[32];
+      tmem_ld32(trow + cc * 32, hh);
+      tmem_ld32(trow + tc::BN + cc * 32, xx);
+      tmem_wait_ld();
+      const int c0 = j0 + cc * 32;
+      if (!SYM) {
+        if (r < plain_n) {
+          for (int j = 0; j < 32; ++j) {
+            const int c = c0 + j;
+            if (c < plain_n)
+              plain_out[(size_t)r * plain_n + c] =
+                  (float)((double)__uint_as_float(hh[j]) + TR::kInv * (double)__uint_as_float(xx[j]));
+          }
+        }
+        continue;
+      }
+      alignas(16) T ehi[32], elo[32], nhi[32], nlo[32];
+      {
+        const uint4* src_h = reinterpret_cast<const uint4*>(Ehi + (size_t)r * np + c0);
+        const uint4* src_l = reinterpret_cast<const uint4*>(Elo + (size_t)r * np + c0);
+        uint4* dh = reinterpret_cast<uint4*>(ehi);
+        uint4* dl = reinterpret_cast<uint4*>(elo);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { dh[q] = src_h[q]; dl[q] = src_l[q]; }
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int c = c0 + j;
+        const double P = (double)__uint_as_float(hh[j]) + TR::kInv * (double)__uint_as_float(xx[j]);
+        const double x = TR::to_d(ehi[j]) + TR::kInv * TR::to_d(elo[j]);
+        const double v = alpha * P + beta * x;
+        const T h = TR::from_d(v);
+        const T l = TR::from_d((v - TR::to_d(h)) * TR::kScale);
+        const double vs = TR::to_d(h) + TR::kInv * TR::to_d(l);
+        nhi[j] = h;
+        nlo[j] = l;
+        const int w = sym_weight(diag, r, c);
+        const double dres = x - P;
+        sums[0] += w * vs * vs;
+        sums[2] += core_weight(w, r, c, p.core) * dres * dres;
+        if (r == c) { sums[1] += vs; sums[3] += P; }
+        if (Ohi && w && r != c) {
+          Ohi[(size_t)c * np + r] = h;
+          Olo[(size_t)c * np + r] = l;
+        }
+      }
+      if (Ohi) {
+        if (!diag) {
+          uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * np + c0);
+          uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * np + c0);
+          const uint4* sh = reinterpret_cast<const uint4*>(nhi);
+          const uint4* sl = reinterpret_cast<const uint4*>(nlo);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) { dh[q] = sh[q]; dl[q] = sl[q]; }
+        } else {
+          for (int j = 0; j < 32; ++j)
+            if (r <= c0 + j) {
+              Ohi[(size_t)r * np + c0 + j] = nhi[j];
+              Olo[(size_t)r * np + c0 + j] = nlo[j];
+            }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, tc::TMEM_COLS);
+  if (!good && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+  if (SYM) {
+    if (p.out) __threadfence();
+    publish_and_finalize(p, sums, red, &s_flag);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Elementwise kernels of the split path
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_normalize_split(const double* __restrict__ h, int n, int ld, int np,
+                                  const double* __restrict__ bounds, T* __restrict__ hi,
+                                  T* __restrict__ lo, double* partials, unsigned* counter,
+                                  SP2Rec* rec0, double* norm_out) {
+  using TR = SplitTraits<T>;
+  __shared__ double red[32 * 4];
+  __shared__ int s_last;
+  const double emin = bounds[0], emax = bounds[1];
+  const double mm = emax - emin;
+  const double alpha = -1.0 / mm, beta = emax / mm;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  const size_t total = (size_t)np * np;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / np), c = (int)(idx % np);
+    double v = 0.0;
+    if (r < n && c < n) {
+      v = alpha * h[(size_t)r * ld + c];
+      if (r == c) v += beta;
+    }
+    const T a = TR::from_d(v);
+    const T b = TR::from_d((v - TR::to_d(a)) * TR::kScale);
+    hi[idx] = a;
+    lo[idx] = b;
+    const double vs = TR::to_d(a) + TR::kInv * TR::to_d(b);
+    s[0] += vs * vs;
+    if (r == c) s[1] += vs;
+  }
+  block_sum<4>(s, red);
+  if (threadIdx.x == 0) {
+    partials[4 * blockIdx.x] = s[0];
+    partials[4 * blockIdx.x + 1] = s[1];
+    __threadfence();
+    s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double t[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) {
+    t[0] += __ldcg(partials + 4 * j);
+    t[1] += __ldcg(partials + 4 * j + 1);
+  }
+  block_sum<4>(t, red);
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    SP2Rec r0;
+    memset(&r0, 0, sizeof(r0));
+    r0.trx = t[1];
+    r0.trx_data = t[1];
+    r0.fro2 = t[0];
+    r0.last_branch = -1;
+    if (!(t[0] == t[0]) || !(mm > 0.0)) {
+      r0.status = SP2B_BAD_INPUT;
+      r0.done = 1;
+    }
+    *rec0 = r0;
+    norm_out[0] = emin;
+    norm_out[1] = emax;
+    norm_out[2] = t[1];
+    norm_out[3] = t[0];
+  }
+}
+
+template <typename T>
+__global__ void k_split_to_f64(const T* __restrict__ hi, const T* __restrict__ lo, size_t total,
+                               double* __restrict__ x) {
+  using TR = SplitTraits<T>;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = TR::to_d(hi[i]) + TR::kInv * TR::to_d(lo[i]);
+}
+
+__global__ void k_f32_to_split(const float* __restrict__ a, int n, int np, __half* __restrict__ hi,
+                               __half* __restrict__ lo) {
+  using TR = SplitTraits<__half>;
+  const size_t total = (size_t)np * np;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / np), c = (int)(idx % np);
+    const double v = (r < n && c < n) ? (double)a[(size_t)r * n + c] : 0.0;
+    const __half h = TR::from_d(v);
+    hi[idx] = h;
+    lo[idx] = TR::from_d((v - TR::to_d(h)) * TR::kScale);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Host side: tensor maps and launches
+// ---------------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* ptr = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  });
+  return fn;
+}
+
+// rows x cols (cols contiguous, row pitch ld elements) 16-bit matrix; box 64 x 128.
+static bool make_tmap(CUtensorMap* tm, const void* base, long long rows, long long cols,
+                      long long ld, bool bf16) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(tm, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                  const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+int tc_ntiles(int np) {
+  const int t = np / tc::BM;
+  return t * (t + 1) / 2;
+}
+
+template <typename T, bool SYM>
+static cudaError_t launch_tc(const StepArgs& a, dim3 grid, float* plain_out, int plain_n,
+                             cudaStream_t st) {
+  const bool bf16 = std::is_same<T, __nv_bfloat16>::value;
+  CUtensorMap m[4];
+  if (!make_tmap(&m[0], a.A, a.np, a.np, a.np, bf16) ||
+      !make_tmap(&m[1], a.A_lo, a.np, a.np, a.np, bf16) ||
+      !make_tmap(&m[2], a.B, a.np, a.np, a.np, bf16) ||
+      !make_tmap(&m[3], a.B_lo, a.np, a.np, a.np, bf16))
+    return cudaErrorInvalidValue;
+  auto kern = k_tc_gemm<T, SYM>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 128, tc::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, plain_out, plain_n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sym_gemm_tc(const StepArgs& a, int bf16, cudaStream_t st) {
+  if (a.np % tc::BM != 0) return cudaErrorInvalidValue;
+  dim3 grid(tc_ntiles(a.np));
+  return bf16 ? launch_tc<__nv_bfloat16, true>(a, grid, nullptr, 0, st)
+              : launch_tc<__half, true>(a, grid, nullptr, 0, st);
+}
+
+cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,
+                            const __half* blo, int np, float* c, int n, cudaStream_t st,
+                            int* err) {
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.A = ahi;
+  a.A_lo = alo;
+  a.B = bhi;
+  a.B_lo = blo;
+  a.np = np;
+  a.err = err;
+  dim3 grid(np / tc::BN, np / tc::BM);
+  return launch_tc<__half, false>(a, grid, c, n, st);
+}
+
+static int ew_grid(size_t total) {
+  size_t g = (total + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  return (int)(g ? g : 1);
+}
+
+cudaError_t launch_normalize_split(const double* h, int n, int ld, int np,
+                                   const double* bounds, __half* hi, __half* lo, int bf16,
+                                   double* partials, unsigned* counter, SP2Rec* rec0,
+                                   double* norm_out, cudaStream_t st) {
+  const int g = ew_grid((size_t)np * np);
+  if (bf16)
+    k_normalize_split<__nv_bfloat16><<<g, 256, 0, st>>>(
+        h, n, ld, np, bounds, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, partials, counter, rec0,
+        norm_out);
+  else
+    k_normalize_split<__half><<<g, 256, 0, st>>>(h, n, ld, np, bounds, hi, lo, partials, counter,
+                                                 rec0, norm_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int bf16, double* x,
+                                cudaStream_t st) {
+  const size_t total = (size_t)np * np;
+  if (bf16)
+    k_split_to_f64<__nv_bfloat16><<<ew_grid(total), 256, 0, st>>>(
+        (const __nv_bfloat16*)hi, (const __nv_bfloat16*)lo, total, x);
+  else
+    k_split_to_f64<__half><<<ew_grid(total), 256, 0, st>>>(hi, lo, total, x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
+                                cudaStream_t st) {
+  k_f32_to_split<<<ew_grid((size_t)np * np), 256, 0, st>>>(a, n, np, hi, lo);
+  return cudaGetLastError();
+}
+
+}  // namespace sp2b

@@ -1,0 +1,79 @@
+// Launch interfaces shared by the sp2b translation units.
+#pragma once
+#include "sp2b_common.cuh"
+
+namespace sp2b {
+
+// Outcome of a dense solve, written by the device.
+struct SolveOut {
+  int done;     // loop finished
+  int nupd;     // number of X updates applied (final X lives in buffer nupd & 1)
+  int status;   // SP2B_* code
+  int iter;     // Fortran iteration count ("icount")
+};
+
+// Arguments of one symmetric-tile product launch (FP64 or split precision).
+//   acc(m, n) = sum_k A[k][m] * B[k][n]   (A, B stored np x np, symmetric)
+//   out       = alpha * acc + beta * E     (upper tiles computed, mirrored on store)
+// In control mode (ctl/rec set) alpha/beta come from the SP2 branch rule.
+struct StepArgs {
+  const void* A;
+  const void* B;
+  const void* A_lo;     // split mode: lo halves of the operands
+  const void* B_lo;
+  const void* E;        // elementwise operand (FP64; or hi/lo pair in split mode)
+  void* out;            // nullptr: sums only
+  const void* E_lo;     // split mode: lo half of E
+  void* out_lo;         // split mode: lo half of out
+  int np;               // padded dimension (= leading dimension)
+  int ntiles;
+  double alpha, beta;
+  int core;             // > 0: residual sums over the first `core` rows only
+  // SP2 control (control = 1)
+  int control;
+  SP2Ctl ctl;
+  SP2Rec* rec;
+  int k;
+  const int* pp_in;
+  int* pp_out;
+  double* vv_out;
+  int vv_accumulate;    // 1: vv_out[k] += res (submatrix); 0: vv_out[k] = sqrt(res)
+  SolveOut* sout;
+  // reductions
+  double* partials;     // [ntiles][4]
+  unsigned* counter;
+  double* sums_out;     // non-control: the 4 totals {||out||^2, Tr out, ||E-acc||^2, Tr acc}
+  int* err;             // device error word (timeouts)
+};
+
+// FP64 path ---------------------------------------------------------------------------
+int f64_tile(int np);  // tile edge chosen for this size (64 or 128)
+int f64_ntiles(int np);
+cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsplit,
+                         double* bounds, cudaStream_t st);
+int gersh_nsplit(int n);
+cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const double* bounds,
+                                 double* x, double* partials, unsigned* counter, SP2Rec* rec0,
+                                 double* norm_out, cudaStream_t st);
+cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st);
+cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, double* rho,
+                              int ld, cudaStream_t st);
+cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,
+                           cudaStream_t st);
+
+// Split-precision (tcgen05) path ------------------------------------------------------
+int tc_ntiles(int np);
+cudaError_t launch_normalize_split(const double* h, int n, int ld, int np,
+                                   const double* bounds, __half* hi, __half* lo, int bf16,
+                                   double* partials, unsigned* counter, SP2Rec* rec0,
+                                   double* norm_out, cudaStream_t st);
+cudaError_t launch_sym_gemm_tc(const StepArgs& a, int bf16, cudaStream_t st);
+cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int bf16,
+                                double* x, cudaStream_t st);
+cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
+                                cudaStream_t st);
+cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,
+                            const __half* blo, int np, float* c, int n, cudaStream_t st,
+                            int* err);
+
+}  // namespace sp2b

@@ -1,0 +1,220 @@
+// Shared definitions for the sp2b CUDA library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/sp2b.h"
+
+namespace sp2b {
+
+// Internal square buffers are padded to a multiple of this (zero padding is
+// invariant under X^2 and 2X - X^2, so the padded block never changes).
+constexpr int kPad = 128;
+
+inline int padded(int n) { return (n + kPad - 1) / kPad * kPad; }
+
+// Bounded spin limit for every device-side wait (mbarrier polls).  A wait that
+// runs out records SP2B_TIMEOUT in the per-call error word and gives up.
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+// -------------------------------------------------------------------------------------
+// Scalar SP2 control: the branch rule of each reference algorithm, evaluated on the
+// device from FP64 sums produced by the previous launch, so that no host round trip
+// sits between SP2 steps.
+// -------------------------------------------------------------------------------------
+enum Algo : int {
+  ALGO_ALG2 = 0,         // prg_sp2_alg2           src/prg_sp2_mod.F90:263-380
+  ALGO_ALG2_GENSEQ = 1,  // prg_sp2_alg2_genseq    :395-533
+  ALGO_ALG1 = 2,         // prg_sp2_alg1           :734-864
+  ALGO_ALG1_GENSEQ = 3,  // prg_sp2_alg1_genseq    :879-1000
+  ALGO_BASIC = 4,        // prg_sp2_basic          :49-135
+  ALGO_SEQ = 5,          // *_seq / *_seq_inplace / submatrix: replay pp
+  ALGO_MIXED = 6,        // mixed-precision alg2 with a precision-aware stop rule
+};
+
+enum Conv : int { CONV_NONE = 0, CONV_REL = 1, CONV_ABS = 2 };
+
+enum Branch : int { BR_2X_MINUS_X2 = 0, BR_X2 = 1, BR_STOP = 2 };
+
+struct SP2Ctl {
+  int algo;
+  int minit, maxit;
+  int conv;
+  int icount;          // replay length (ALGO_SEQ)
+  int n;               // logical dimension
+  double occ, idemtol;
+  double mixed_tol;    // ALGO_MIXED: stop once Tr(X - X^2) falls below this
+};
+
+// State entering SP2 launch k (slot k of a per-solve array).
+struct SP2Rec {
+  double trx;          // tracked trace (alg2 / alg1 bookkeeping)
+  double trx_data;     // Tr X_k summed from the stored data
+  double fro2;         // ||X_k||_F^2 from stored data (= Tr X_k^2 for symmetric X_k)
+  double idemperr, idemperr1, idemperr2;
+  double err_hist[2];  // ALGO_MIXED: Tr(X - X^2) two and one steps back
+  int iter;            // completed Fortran iterations ("iter")
+  int done;            // 1: the loop finished before launch k
+  int status;          // SP2B_OK or an error code
+  int last_branch;
+};
+
+struct SP2Decision {
+  int branch;          // Branch
+  SP2Rec next;         // scalar part of the next record (sums filled later)
+};
+
+__host__ __device__ inline double dabs(double x) { return x < 0 ? -x : x; }
+
+// Evaluate one SP2 step's control logic.  pp_in is only read in ALGO_SEQ.
+__host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec& r, int k,
+                                                  const int* pp_in) {
+  SP2Decision d;
+  d.next = r;
+  SP2Rec& nx = d.next;
+  const double occ = c.occ, tol = c.idemtol;
+  switch (c.algo) {
+    case ALGO_ALG2:
+    case ALGO_ALG2_GENSEQ:
+    case ALGO_MIXED: {
+      int it = r.iter + 1;
+      double trx = (c.algo == ALGO_ALG2) ? r.trx : r.trx_data;  // genseq: trx = trace(1) (:452)
+      const double trx2 = r.fro2;
+      const double tr2xx2 = 2.0 * trx - trx2;                   // :325
+      const double trxold = trx;
+      const double limdiff = dabs(trx2 - occ) - dabs(tr2xx2 - occ);
+      int stop = 0;
+      if (limdiff >= tol) {                                     // :329
+        d.branch = BR_2X_MINUS_X2;
+        trx = tr2xx2;
+      } else if (limdiff < -tol) {                              // :336
+        d.branch = BR_X2;
+        trx = trx2;
+      } else {                                                  // :343
+        d.branch = BR_STOP;
+        it -= 1;
+        trx = trxold;
+        stop = 1;
+      }
+      if (c.algo == ALGO_MIXED && d.branch != BR_STOP) {
+        // Precision-aware stop: the FP32-level trace noise keeps limdiff from ever
+        // reaching idemtol, so stop (before updating) once the idempotency error
+        // e = Tr(X - X^2) is below mixed_tol, or has not improved over two steps
+        // (the same two-step test as src/sp2_tensorcore/src/prg_sp2_tensorcore.cu:312).
+        const double e = r.trx_data - r.fro2;
+        if (e <= c.mixed_tol || (r.iter >= 2 && e >= r.err_hist[0])) {
+          d.branch = BR_STOP;
+          it -= 1;
+          trx = trxold;
+          stop = 1;
+        }
+        nx.err_hist[0] = r.err_hist[1];
+        nx.err_hist[1] = e;
+      }
+      nx.idemperr2 = r.idemperr1;                               // :351
+      nx.idemperr1 = r.idemperr;
+      nx.idemperr = dabs(trx - trxold);
+      if (c.conv == CONV_REL && it >= c.minit &&
+          (nx.idemperr >= nx.idemperr2 || nx.idemperr < tol))
+        stop = 1;                                               // :355
+      if (it == c.maxit) {                                      // :360 (reference: STOP)
+        stop = 1;
+        nx.status = SP2B_NOT_CONVERGED;
+      }
+      nx.iter = it;
+      nx.trx = trx;
+      nx.done = stop;
+      break;
+    }
+    case ALGO_ALG1:
+    case ALGO_ALG1_GENSEQ: {
+      const bool genseq = c.algo == ALGO_ALG1_GENSEQ;
+      int it = r.iter + 1;
+      double trx = r.trx;
+      const double trx2 = r.trx_data - r.fro2;                  // Tr(X - X^2) (:786)
+      const double limdiff = dabs(trx - trx2 - occ) - dabs(trx + trx2 - occ);  // :801
+      int stop = 0, exit_now = 0;
+      if (limdiff >= tol) {
+        d.branch = BR_2X_MINUS_X2;
+        trx = trx + trx2;
+      } else if (limdiff < -tol) {
+        d.branch = BR_X2;
+        trx = trx - trx2;
+      } else if (!genseq && limdiff == 0.0 && it == 1) {        // :818
+        d.branch = BR_X2;
+        trx = trx - trx2;
+      } else {
+        d.branch = BR_STOP;
+        it -= 1;
+        stop = 1;
+      }
+      nx.idemperr2 = r.idemperr1;
+      nx.idemperr1 = r.idemperr;
+      nx.idemperr = dabs(trx2);
+      if (c.conv == CONV_REL && it >= c.minit &&
+          (nx.idemperr2 <= nx.idemperr || nx.idemperr < tol))
+        stop = 1;                                               // :838 / :971
+      if (genseq && c.conv == CONV_ABS && dabs(limdiff) < tol) {  // :976 exit
+        stop = 1;
+        exit_now = 1;
+      }
+      if (!exit_now && it == c.maxit) {
+        stop = 1;
+        nx.status = SP2B_NOT_CONVERGED;
+      }
+      nx.iter = it;
+      nx.trx = trx;
+      nx.done = stop;
+      break;
+    }
+    case ALGO_BASIC: {
+      const int it = r.iter;                                    // do iter = 0, maxsp2iter
+      double trx = r.trx_data;                                  // :80
+      const double trx2 = r.fro2;
+      if (trx - occ <= 0.0) {                                   // :96
+        d.branch = BR_2X_MINUS_X2;
+        trx = 2.0 * trx - trx2;
+      } else {
+        d.branch = BR_X2;
+        trx = trx2;
+      }
+      int stop = 0;
+      if (dabs(occ - trx) < tol && it > c.minit) stop = 1;      // :112
+      else if (it == c.maxit) {                                 // :114
+        stop = 1;
+        nx.status = SP2B_NOT_CONVERGED;
+      }
+      nx.iter = it + 1;
+      nx.trx = trx;
+      nx.done = stop;
+      break;
+    }
+    default: {  // ALGO_SEQ
+      d.branch = pp_in[k] == 0 ? BR_2X_MINUS_X2 : BR_X2;
+      nx.iter = k + 1;
+      nx.done = (k + 1 >= c.icount) ? 1 : 0;
+      // tracked trace as the reference does (:596 / :1060); informational only
+      nx.trx = (d.branch == BR_2X_MINUS_X2) ? 2.0 * r.trx_data - r.fro2 : r.fro2;
+      break;
+    }
+  }
+  return d;
+}
+
+}  // namespace sp2b
+
+#define SP2B_CUDA_TRY(expr)                                                         \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess) {                                                        \
+      sp2b::set_last_error("%s:%d %s: %s", __FILE__, __LINE__, #expr,              \
+                           cudaGetErrorString(_e));                                 \
+      return SP2B_CUDA_ERROR;                                                       \
+    }                                                                               \
+  } while (0)
+
+namespace sp2b {
+void set_last_error(const char* fmt, ...);
+}

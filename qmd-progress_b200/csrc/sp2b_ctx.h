@@ -1,0 +1,74 @@
+// Per-device library context and the dense-solve job description.
+#pragma once
+#include <algorithm>
+#include <mutex>
+
+#include "kernels.cuh"
+
+namespace sp2b {
+
+struct Ctx {
+  bool init = false;
+  int dev = -1;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  // FP64 square buffers (np x np): ping-pong iterates, plus one for McWeeny
+  double* x64[3] = {nullptr, nullptr, nullptr};
+  size_t x64_cap[3] = {0, 0, 0};
+  // split-precision iterates (hi/lo ping-pong)
+  __half* hi[2] = {nullptr, nullptr};
+  __half* lo[2] = {nullptr, nullptr};
+  size_t hi_cap[2] = {0, 0}, lo_cap[2] = {0, 0};
+  // host-pointer staging of H / rho (n x n)
+  double* hin = nullptr;
+  size_t hin_cap = 0;
+  // reductions and control
+  double* partials = nullptr;
+  size_t partials_cap = 0;
+  unsigned* counter = nullptr;
+  SP2Rec* rec = nullptr;
+  size_t rec_cap = 0;
+  int* pp_dev = nullptr;
+  size_t pp_cap = 0;
+  double* vv_dev = nullptr;
+  size_t vv_cap = 0;
+  double* rowsum = nullptr;
+  size_t rowsum_cap = 0;
+  double* small = nullptr;      // device scratch scalars
+  double* h_small = nullptr;    // pinned host mirror
+  SolveOut* sout = nullptr;
+  SolveOut* h_sout = nullptr;   // pinned
+  int* err = nullptr;
+
+  cudaError_t ensure_f64(int np, int nbuf);
+  cudaError_t ensure_split(int np);
+  cudaError_t ensure_common(size_t nin, int np, int maxlaunch, int n);
+};
+
+Ctx* get_ctx(int* status);
+
+struct DenseJob {
+  const double* h;
+  double* rho;
+  int n;
+  int prec;
+  bool dev_ptrs;
+  cudaStream_t stream;
+  bool inplace;        // H read from rho (the *_inplace routines)
+  bool given_bounds;   // use mineval/maxeval instead of Gershgorin
+  double mineval, maxeval;
+  SP2Ctl ctl;
+  const int* pp_in;
+  int* pp_out;
+  double* vv_out;
+  int vv_accumulate;
+  int core;
+  int* icount_out;
+  int* iters_out;
+  double* bounds_out;
+  int mcweeny;
+};
+
+int dense_solve(const DenseJob& j);
+
+}  // namespace sp2b

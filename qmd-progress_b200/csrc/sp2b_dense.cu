@@ -1,0 +1,659 @@
+// Host driver of the dense SP2 path and its C-ABI entry points.
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "sp2b_ctx.h"
+
+namespace sp2b {
+
+static thread_local char g_err[1024] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+// ------------------------------------------------------------------------------------
+// Per-device context: cached device buffers, one stream, pinned status words.
+// Calls on the same device are serialised by the context mutex.
+// ------------------------------------------------------------------------------------
+static Ctx g_ctx[64];
+static std::mutex g_ctx_mu;
+
+template <typename T>
+static cudaError_t grow(T*& p, size_t& cap, size_t need) {
+  if (need <= cap && p) return cudaSuccess;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc((void**)&p, need * sizeof(T));
+  if (e == cudaSuccess) cap = need;
+  return e;
+}
+
+Ctx* get_ctx(int* status) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    set_last_error("no CUDA device available");
+    *status = SP2B_NO_DEVICE;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  Ctx& c = g_ctx[dev];
+  if (!c.init) {
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost((void**)&c.h_sout, sizeof(SolveOut)) != cudaSuccess ||
+        cudaMallocHost((void**)&c.h_small, 64 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c.small, 64 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c.counter, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc((void**)&c.sout, sizeof(SolveOut)) != cudaSuccess ||
+        cudaMalloc((void**)&c.err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c.counter, 0, 4 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(c.err, 0, sizeof(int)) != cudaSuccess) {
+      set_last_error("context setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+      *status = SP2B_CUDA_ERROR;
+      return nullptr;
+    }
+    c.dev = dev;
+    c.init = true;
+  }
+  return &c;
+}
+
+cudaError_t Ctx::ensure_f64(int np, int nbuf) {
+  for (int i = 0; i < nbuf; ++i) {
+    cudaError_t e = grow(x64[i], x64_cap[i], (size_t)np * np);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t Ctx::ensure_split(int np) {
+  for (int i = 0; i < 2; ++i) {
+    cudaError_t e = grow(hi[i], hi_cap[i], (size_t)np * np);
+    if (e != cudaSuccess) return e;
+    e = grow(lo[i], lo_cap[i], (size_t)np * np);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t Ctx::ensure_common(size_t nin, int np, int maxlaunch, int n) {
+  cudaError_t e;
+  if (nin) {
+    e = grow(hin, hin_cap, nin);
+    if (e != cudaSuccess) return e;
+  }
+  const size_t parts = 4 * (size_t)std::max(std::max(f64_ntiles(np), tc_ntiles(np)), 148 * 8);
+  if ((e = grow(partials, partials_cap, parts)) != cudaSuccess) return e;
+  if ((e = grow(rec, rec_cap, (size_t)maxlaunch + 2)) != cudaSuccess) return e;
+  if ((e = grow(pp_dev, pp_cap, (size_t)maxlaunch + 2)) != cudaSuccess) return e;
+  if ((e = grow(vv_dev, vv_cap, (size_t)maxlaunch + 2)) != cudaSuccess) return e;
+  const int nsplit = gersh_nsplit(std::max(n, 1));
+  if ((e = grow(rowsum, rowsum_cap, (size_t)nsplit * std::max(n, 1))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// ------------------------------------------------------------------------------------
+// Dense solve
+// ------------------------------------------------------------------------------------
+static int parse_conv(const char* s) {
+  if (!s) return CONV_NONE;
+  // Fortran blank-padded comparison: "Rel" == "Rel   "; case-sensitive.
+  std::string t(s);
+  while (!t.empty() && t.back() == ' ') t.pop_back();
+  if (t == "Rel") return CONV_REL;
+  if (t == "Abs") return CONV_ABS;
+  return CONV_NONE;
+}
+
+static cudaStream_t pick_stream(const sp2b_opts* o, Ctx* c) {
+  return (o && o->stream) ? (cudaStream_t)o->stream : c->stream;
+}
+
+int dense_solve(const DenseJob& j) {
+  if (j.n <= 0 || !j.rho || (!j.h && !j.inplace)) {
+    set_last_error("bad argument: n=%d h=%p rho=%p", j.n, (void*)j.h, (void*)j.rho);
+    return SP2B_BAD_ARG;
+  }
+  if (j.ctl.algo == ALGO_SEQ && j.ctl.icount < 0) {
+    set_last_error("bad argument: icount=%d", j.ctl.icount);
+    return SP2B_BAD_ARG;
+  }
+  if (j.ctl.algo != ALGO_SEQ && j.ctl.maxit < 1) {
+    set_last_error("bad argument: maxsp2iter=%d", j.ctl.maxit);
+    return SP2B_BAD_ARG;
+  }
+  if (j.ctl.algo == ALGO_SEQ && j.ctl.icount > 0 && !j.pp_in) {
+    set_last_error("bad argument: pp is NULL");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t st = j.stream ? j.stream : c->stream;
+  const int n = j.n, np = padded(n);
+  const bool split = j.prec != SP2B_PREC_FP64;
+  const int bf16 = j.prec == SP2B_PREC_MIXED_BF16;
+  int maxlaunch;
+  if (j.ctl.algo == ALGO_SEQ) maxlaunch = j.ctl.icount;
+  else if (j.ctl.algo == ALGO_BASIC) maxlaunch = j.ctl.maxit + 1;
+  else maxlaunch = j.ctl.maxit;
+
+  const size_t nn = (size_t)n * n;
+  SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
+  SP2B_CUDA_TRY(c->ensure_f64(np, split ? 3 : 2));
+  if (split) SP2B_CUDA_TRY(c->ensure_split(np));
+
+  // ---- input ----
+  const double* hsrc = j.inplace ? j.rho : j.h;
+  const double* hdev = hsrc;
+  if (!j.dev_ptrs) {
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, hsrc, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    hdev = c->hin;
+  }
+  double* bounds = c->small;       // [0..1]
+  double* norm_out = c->small + 4; // [4..7]
+  if (j.given_bounds) {
+    c->h_small[0] = j.mineval;
+    c->h_small[1] = j.maxeval;
+    SP2B_CUDA_TRY(cudaMemcpyAsync(bounds, c->h_small, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    SP2B_CUDA_TRY(launch_gersh(hdev, n, n, c->rowsum, gersh_nsplit(n), bounds, st));
+  }
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), st));
+  if (split)
+    SP2B_CUDA_TRY(launch_normalize_split(hdev, n, n, np, bounds, c->hi[0], c->lo[0], bf16,
+                                         c->partials, c->counter, c->rec, norm_out, st));
+  else
+    SP2B_CUDA_TRY(launch_normalize_f64(hdev, n, n, np, bounds, c->x64[0], c->partials, c->counter,
+                                       c->rec, norm_out, st));
+
+  // ---- control inputs ----
+  if (j.ctl.algo == ALGO_SEQ && j.ctl.icount > 0) {
+    if (j.dev_ptrs)
+      SP2B_CUDA_TRY(cudaMemcpyAsync(c->pp_dev, j.pp_in, j.ctl.icount * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    else
+      SP2B_CUDA_TRY(cudaMemcpyAsync(c->pp_dev, j.pp_in, j.ctl.icount * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  if (j.vv_out && j.vv_accumulate && maxlaunch > 0) {
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->vv_dev, j.vv_out, maxlaunch * sizeof(double),
+                                  j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  } else {
+    SP2B_CUDA_TRY(cudaMemsetAsync(c->vv_dev, 0, (maxlaunch + 2) * sizeof(double), st));
+  }
+  int* pp_out_dev = (j.ctl.algo == ALGO_SEQ) ? nullptr : c->pp_dev;
+
+  // ---- SP2 steps: one launch each, chunked host polling of the device "done" word ----
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.np = np;
+  a.control = 1;
+  a.ctl = j.ctl;
+  a.rec = c->rec;
+  a.pp_in = c->pp_dev;
+  a.pp_out = pp_out_dev;
+  a.vv_out = c->vv_dev;
+  a.vv_accumulate = j.vv_accumulate;
+  a.core = j.core;
+  a.sout = c->sout;
+  a.partials = c->partials;
+  a.counter = c->counter;
+  a.err = c->err;
+  int k = 0;
+  int chunk = 4;
+  bool done = (maxlaunch == 0);
+  while (!done && k < maxlaunch) {
+    const int kend = std::min(maxlaunch, k + chunk);
+    for (; k < kend; ++k) {
+      a.k = k;
+      const int bin = k & 1, bout = (k + 1) & 1;
+      if (split) {
+        a.A = a.B = a.E = c->hi[bin];
+        a.A_lo = a.B_lo = a.E_lo = c->lo[bin];
+        a.out = c->hi[bout];
+        a.out_lo = c->lo[bout];
+        a.ntiles = tc_ntiles(np);
+        SP2B_CUDA_TRY(launch_sym_gemm_tc(a, bf16, st));
+      } else {
+        a.A = a.B = a.E = c->x64[bin];
+        a.out = c->x64[bout];
+        a.ntiles = f64_ntiles(np);
+        SP2B_CUDA_TRY(launch_sym_gemm_f64(a, st));
+      }
+    }
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_sout, c->sout, sizeof(SolveOut), cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    done = c->h_sout->done != 0;
+    chunk = std::min(chunk * 2, 16);
+  }
+  SolveOut so = *c->h_sout;
+  if (maxlaunch == 0) so.nupd = 0;
+  // normalisation itself may have flagged bad input
+  SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small + 8, norm_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  const double emin = c->h_small[8], emax = c->h_small[9];
+  if (!(emax - emin > 0.0) || !(emin == emin) || !(emax == emax)) {
+    set_last_error("non-finite or degenerate spectral bounds (%g, %g)", emin, emax);
+    return SP2B_BAD_INPUT;
+  }
+  if (!done && maxlaunch > 0) {
+    set_last_error("SP2 loop ended without a final state");
+    return SP2B_CUDA_ERROR;
+  }
+
+  // ---- final density: D = 2 X (FP64) or FP64 McWeeny refinement of the split iterate ----
+  const int fb = so.nupd & 1;
+  double* xfin;
+  if (split) {
+    SP2B_CUDA_TRY(launch_split_to_f64(c->hi[fb], c->lo[fb], np, bf16, c->x64[0], st));
+    double* X = c->x64[0];
+    double* P = c->x64[1];
+    double* D = c->x64[2];
+    for (int m = 0; m < j.mcweeny; ++m) {
+      StepArgs q;
+      memset(&q, 0, sizeof(q));
+      q.np = np;
+      q.partials = c->partials;
+      q.counter = c->counter;
+      q.sums_out = c->small + 16;
+      // P = X X
+      q.A = q.B = q.E = X;
+      q.out = P;
+      q.alpha = 1.0;
+      q.beta = 0.0;
+      SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+      // D = 3 P - 2 P X   (McWeeny: 3X^2 - 2X^3)
+      q.A = P;
+      q.B = X;
+      q.E = P;
+      q.out = D;
+      q.alpha = -2.0;
+      q.beta = 3.0;
+      SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+      std::swap(X, D);
+    }
+    xfin = X;
+  } else {
+    xfin = c->x64[fb];
+  }
+  double* rho_dev = j.dev_ptrs ? j.rho : c->hin;
+  SP2B_CUDA_TRY(launch_finish_f64(xfin, np, n, 2.0, rho_dev, n, st));
+  if (!j.dev_ptrs)
+    SP2B_CUDA_TRY(cudaMemcpyAsync(j.rho, rho_dev, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+
+  // ---- sequence outputs ----
+  const int iters = so.iter;
+  if (j.pp_out && iters > 0)
+    SP2B_CUDA_TRY(cudaMemcpyAsync(j.pp_out, c->pp_dev, iters * sizeof(int),
+                                  j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  if (j.vv_out) {
+    const int nvv = j.vv_accumulate ? maxlaunch : (j.ctl.algo == ALGO_SEQ ? j.ctl.icount : iters);
+    if (nvv > 0)
+      SP2B_CUDA_TRY(cudaMemcpyAsync(j.vv_out, c->vv_dev, nvv * sizeof(double),
+                                    j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  }
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  if (j.icount_out) *j.icount_out = iters;
+  if (j.iters_out) *j.iters_out = iters;
+  if (j.bounds_out) {
+    j.bounds_out[0] = emin;
+    j.bounds_out[1] = emax;
+  }
+  if (so.status != SP2B_OK) {
+    if (so.status == SP2B_NOT_CONVERGED)
+      set_last_error("SP2 purification is not converging (maxsp2iter=%d)", j.ctl.maxit);
+    else if (so.status == SP2B_TIMEOUT)
+      set_last_error("a device-side wait timed out");
+    else if (so.status == SP2B_BAD_INPUT)
+      set_last_error("non-finite values during SP2");
+    return so.status;
+  }
+  return SP2B_OK;
+}
+
+}  // namespace sp2b
+
+using namespace sp2b;
+
+// ======================================================================================
+// C ABI
+// ======================================================================================
+extern "C" {
+
+const char* sp2b_last_error(void) { return g_err; }
+
+int sp2b_opts_default(sp2b_opts* o) {
+  if (!o) return SP2B_BAD_ARG;
+  memset(o, 0, sizeof(*o));
+  o->precision = SP2B_PREC_FP64;
+  o->mcweeny = 1;
+  o->mixed_tol = 1e-3;
+  return SP2B_OK;
+}
+
+static std::mutex g_def_mu;
+static bool g_def_init = false;
+static sp2b_opts g_def;
+
+int sp2b_get_default_opts(sp2b_opts* o) {
+  if (!o) return SP2B_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_def_mu);
+  if (!g_def_init) {
+    sp2b_opts_default(&g_def);
+    const char* e = getenv("SP2B_PRECISION");
+    if (e) {
+      if (!strcmp(e, "mixed") || !strcmp(e, "mixed_fp16")) g_def.precision = SP2B_PREC_MIXED_FP16;
+      else if (!strcmp(e, "mixed_bf16")) g_def.precision = SP2B_PREC_MIXED_BF16;
+    }
+    g_def_init = true;
+  }
+  *o = g_def;
+  return SP2B_OK;
+}
+
+int sp2b_set_default_opts(const sp2b_opts* o) {
+  if (!o) return SP2B_BAD_ARG;
+  std::lock_guard<std::mutex> lk(g_def_mu);
+  g_def = *o;
+  g_def_init = true;
+  return SP2B_OK;
+}
+
+static DenseJob base_job(const double* h, double* rho, int n, const sp2b_opts* o) {
+  DenseJob j;
+  memset(&j, 0, sizeof(j));
+  sp2b_opts d;
+  if (!o) {
+    sp2b_opts_default(&d);
+    o = &d;
+  }
+  j.h = h;
+  j.rho = rho;
+  j.n = n;
+  j.prec = o->precision;
+  j.dev_ptrs = o->device_ptrs != 0;
+  j.stream = (cudaStream_t)o->stream;
+  j.mcweeny = o->mcweeny;
+  j.ctl.n = n;
+  j.ctl.mixed_tol = o->mixed_tol;
+  j.ctl.icount = 0;
+  return j;
+}
+
+static void set_trace_ctl(DenseJob& j, int algo, double bndfil, int minit, int maxit,
+                          const char* conv, double idemtol) {
+  j.ctl.algo = algo;
+  if (j.prec != SP2B_PREC_FP64 && algo != ALGO_SEQ) j.ctl.algo = ALGO_MIXED;
+  j.ctl.minit = minit;
+  j.ctl.maxit = maxit;
+  j.ctl.conv = parse_conv(conv);
+  j.ctl.idemtol = idemtol;
+  j.ctl.occ = bndfil * (double)j.n;
+}
+
+int sp2b_sp2_alg2(const double* h, double* rho, int n, double threshold, double bndfil,
+                  int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                  int verbose, const sp2b_opts* opts, int* iters_out) {
+  (void)threshold; (void)verbose;
+  DenseJob j = base_job(h, rho, n, opts);
+  set_trace_ctl(j, ALGO_ALG2, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.iters_out = iters_out;
+  return dense_solve(j);
+}
+
+int sp2b_sp2_alg2_genseq(const double* h, double* rho, int n, double threshold, double bndfil,
+                         int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                         int* pp, int* icount, double* vv, int verbose, const sp2b_opts* opts) {
+  (void)threshold; (void)verbose;
+  DenseJob j = base_job(h, rho, n, opts);
+  set_trace_ctl(j, ALGO_ALG2_GENSEQ, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.pp_out = pp;
+  j.vv_out = vv;
+  j.icount_out = icount;
+  return dense_solve(j);
+}
+
+static int seq_job(const double* h, double* rho, int n, const int* pp, int icount, double* vv,
+                   bool inplace, double mineval, double maxeval, int core, int accumulate,
+                   const sp2b_opts* opts) {
+  DenseJob j = base_job(h, rho, n, opts);
+  j.ctl.algo = ALGO_SEQ;
+  j.ctl.icount = icount;
+  j.pp_in = pp;
+  j.vv_out = vv;
+  j.inplace = inplace;
+  j.given_bounds = inplace;
+  j.mineval = mineval;
+  j.maxeval = maxeval;
+  j.core = core;
+  j.vv_accumulate = accumulate;
+  return dense_solve(j);
+}
+
+int sp2b_sp2_alg2_seq(const double* h, double* rho, int n, double threshold, const int* pp,
+                      int icount, double* vv, int verbose, const sp2b_opts* opts) {
+  (void)threshold; (void)verbose;
+  return seq_job(h, rho, n, pp, icount, vv, false, 0, 0, 0, 0, opts);
+}
+
+int sp2b_sp2_alg2_seq_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                              double* vv, double mineval, double maxeval, int verbose,
+                              const sp2b_opts* opts) {
+  (void)threshold; (void)verbose;
+  return seq_job(nullptr, rho, n, pp, icount, vv, true, mineval, maxeval, 0, 0, opts);
+}
+
+int sp2b_sp2_alg1(const double* h, double* rho, int n, double threshold, double bndfil,
+                  int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                  int verbose, const sp2b_opts* opts, int* iters_out) {
+  (void)threshold; (void)verbose;
+  DenseJob j = base_job(h, rho, n, opts);
+  set_trace_ctl(j, ALGO_ALG1, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.iters_out = iters_out;
+  return dense_solve(j);
+}
+
+int sp2b_sp2_alg1_genseq(const double* h, double* rho, int n, double threshold, double bndfil,
+                         int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                         int* pp, int* icount, double* vv, const sp2b_opts* opts) {
+  (void)threshold;
+  DenseJob j = base_job(h, rho, n, opts);
+  set_trace_ctl(j, ALGO_ALG1_GENSEQ, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.pp_out = pp;
+  j.vv_out = vv;
+  j.icount_out = icount;
+  return dense_solve(j);
+}
+
+int sp2b_sp2_alg1_seq(const double* h, double* rho, int n, double threshold, const int* pp,
+                      int icount, double* vv, const sp2b_opts* opts) {
+  (void)threshold;
+  return seq_job(h, rho, n, pp, icount, vv, false, 0, 0, 0, 0, opts);
+}
+
+int sp2b_sp2_alg1_seq_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                              double* vv, double mineval, double maxeval, const sp2b_opts* opts) {
+  (void)threshold;
+  return seq_job(nullptr, rho, n, pp, icount, vv, true, mineval, maxeval, 0, 0, opts);
+}
+
+int sp2b_sp2_basic(const double* h, double* rho, int n, double threshold, double bndfil,
+                   int minsp2iter, int maxsp2iter, const char* sp2conv, double idemtol,
+                   int verbose, const sp2b_opts* opts, int* iters_out) {
+  (void)threshold; (void)verbose;
+  DenseJob j = base_job(h, rho, n, opts);
+  set_trace_ctl(j, ALGO_BASIC, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.iters_out = iters_out;
+  return dense_solve(j);
+}
+
+int sp2b_sp2_submatrix_inplace(double* rho, int n, double threshold, const int* pp, int icount,
+                               double* vv, double mineval, double maxeval, int core_size,
+                               const sp2b_opts* opts) {
+  (void)threshold;
+  if (core_size < 0 || core_size > n) {
+    set_last_error("bad argument: core_size=%d n=%d", core_size, n);
+    return SP2B_BAD_ARG;
+  }
+  return seq_job(nullptr, rho, n, pp, icount, vv, true, mineval, maxeval,
+                 core_size > 0 ? core_size : -1, 1, opts);
+}
+
+int sp2b_sp2_submatrix(const double* ham, double* rho, int n, double threshold, const int* pp,
+                       int icount, double* vv, double mineval, double maxeval, int core_size,
+                       const sp2b_opts* opts) {
+  (void)threshold;
+  if (core_size < 0 || core_size > n) {
+    set_last_error("bad argument: core_size=%d n=%d", core_size, n);
+    return SP2B_BAD_ARG;
+  }
+  DenseJob j = base_job(ham, rho, n, opts);
+  j.ctl.algo = ALGO_SEQ;
+  j.ctl.icount = icount;
+  j.pp_in = pp;
+  j.vv_out = vv;
+  j.given_bounds = true;
+  j.mineval = mineval;
+  j.maxeval = maxeval;
+  j.core = core_size > 0 ? core_size : -1;
+  j.vv_accumulate = 1;
+  return dense_solve(j);
+}
+
+int sp2b_gershgorin(const double* h, int n, double* mineval, double* maxeval,
+                    const sp2b_opts* opts) {
+  if (n <= 0 || !h || !mineval || !maxeval) {
+    set_last_error("bad argument");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const bool dev = opts && opts->device_ptrs;
+  cudaStream_t st = pick_stream(opts, c);
+  const size_t nn = (size_t)n * n;
+  SP2B_CUDA_TRY(c->ensure_common(dev ? 0 : nn, padded(n), 1, n));
+  const double* hd = h;
+  if (!dev) {
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, h, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    hd = c->hin;
+  }
+  SP2B_CUDA_TRY(launch_gersh(hd, n, n, c->rowsum, gersh_nsplit(n), c->small, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small, c->small, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  *mineval = c->h_small[0];
+  *maxeval = c->h_small[1];
+  if (!(c->h_small[0] == c->h_small[0]) || !(c->h_small[1] == c->h_small[1])) {
+    set_last_error("non-finite values in H");
+    return SP2B_BAD_INPUT;
+  }
+  return SP2B_OK;
+}
+
+int sp2b_normalize(double* h, int n, double* mineval, double* maxeval, const sp2b_opts* opts) {
+  double lo, hi;
+  int s = sp2b_gershgorin(h, n, &lo, &hi, opts);
+  if (s != SP2B_OK) return s;
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const bool dev = opts && opts->device_ptrs;
+  cudaStream_t st = pick_stream(opts, c);
+  const int np = padded(n);
+  const size_t nn = (size_t)n * n;
+  SP2B_CUDA_TRY(c->ensure_common(dev ? 0 : nn, np, 1, n));
+  SP2B_CUDA_TRY(c->ensure_f64(np, 1));
+  const double* hd = h;
+  if (!dev) {
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, h, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    hd = c->hin;
+  }
+  c->h_small[0] = lo;
+  c->h_small[1] = hi;
+  SP2B_CUDA_TRY(cudaMemcpyAsync(c->small, c->h_small, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
+  SP2B_CUDA_TRY(launch_normalize_f64(hd, n, n, np, c->small, c->x64[0], c->partials, c->counter,
+                                     c->rec, c->small + 4, st));
+  double* out = dev ? h : c->hin;
+  SP2B_CUDA_TRY(launch_finish_f64(c->x64[0], np, n, 1.0, out, n, st));
+  if (!dev) SP2B_CUDA_TRY(cudaMemcpyAsync(h, out, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  if (mineval) *mineval = lo;
+  if (maxeval) *maxeval = hi;
+  return SP2B_OK;
+}
+
+int sp2b_check_idempotency(const double* a, int n, double threshold, double* idempotency,
+                           const sp2b_opts* opts) {
+  (void)threshold;
+  if (n <= 0 || !a || !idempotency) {
+    set_last_error("bad argument");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const bool dev = opts && opts->device_ptrs;
+  cudaStream_t st = pick_stream(opts, c);
+  const int np = padded(n);
+  const size_t nn = (size_t)n * n;
+  SP2B_CUDA_TRY(c->ensure_common(dev ? 0 : nn, np, 1, n));
+  SP2B_CUDA_TRY(c->ensure_f64(np, 1));
+  const double* ad = a;
+  if (!dev) {
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, a, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    ad = c->hin;
+  }
+  SP2B_CUDA_TRY(launch_copy_in(ad, n, n, np, c->x64[0], st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
+  StepArgs q;
+  memset(&q, 0, sizeof(q));
+  q.np = np;
+  q.A = q.B = q.E = c->x64[0];
+  q.out = nullptr;
+  q.alpha = 1.0;
+  q.beta = 0.0;
+  q.partials = c->partials;
+  q.counter = c->counter;
+  q.sums_out = c->small + 16;
+  SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small + 16, c->small + 16, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  *idempotency = sqrt(c->h_small[18]);
+  return SP2B_OK;
+}
+
+int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* cout, int n, void* stream) {
+  if (n <= 0 || !a || !b || !cout) {
+    set_last_error("bad argument");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const int np = padded(n);
+  SP2B_CUDA_TRY(c->ensure_split(np));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
+  SP2B_CUDA_TRY(launch_f32_to_split(a, n, np, c->hi[0], c->lo[0], st));
+  SP2B_CUDA_TRY(launch_f32_to_split(b, n, np, c->hi[1], c->lo[1], st));
+  SP2B_CUDA_TRY(launch_tc_plain(c->hi[0], c->lo[0], c->hi[1], c->lo[1], np, cout, n, st, c->err));
+  return SP2B_OK;
+}
+
+}  // extern "C"

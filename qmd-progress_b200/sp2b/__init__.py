@@ -1,0 +1,242 @@
+"""sp2b: B200-native SP2 density-matrix purification (Python view of the C ABI).
+
+The functions mirror the PROGRESS SP2 routines (src/prg_sp2_mod.F90) by name and
+argument meaning; matrices are FP64 numpy arrays (symmetric, so row/column-major
+coincide) and results come back as :class:`SP2Result`.  Every call goes through the
+CUDA library (libsp2b.so); nothing here computes on the CPU.  Where the reference
+stops the process on non-convergence, these raise :class:`SP2Error` with status
+``SP2B_NOT_CONVERGED``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (PREC_FP64, PREC_MIXED_BF16, PREC_MIXED_FP16, SP2Error, check, lib,
+                   make_opts)
+
+__all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq",
+           "sp2_alg2_seq_inplace", "sp2_alg1", "sp2_alg1_genseq", "sp2_alg1_seq",
+           "sp2_alg1_seq_inplace", "sp2_basic", "sp2_submatrix_inplace", "sp2_submatrix",
+           "gershgorin", "normalize", "check_idempotency", "sp2sequence", "homolumogap",
+           "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16"]
+
+
+@dataclass
+class SP2Result:
+    rho: np.ndarray
+    pp: list = field(default_factory=list)
+    vv: list = field(default_factory=list)
+    icount: int = 0
+    iters: int = 0
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("expected a square matrix")
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _opts(precision, mcweeny, mixed_tol):
+    return make_opts(precision=precision, mcweeny=mcweeny, mixed_tol=mixed_tol)
+
+
+def _conv(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+def sp2_alg2(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
+             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+    """prg_sp2_alg2 (src/prg_sp2_mod.F90:263-380)."""
+    h = _f64(h)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    it = C.c_int(0)
+    o = _opts(precision, mcweeny, mixed_tol)
+    check(lib().sp2b_sp2_alg2(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter, maxsp2iter,
+                              _conv(sp2conv), idemtol, 0, C.byref(o), C.byref(it)), "sp2_alg2")
+    return SP2Result(rho=rho, iters=it.value, icount=it.value)
+
+
+def sp2_alg2_genseq(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
+                    threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+    """prg_sp2_alg2_genseq (src/prg_sp2_mod.F90:395-533): also pp, icount, vv."""
+    h = _f64(h)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    pp = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.int32)
+    vv = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.float64)
+    ic = C.c_int(0)
+    o = _opts(precision, mcweeny, mixed_tol)
+    check(lib().sp2b_sp2_alg2_genseq(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter,
+                                     maxsp2iter, _conv(sp2conv), idemtol, _ptr(pp), C.byref(ic),
+                                     _ptr(vv), 0, C.byref(o)), "sp2_alg2_genseq")
+    k = ic.value
+    return SP2Result(rho=rho, pp=pp[:k].tolist(), vv=vv[:k].tolist(), icount=k, iters=k)
+
+
+def _seq_common(fn_name, h, pp, icount, inplace, mineval=0.0, maxeval=0.0, precision=PREC_FP64):
+    h = _f64(h)
+    n = h.shape[0]
+    pp_a = np.ascontiguousarray(pp, dtype=np.int32)
+    vv = np.zeros(max(icount, 1), dtype=np.float64)
+    o = _opts(precision, 1, 1e-3)
+    L = lib()
+    if inplace:
+        rho = h.copy()
+        extra = (0,) if fn_name == "sp2b_sp2_alg2_seq_inplace" else ()
+        check(getattr(L, fn_name)(_ptr(rho), n, 0.0, _ptr(pp_a), icount, _ptr(vv), mineval, maxeval,
+                                  *extra, C.byref(o)), fn_name)
+    else:
+        rho = np.empty_like(h)
+        extra = (0,) if fn_name == "sp2b_sp2_alg2_seq" else ()
+        check(getattr(L, fn_name)(_ptr(h), _ptr(rho), n, 0.0, _ptr(pp_a), icount, _ptr(vv), *extra,
+                                  C.byref(o)), fn_name)
+    return SP2Result(rho=rho, pp=list(pp_a[:icount]), vv=vv[:icount].tolist(), icount=icount,
+                     iters=icount)
+
+
+def sp2_alg2_seq(h, pp, icount, precision=PREC_FP64):
+    """prg_sp2_alg2_seq (src/prg_sp2_mod.F90:543-627)."""
+    return _seq_common("sp2b_sp2_alg2_seq", h, pp, icount, False, precision=precision)
+
+
+def sp2_alg2_seq_inplace(rho, pp, icount, mineval, maxeval, precision=PREC_FP64):
+    """prg_prg_sp2_alg2_seq_inplace (src/prg_sp2_mod.F90:638-722)."""
+    return _seq_common("sp2b_sp2_alg2_seq_inplace", rho, pp, icount, True, mineval, maxeval,
+                       precision)
+
+
+def sp2_alg1(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
+             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+    """prg_sp2_alg1 (src/prg_sp2_mod.F90:734-864)."""
+    h = _f64(h)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    it = C.c_int(0)
+    o = _opts(precision, mcweeny, mixed_tol)
+    check(lib().sp2b_sp2_alg1(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter, maxsp2iter,
+                              _conv(sp2conv), idemtol, 0, C.byref(o), C.byref(it)), "sp2_alg1")
+    return SP2Result(rho=rho, iters=it.value, icount=it.value)
+
+
+def sp2_alg1_genseq(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
+                    threshold=0.0, precision=PREC_FP64):
+    """prg_sp2_alg1_genseq (src/prg_sp2_mod.F90:879-1000)."""
+    h = _f64(h)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    pp = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.int32)
+    vv = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.float64)
+    ic = C.c_int(0)
+    o = _opts(precision, 1, 1e-3)
+    check(lib().sp2b_sp2_alg1_genseq(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter,
+                                     maxsp2iter, _conv(sp2conv), idemtol, _ptr(pp), C.byref(ic),
+                                     _ptr(vv), C.byref(o)), "sp2_alg1_genseq")
+    k = ic.value
+    return SP2Result(rho=rho, pp=pp[:k].tolist(), vv=vv[:k].tolist(), icount=k, iters=k)
+
+
+def sp2_alg1_seq(h, pp, icount):
+    """prg_sp2_alg1_seq (src/prg_sp2_mod.F90:1010-1089)."""
+    return _seq_common("sp2b_sp2_alg1_seq", h, pp, icount, False)
+
+
+def sp2_alg1_seq_inplace(rho, pp, icount, mineval, maxeval):
+    """prg_prg_sp2_alg1_seq_inplace (src/prg_sp2_mod.F90:1100-1177)."""
+    return _seq_common("sp2b_sp2_alg1_seq_inplace", rho, pp, icount, True, mineval, maxeval)
+
+
+def sp2_basic(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
+              threshold=0.0, precision=PREC_FP64):
+    """prg_sp2_basic (src/prg_sp2_mod.F90:49-135)."""
+    h = _f64(h)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    it = C.c_int(0)
+    o = _opts(precision, 1, 1e-3)
+    check(lib().sp2b_sp2_basic(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter, maxsp2iter,
+                               _conv(sp2conv), idemtol, 0, C.byref(o), C.byref(it)), "sp2_basic")
+    return SP2Result(rho=rho, iters=it.value, icount=it.value)
+
+
+def sp2_submatrix_inplace(x, pp, icount, vv, mineval, maxeval, core_size):
+    """prg_sp2_submatrix_inplace (src/prg_sp2_mod.F90:1259-1310); vv is accumulated in place."""
+    rho = _f64(x).copy()
+    n = rho.shape[0]
+    pp_a = np.ascontiguousarray(pp, dtype=np.int32)
+    if not (isinstance(vv, np.ndarray) and vv.dtype == np.float64 and vv.flags.c_contiguous):
+        raise TypeError("vv must be a contiguous float64 numpy array (accumulated in place)")
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_sp2_submatrix_inplace(_ptr(rho), n, 0.0, _ptr(pp_a), icount, _ptr(vv),
+                                           mineval, maxeval, core_size, C.byref(o)),
+          "sp2_submatrix_inplace")
+    return rho
+
+
+def sp2_submatrix(ham, pp, icount, vv, mineval, maxeval, core_size):
+    """prg_sp2_submatrix (src/prg_sp2_mod.F90:1190-1246)."""
+    return sp2_submatrix_inplace(ham, pp, icount, vv, mineval, maxeval, core_size)
+
+
+def gershgorin(h):
+    h = _f64(h)
+    lo, hi = C.c_double(), C.c_double()
+    check(lib().sp2b_gershgorin(_ptr(h), h.shape[0], C.byref(lo), C.byref(hi), None), "gershgorin")
+    return lo.value, hi.value
+
+
+def normalize(h):
+    """prg_normalize (src/prg_normalize_mod.F90:32-46): returns (X0, mineval, maxeval)."""
+    x = _f64(h).copy()
+    lo, hi = C.c_double(), C.c_double()
+    check(lib().sp2b_normalize(_ptr(x), x.shape[0], C.byref(lo), C.byref(hi), None), "normalize")
+    return x, lo.value, hi.value
+
+
+def check_idempotency(a):
+    """prg_check_idempotency (src/prg_densitymatrix_mod.F90:862-880): ||A^2 - A||_F."""
+    a = _f64(a)
+    out = C.c_double()
+    check(lib().sp2b_check_idempotency(_ptr(a), a.shape[0], 0.0, C.byref(out), None),
+          "check_idempotency")
+    return out.value
+
+
+def sp2sequence(mineval, maxeval, ehomo, elumo, errlimit, ppmax=100):
+    """prg_sp2sequence (src/prg_homolumo_mod.F90:97-147): returns (pp, imax)."""
+    pp = (C.c_int * ppmax)()
+    imax = C.c_int(0)
+    check(lib().sp2b_sp2sequence(pp, C.byref(imax), mineval, maxeval, ehomo, elumo, errlimit,
+                                 ppmax), "sp2sequence")
+    return [pp[i] for i in range(imax.value)], imax.value
+
+
+def homolumogap(vv, imax, pp, mineval, maxeval):
+    """prg_homolumogap (src/prg_homolumo_mod.F90:22-89): returns (ehomo, elumo, egap)."""
+    vv_a = np.ascontiguousarray(vv, dtype=np.float64)
+    pp_a = np.ascontiguousarray(pp, dtype=np.int32)
+    eh, el, eg = C.c_double(), C.c_double(), C.c_double()
+    check(lib().sp2b_homolumogap(_ptr(vv_a), imax, _ptr(pp_a), mineval, maxeval, C.byref(eh),
+                                 C.byref(el), C.byref(eg)), "homolumogap")
+    return eh.value, el.value, eg.value
+
+
+def equal_partition(nodes_per_part, nnodes):
+    """prg_equalPartition (src/prg_graph_mod.F90:359-399): list of node arrays."""
+    npart = C.c_int(0)
+    check(lib().sp2b_equal_partition(nodes_per_part, nnodes, C.byref(npart), None, None),
+          "equal_partition")
+    ptr = np.zeros(npart.value + 1, dtype=np.int32)
+    nodes = np.zeros(nnodes, dtype=np.int32)
+    check(lib().sp2b_equal_partition(nodes_per_part, nnodes, C.byref(npart), _ptr(ptr), _ptr(nodes)),
+          "equal_partition")
+    return [nodes[ptr[i]:ptr[i + 1]].copy() for i in range(npart.value)]

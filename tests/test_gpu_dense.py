@@ -1,0 +1,209 @@
+"""Dense SP2 on the GPU, through the C ABI, against the CPU oracle.
+
+FP64 form: same branch sequence and iteration count as the oracle, D within 1e-10
+relative Frobenius, vv within 1e-9.  Mixed form (FP16 hi+lo tcgen05 products, FP64
+traces, FP64 McWeeny): the branch sequence agrees with the FP64 oracle on every step
+both took, and ||D - D_ref||_F / N <= 1e-6.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import sp2_oracle as O
+import sp2b
+from sp2b import _lib, modelham as M
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+@pytest.mark.parametrize("n", [2, 7, 33, 130, 256, 1024])
+def test_alg2_genseq_fp64_parity(cuda, n):
+    h = M.two_band_1d(n, seed=n)
+    ref = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    assert got.pp == ref.pp
+    assert got.icount == ref.icount
+    assert rel(got.rho, ref.rho) <= FP64_TOL
+    assert np.allclose(got.vv, ref.vv, rtol=1e-9, atol=1e-12)
+    assert np.array_equal(got.rho, got.rho.T)  # exactly symmetric by construction
+
+
+@pytest.mark.parametrize("fn_ora,fn_gpu", [
+    (O.sp2_alg2, sp2b.sp2_alg2), (O.sp2_alg1, sp2b.sp2_alg1), (O.sp2_basic, sp2b.sp2_basic),
+    (O.sp2_alg1_genseq, sp2b.sp2_alg1_genseq)])
+@pytest.mark.parametrize("conv", ["None", "Rel"])
+def test_dense_variants_fp64_parity(cuda, fn_ora, fn_gpu, conv):
+    n = 384
+    h = M.two_band_1d(n, seed=1)
+    ref = fn_ora(h, 0.5, 4, 100, conv, 1e-10)
+    got = fn_gpu(h, 0.5, 4, 100, conv, 1e-10)
+    assert got.iters == ref.iters
+    assert rel(got.rho, ref.rho) <= FP64_TOL
+    if got.pp:
+        assert got.pp == ref.pp[:ref.iters]
+
+
+def test_seq_variants_fp64_parity(cuda):
+    n = 300
+    h = M.two_band_1d(n, seed=4)
+    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    emin, emax = O.gershgorin(h)
+    for ora, gpu in [(O.sp2_alg2_seq(h, g.pp, g.icount), sp2b.sp2_alg2_seq(h, g.pp, g.icount)),
+                     (O.sp2_alg1_seq(h, g.pp, g.icount), sp2b.sp2_alg1_seq(h, g.pp, g.icount)),
+                     (O.sp2_alg2_seq_inplace(h, g.pp, g.icount, emin, emax),
+                      sp2b.sp2_alg2_seq_inplace(h, g.pp, g.icount, emin, emax)),
+                     (O.sp2_alg1_seq_inplace(h, g.pp, g.icount, emin, emax),
+                      sp2b.sp2_alg1_seq_inplace(h, g.pp, g.icount, emin, emax))]:
+        assert rel(gpu.rho, ora.rho) <= FP64_TOL
+        assert np.allclose(gpu.vv, ora.vv, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("core", [1, 50, 200])
+def test_submatrix_inplace_fp64_parity(cuda, core):
+    n = 200
+    h = M.two_band_1d(n, seed=8)
+    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    emin, emax = O.gershgorin(h)
+    vv_ref = [0.5] * g.icount
+    d_ref = O.sp2_submatrix_inplace(h.copy(), g.pp, g.icount, vv_ref, emin - 0.1, emax + 0.2, core)
+    vv = np.full(g.icount, 0.5)
+    d = sp2b.sp2_submatrix_inplace(h, g.pp, g.icount, vv, emin - 0.1, emax + 0.2, core)
+    assert rel(d, d_ref) <= FP64_TOL
+    assert np.allclose(vv, vv_ref, rtol=1e-9, atol=1e-12)
+
+
+def test_normalize_gershgorin_idempotency(cuda):
+    h = M.two_band_1d(257, seed=2)
+    lo, hi = sp2b.gershgorin(h)
+    rlo, rhi = O.gershgorin(h)
+    assert lo == pytest.approx(rlo, rel=1e-14) and hi == pytest.approx(rhi, rel=1e-14)
+    x, lo2, hi2 = sp2b.normalize(h)
+    assert np.allclose(x, O.normalize_bounds(h, rlo, rhi), rtol=0, atol=1e-15)
+    d = O.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10).rho
+    assert sp2b.check_idempotency(d / 2) == pytest.approx(O.check_idempotency(d / 2), rel=1e-6, abs=1e-14)
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=(129, 129))
+    a = (a + a.T) / 2
+    assert sp2b.check_idempotency(a) == pytest.approx(O.check_idempotency(a), rel=1e-12)
+
+
+def test_eigh_oracle_config0(cuda):
+    """Config 0: N=1024 two-band, FP64, stop at idempotency error < 1e-10."""
+    n = 1024
+    h = M.two_band_1d(n, seed=0)
+    dref, _ = O.build_density_t0(h, 0.5)
+    got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    assert np.linalg.norm(got.rho - dref) / n < 1e-12
+    assert abs(np.trace(got.rho) - n) < 1e-8
+    assert np.linalg.norm((got.rho / 2) @ (got.rho / 2) - got.rho / 2) < 1e-8
+
+
+def test_poly512_fp64_matches_fixture(cuda, poly512):
+    d = poly512
+    got = sp2b.sp2_alg2_genseq(d["h"], 0.5, 25, 100, "Rel", 1e-10)
+    assert got.pp == list(d["alg2_pp"])
+    assert got.icount == int(d["alg2_icount"])
+    assert np.allclose(got.vv, d["alg2_vv"], rtol=1e-8, atol=1e-10)
+    assert abs(np.trace(got.rho) - float(d["alg2_trace"])) < 1e-8
+    cols = d["sample_cols"]
+    assert np.allclose(got.rho[:, cols], d["alg2_rho_cols"], rtol=0, atol=1e-9)
+    # reference acceptance (tests/src/main.F90:382-414)
+    assert sp2b.check_idempotency(got.rho / 2) <= 1e-6
+
+
+def test_progress_named_exports(cuda):
+    n = 200
+    h = np.asfortranarray(M.two_band_1d(n, seed=6))
+    rho = np.zeros((n, n), order="F")
+    L = _lib.lib()
+    hb = L.sp2b_bml_wrap_dense(h.ctypes.data_as(C.c_void_p), n)
+    rb = L.sp2b_bml_wrap_dense(rho.ctypes.data_as(C.c_void_p), n)
+    L.prg_sp2_alg2(hb, rb, 1e-9, 0.5, 0, 100, b"Rel", 1e-10, 0)
+    assert L.sp2b_prg_last_status() == 0
+    ref = O.sp2_alg2(h, 0.5, 0, 100, "Rel", 1e-10)
+    assert rel(rho, ref.rho) <= FP64_TOL
+    idem = C.c_double()
+    half = np.asfortranarray(rho / 2)
+    hb2 = L.sp2b_bml_wrap_dense(half.ctypes.data_as(C.c_void_p), n)
+    L.prg_check_idempotency(hb2, 1e-9, C.byref(idem))
+    assert idem.value < 1e-8
+    pp = np.zeros(100, dtype=np.int32)
+    vv = np.zeros(100)
+    ic = C.c_int(0)
+    L.prg_sp2_alg2_genseq(hb, rb, 1e-9, 0.5, 0, 100, b"Rel", 1e-10,
+                          pp.ctypes.data_as(C.c_void_p), C.byref(ic), vv.ctypes.data_as(C.c_void_p), 0)
+    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "Rel", 1e-10)
+    assert ic.value == g.icount and list(pp[:ic.value]) == g.pp
+    for b in (hb, rb, hb2):
+        L.sp2b_bml_free(b)
+
+
+def test_error_statuses(cuda):
+    h = M.two_band_1d(64, seed=1)
+    with pytest.raises(_lib.SP2Error) as e:
+        sp2b.sp2_alg2(h, 0.5, 0, 3, "None", 1e-10)
+    assert e.value.status == _lib.SP2B_NOT_CONVERGED
+    with pytest.raises(_lib.SP2Error) as e:
+        sp2b.sp2_basic(h, 0.5, 0, 2, "None", 1e-10)
+    assert e.value.status == _lib.SP2B_NOT_CONVERGED
+    bad = h.copy()
+    bad[3, 5] = np.nan
+    with pytest.raises(_lib.SP2Error) as e:
+        sp2b.sp2_alg2(bad, 0.5)
+    assert e.value.status == _lib.SP2B_BAD_INPUT
+    with pytest.raises(_lib.SP2Error) as e:
+        sp2b.sp2_alg2(np.ones((1, 1)), 0.5)   # zero-width spectrum: bounds degenerate
+    assert e.value.status == _lib.SP2B_BAD_INPUT
+    with pytest.raises(_lib.SP2Error) as e:
+        sp2b.sp2_alg2(h, 0.5, 0, 0)
+    assert e.value.status == _lib.SP2B_BAD_ARG
+    # the library stays usable after errors
+    ok = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10)
+    assert rel(ok.rho, O.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10).rho) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [256, 1024, 2048])
+def test_mixed_fp16_against_fp64(cuda, n):
+    h = M.two_band_1d(n, seed=n + 1)
+    ref = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
+    k = min(len(got.pp), len(ref.pp))
+    assert got.pp[:k] == ref.pp[:k]
+    assert abs(len(got.pp) - len(ref.pp)) <= 2
+    err = np.linalg.norm(got.rho - ref.rho) / n
+    assert err <= 1e-6, err
+    assert abs(np.trace(got.rho) - n) < 1e-5 * n
+
+
+def test_mixed_bf16_runs(cuda):
+    n = 512
+    h = M.two_band_1d(n, seed=3)
+    ref = O.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10)
+    got = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_BF16)
+    assert np.linalg.norm(got.rho - ref.rho) / n <= 1e-5
+
+
+def test_dev_sym_gemm_f32(cuda):
+    torch = cuda
+    for n in (64, 200, 512):
+        g = torch.Generator().manual_seed(n)
+        a = torch.randn(n, n, generator=g, dtype=torch.float64)
+        b = torch.randn(n, n, generator=g, dtype=torch.float64)
+        a = ((a + a.T) / 2).float().cuda()
+        b = ((b + b.T) / 2).float().cuda()
+        c = torch.empty(n, n, device="cuda", dtype=torch.float32)
+        st = torch.cuda.current_stream().cuda_stream
+        _lib.check(_lib.lib().sp2b_dev_sym_gemm_f32(a.data_ptr(), b.data_ptr(), c.data_ptr(), n, st),
+                   "sym_gemm")
+        torch.cuda.synchronize()
+        ref = a.double() @ b.double()
+        err = ((c.double() - ref).norm() / ref.norm()).item()
+        assert err < 2e-6, (n, err)
