@@ -104,7 +104,7 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
         // e = Tr(X - X^2) is below mixed_tol, or has not improved over two steps
         // (the same two-step test as src/sp2_tensorcore/src/prg_sp2_tensorcore.cu:312).
         const double e = r.trx_data - r.fro2;
-        if (e <= c.mixed_tol || (r.iter >= 2 && e >= r.err_hist[0])) {
+        if (e <= c.mixed_tol || (r.iter >= 2 && r.err_hist[0] < 1.0 && e >= r.err_hist[0])) {
           d.branch = BR_STOP;
           it -= 1;
           trx = trxold;
