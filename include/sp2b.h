@@ -182,6 +182,22 @@ int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
  * computed as hi/lo FP16 tcgen05 products with FP32 accumulation. */
 int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* c, int n, void* stream);
 
+/* ---- diagnostics ------------------------------------------------------------------ */
+
+/* State of the last dense solve on the current device: SP2 step launches issued by
+ * the host, X updates applied, Fortran iteration count, status; and, if recs != NULL,
+ * up to max_recs control records as 8 doubles each
+ * {trx, trx_data, fro2, idemperr, iter, done, status, last_branch}. */
+int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, double* recs,
+                         int max_recs);
+
+/* Kernel launches issued by this library since load (all kernels, all devices), and
+ * the device time of the SP2 step kernels recorded with CUDA events when
+ * sp2b_set_step_timing(1) is on (ms, number of timed launches). */
+long long sp2b_launch_count(void);
+int sp2b_set_step_timing(int enable);
+int sp2b_step_timing(double* ms, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

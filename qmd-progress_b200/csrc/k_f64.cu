@@ -66,7 +66,9 @@ cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsp
   const int ncol = (n + nsplit - 1) / nsplit;
   dim3 grid((n + 255) / 256, nsplit);
   k_gersh_partial<<<grid, 256, 0, st>>>(h, n, ld, ncol, rowsum);
+  note_launch();
   k_gersh_final<<<1, 1024, 0, st>>>(h, n, ld, nsplit, rowsum, bounds);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -146,6 +148,7 @@ cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const d
                                  double* norm_out, cudaStream_t st) {
   k_normalize_f64<<<norm_grid(np), 256, 0, st>>>(h, n, ld, np, bounds, x, partials, counter,
                                                  rec0, norm_out);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -162,6 +165,7 @@ __global__ void k_copy_in(const double* __restrict__ src, int n, int ld, int np,
 cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,
                            cudaStream_t st) {
   k_copy_in<<<norm_grid(np), 256, 0, st>>>(src, n, ld, np, x);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -178,6 +182,7 @@ __global__ void k_finish_f64(const double* __restrict__ x, int np, int n, double
 cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, double* rho,
                               int ld, cudaStream_t st) {
   k_finish_f64<<<norm_grid(np), 256, 0, st>>>(x, np, n, scale, rho, ld);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -342,11 +347,13 @@ cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st) {
     auto kern = k_sym_gemm_f64<128, 2, 4>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
+    note_launch();
   } else {
     using C = F64Cfg<64, 2, 2>;
     auto kern = k_sym_gemm_f64<64, 2, 2>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
+    note_launch();
   }
   return cudaGetLastError();
 }

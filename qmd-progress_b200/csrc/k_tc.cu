@@ -498,6 +498,7 @@ static cudaError_t launch_tc(const StepArgs& a, dim3 grid, float* plain_out, int
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   kern<<<grid, 128, tc::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, plain_out, plain_n);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -541,6 +542,7 @@ cudaError_t launch_normalize_split(const double* h, int n, int ld, int np,
   else
     k_normalize_split<__half><<<g, 256, 0, st>>>(h, n, ld, np, bounds, hi, lo, partials, counter,
                                                  rec0, norm_out);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -552,12 +554,14 @@ cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int 
         (const __nv_bfloat16*)hi, (const __nv_bfloat16*)lo, total, x);
   else
     k_split_to_f64<__half><<<ew_grid(total), 256, 0, st>>>(hi, lo, total, x);
+  note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
                                 cudaStream_t st) {
   k_f32_to_split<<<ew_grid((size_t)np * np), 256, 0, st>>>(a, n, np, hi, lo);
+  note_launch();
   return cudaGetLastError();
 }
 

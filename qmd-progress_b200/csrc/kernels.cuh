@@ -4,6 +4,9 @@
 
 namespace sp2b {
 
+// Counts kernel launches issued by the library (diagnostics / bench).
+void note_launch(int k = 1);
+
 // Outcome of a dense solve, written by the device.
 struct SolveOut {
   int done;     // loop finished

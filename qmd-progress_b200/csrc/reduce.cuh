@@ -86,13 +86,16 @@ __device__ inline void publish_and_finalize(const StepArgs& p, double (&s)[4], d
 // Handles the start of a control-mode launch.  Returns the branch to apply, or -1 if
 // this launch has nothing to do (loop already finished or stopping before update).
 __device__ inline int control_prologue(const StepArgs& p) {
+  // The solve-wide done word is set by the launch that finished the loop; every
+  // later launch of the same solve (the host launches in chunks) returns at once.
+  if (*(volatile const int*)&p.sout->done) return -1;
   const SP2Rec r = p.rec[p.k];
   if (r.done) {
-    // Only reachable at k = 0 when normalisation flagged the input; later launches
-    // find sout->done already set by the launch that finished the loop.
-    if (p.k == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
-      p.sout->nupd = 0;
-      p.sout->iter = 0;
+    // Reached at k = 0 when normalisation flagged the input.
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      p.rec[p.k + 1] = r;
+      p.sout->nupd = p.k;
+      p.sout->iter = r.iter;
       p.sout->status = r.status;
       p.sout->done = 1;
     }

@@ -2,6 +2,7 @@
 #pragma once
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "kernels.cuh"
 
@@ -39,6 +40,8 @@ struct Ctx {
   SolveOut* sout = nullptr;
   SolveOut* h_sout = nullptr;   // pinned
   int* err = nullptr;
+  int last_launches = 0;            // SP2 step launches of the last dense solve
+  std::vector<cudaEvent_t> ev;      // step timing events (pairs)
 
   cudaError_t ensure_f64(int np, int nbuf);
   cudaError_t ensure_split(int np);

@@ -1,4 +1,5 @@
 // Host driver of the dense SP2 path and its C-ABI entry points.
+#include <atomic>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -12,6 +13,13 @@
 namespace sp2b {
 
 static thread_local char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+static std::atomic<int> g_step_timing{0};
+static std::mutex g_timing_mu;
+static double g_step_ms = 0.0;
+static long long g_step_timed = 0;
+
+void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 void set_last_error(const char* fmt, ...) {
   va_list ap;
@@ -213,10 +221,20 @@ int dense_solve(const DenseJob& j) {
   int k = 0;
   int chunk = 4;
   bool done = (maxlaunch == 0);
+  const bool timing = g_step_timing.load() != 0;
   while (!done && k < maxlaunch) {
     const int kend = std::min(maxlaunch, k + chunk);
+    const int k0 = k;
+    if (timing) {
+      while ((int)c->ev.size() < 2 * chunk) {
+        cudaEvent_t e;
+        SP2B_CUDA_TRY(cudaEventCreate(&e));
+        c->ev.push_back(e);
+      }
+    }
     for (; k < kend; ++k) {
       a.k = k;
+      if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev[2 * (k - k0)], st));
       const int bin = k & 1, bout = (k + 1) & 1;
       if (split) {
         a.A = a.B = a.E = c->hi[bin];
@@ -231,12 +249,29 @@ int dense_solve(const DenseJob& j) {
         a.ntiles = f64_ntiles(np);
         SP2B_CUDA_TRY(launch_sym_gemm_f64(a, st));
       }
+      if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev[2 * (k - k0) + 1], st));
     }
     SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_sout, c->sout, sizeof(SolveOut), cudaMemcpyDeviceToHost, st));
     SP2B_CUDA_TRY(cudaStreamSynchronize(st));
     done = c->h_sout->done != 0;
+    if (timing) {
+      // only launches that did work (k < the launch that finished the loop, + itself)
+      double ms = 0.0;
+      long long cnt = 0;
+      const int last = done ? std::max(c->h_sout->nupd, k0) : kend - 1;
+      for (int q = k0; q < kend && q <= last; ++q) {
+        float t = 0.f;
+        SP2B_CUDA_TRY(cudaEventElapsedTime(&t, c->ev[2 * (q - k0)], c->ev[2 * (q - k0) + 1]));
+        ms += t;
+        ++cnt;
+      }
+      std::lock_guard<std::mutex> lk2(g_timing_mu);
+      g_step_ms += ms;
+      g_step_timed += cnt;
+    }
     chunk = std::min(chunk * 2, 16);
   }
+  c->last_launches = k;
   SolveOut so = *c->h_sout;
   if (maxlaunch == 0) so.nupd = 0;
   // normalisation itself may have flagged bad input
@@ -634,6 +669,49 @@ int sp2b_check_idempotency(const double* a, int n, double threshold, double* ide
   SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small + 16, c->small + 16, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));
   *idempotency = sqrt(c->h_small[18]);
+  return SP2B_OK;
+}
+
+long long sp2b_launch_count(void) { return g_launches.load(); }
+
+int sp2b_set_step_timing(int enable) {
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  g_step_timing.store(enable ? 1 : 0);
+  g_step_ms = 0.0;
+  g_step_timed = 0;
+  return SP2B_OK;
+}
+
+int sp2b_step_timing(double* ms, long long* launches) {
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  if (ms) *ms = g_step_ms;
+  if (launches) *launches = g_step_timed;
+  return SP2B_OK;
+}
+
+int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, double* recs,
+                         int max_recs) {
+  int st = SP2B_OK;
+  Ctx* c = get_ctx(&st);
+  if (!c) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (!c->sout) return SP2B_BAD_ARG;
+  SolveOut so;
+  SP2B_CUDA_TRY(cudaMemcpy(&so, c->sout, sizeof(so), cudaMemcpyDeviceToHost));
+  if (launches) *launches = c->last_launches;
+  if (nupd) *nupd = so.nupd;
+  if (iter) *iter = so.iter;
+  if (status) *status = so.status;
+  if (recs && max_recs > 0 && c->rec) {
+    const int m = (int)std::min((size_t)max_recs, c->rec_cap);
+    std::vector<SP2Rec> r(m);
+    SP2B_CUDA_TRY(cudaMemcpy(r.data(), c->rec, m * sizeof(SP2Rec), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < m; ++i) {
+      double* o = recs + 8 * i;
+      o[0] = r[i].trx; o[1] = r[i].trx_data; o[2] = r[i].fro2; o[3] = r[i].idemperr;
+      o[4] = r[i].iter; o[5] = r[i].done; o[6] = r[i].status; o[7] = r[i].last_branch;
+    }
+  }
   return SP2B_OK;
 }
 
