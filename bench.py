@@ -1,0 +1,334 @@
+#!/usr/bin/env python3
+"""SP2 benchmark: dense mixed-precision SP2 solves/s on B200 (and the FP64 SP2 beside it).
+
+Workload (default): the two-band 1D model Hamiltonian at N=8192 (seeded), solved by the
+alg2 branch rule with FP16 hi+lo split products on the tcgen05 tensor cores, FP32
+accumulation, FP64 traces and one final FP64 McWeeny step.  A "step" is one complete
+solve H -> D.  Inputs (8192^2 FP64 = 512 MiB) are larger than L2 (126 MB), so no L2
+flush is needed between steps.
+
+  value   solves/s with H resident in HBM (device pointers through the C ABI)
+  e2e     solves/s through the C ABI with host buffers: H2D of H and D2H of D inside
+          every step
+  fp64    the same solve in FP64 (the parity form) for the mixed/FP64 ratio
+
+Multi-GPU (torchrun): independent replicas, one Hamiltonian per rank ("replicas only":
+a dense solve does not shard); value = total solves/s, timed as the max over ranks.
+
+--impl reference times the CPU restatement of the reference's FP64 dense alg2
+(oracle/sp2_oracle.py, numpy with the host BLAS, all host cores) on a bounded sample
+of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "qmd-progress_b200"))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--precision", default="mixed_fp16", choices=["mixed_fp16", "mixed_bf16", "fp64"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_sample(n, iters_per_solve, max_seconds=20.0):
+    """Oracle FP64 alg2 loop on the host cores: time whole SP2 iterations of the N x N
+    workload (bounded to ~max_seconds) and extrapolate to solves/s."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+    import sp2_oracle as O
+    from sp2b import modelham as M
+    h = M.two_band_1d(n, seed=0)
+    x, emin, emax = O.prg_normalize(h)
+    trx = float(np.trace(x))
+    occ = 0.5 * n
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        x2 = x @ x                                   # src/prg_sp2_mod.F90:308
+        trx2 = float(np.trace(x2))
+        limdiff = abs(trx2 - occ) - abs(2 * trx - trx2 - occ)
+        if limdiff >= 0:
+            x = 2.0 * x - x2
+            trx = 2 * trx - trx2
+        else:
+            x = x2
+            trx = trx2
+        done += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or done >= iters_per_solve:
+            break
+    t_iter = el / done
+    return {"value": 1.0 / (t_iter * iters_per_solve), "unit": "solves/s", "cores": os.cpu_count(),
+            "kind": "port", "t_iter_s": t_iter,
+            "sample": f"{done} FP64 SP2 iteration(s) of the N={n} two-band alg2 loop (numpy/OpenBLAS "
+                      f"DGEMM, {os.cpu_count()} threads), extrapolated to {iters_per_solve} iterations per solve"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n = args.n
+    iters = 12  # alg2 iterations of this workload (FP64 genseq, seed 0, any N >= 1024 of the model)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline_sample(min(n, 2048), 1, 5.0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = cpu_baseline_sample(n, iters, max_seconds=15.0)
+        vals.append(r["value"])
+    el = time.perf_counter() - t0
+    v = statistics.median(vals)
+    out = {"metric": "SP2 solves/s (dense two-band N=%d)" % n, "value": v, "unit": "solves/s",
+           "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"two_band_1d_n{n}_alg2", "n": n, "bndfil": 0.5, "seed": 0},
+           "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port",
+                            "sample": r["sample"]},
+           "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import sp2b
+    from sp2b import _lib, modelham as M
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    L = _lib.lib()
+    n = args.n
+    prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
+            "fp64": _lib.PREC_FP64}[args.precision]
+    h_np = M.two_band_1d(n, seed=rank)
+    stream = torch.cuda.current_stream()
+    h_dev = torch.from_numpy(h_np).cuda()
+    rho_dev = torch.empty_like(h_dev)
+    pp = np.zeros(128, dtype=np.int32)
+    vv = np.zeros(128)
+    ic = C.c_int(0)
+
+    def solve_dev(precision):
+        o = _lib.make_opts(precision=precision, device_ptrs=True, stream=stream.cuda_stream)
+        _lib.check(L.sp2b_sp2_alg2_genseq(h_dev.data_ptr(), rho_dev.data_ptr(), n, 0.0, 0.5, 0, 100,
+                                          b"None", 1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
+                                          C.byref(o)), "sp2_alg2_genseq")
+        return ic.value
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up ----
+    for _ in range(args.warmup):
+        iters = solve_dev(prec)
+    # ---- timed region: device-resident ----
+    L.sp2b_set_step_timing(1)
+    launches0 = L.sp2b_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            iters = solve_dev(prec)
+        ev1.record(stream)
+        barrier()
+    launches = L.sp2b_launch_count() - launches0
+    step_ms = C.c_double(0)
+    step_n = C.c_longlong(0)
+    L.sp2b_step_timing(C.byref(step_ms), C.byref(step_n))
+    L.sp2b_set_step_timing(0)
+    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * args.steps / (t_ms / 1e3)
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        h_host = torch.from_numpy(h_np).pin_memory()
+        rho_host = torch.empty_like(h_host).pin_memory()
+        o = _lib.make_opts(precision=prec, device_ptrs=False, stream=stream.cuda_stream)
+
+        def solve_host():
+            _lib.check(L.sp2b_sp2_alg2_genseq(h_host.data_ptr(), rho_host.data_ptr(), n, 0.0, 0.5, 0, 100,
+                                              b"None", 1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
+                                              C.byref(o)), "sp2_alg2_genseq(host)")
+        solve_host()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            solve_host()
+        e1.record(stream)
+        barrier()
+        te = max_over_ranks(e0.elapsed_time(e1))
+        e2e = {"value": world * args.steps / (te / 1e3), "unit": "solves/s",
+               "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8 + 2 * 128 * 8}
+
+    # ---- FP64 (parity form) beside it ----
+    fp64 = None
+    if prec != _lib.PREC_FP64 and args.fp64_steps > 0:
+        solve_dev(_lib.PREC_FP64)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.fp64_steps):
+            it64 = solve_dev(_lib.PREC_FP64)
+        f1.record(stream)
+        barrier()
+        tf = max_over_ranks(f0.elapsed_time(f1))
+        fp64 = {"solves_per_s": world * args.fp64_steps / (tf / 1e3), "iters": it64,
+                "ms_per_solve": tf / args.fp64_steps,
+                "tflops": world * args.fp64_steps * 2.0 * n ** 3 * it64 / (tf / 1e3) / 1e12}
+
+    # ---- roofline of the dominant kernel (the SP2 step) ----
+    peaks, src = load_peaks()
+    step_avg_ms = step_ms.value / max(step_n.value, 1)
+    flops_launch = 2.0 * n ** 3          # one N x N x N product per SP2 step (algorithmic)
+    achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
+    peak_key = "bf16_tflops_sustained" if "bf16_tflops_sustained" in peaks else "bf16_tflops"
+    peak = peaks[peak_key] if prec != _lib.PREC_FP64 else None
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        ent = tj.get(f"sp2_step_{args.precision}_n{n}")
+        if ent:
+            traffic = ent.get("bytes_per_launch")
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": traffic,
+                "peak_source": f"{src} {peak_key}", "kernel": "k_tc_gemm (SP2 step)",
+                "avg_launch_ms": step_avg_ms, "launches_timed": step_n.value,
+                "flops_per_launch": flops_launch}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(n, iters, max_seconds=20.0)
+    if rank == 0:
+        out = {"metric": "SP2 solves/s (dense two-band N=%d, mixed precision)" % n, "value": value,
+               "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f16" if prec == _lib.PREC_MIXED_FP16 else
+               ("bf16" if prec == _lib.PREC_MIXED_BF16 else "f64"),
+               "data": "synthetic",
+               "config": {"workload": f"two_band_1d_n{n}_{args.precision}_alg2_mcweeny1", "n": n,
+                          "bndfil": 0.5, "idemtol": 1e-10, "sp2_iters": iters,
+                          "parallelism": f"replicas{world}", "l2": "inputs 512 MiB > L2, no flush"},
+               # algorithmic: 2N^3 per SP2 step + 4N^3 for the McWeeny step (mixed)
+               "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
+               "fp64": fp64, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clocks, "gpu_launches": launches}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -235,15 +235,26 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
     if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
     else { alpha = -1.0; beta = 2.0; }
   }
-  int bi, bj;
-  upper_tile(blockIdx.x, bi, bj);
+  int bi, bj, nloc = p.np, core = p.core;
+  size_t row0 = 0;
+  if (p.tiles) {
+    const int4 t = p.tiles[blockIdx.x];
+    row0 = (size_t)t.x;
+    bi = t.y >> 16;
+    bj = t.y & 0xffff;
+    nloc = t.z;
+    core = t.w;
+  } else {
+    upper_tile(blockIdx.x, bi, bj);
+  }
   const int i0 = bi * BT, j0 = bj * BT;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = warp / WN, wn = warp % WN;
-  const double* __restrict__ A = (const double*)p.A;
-  const double* __restrict__ B = (const double*)p.B;
-  const int np = p.np;
+  const int ld = p.ld;
+  // the part's square block starts at row row0 of the packed buffers
+  const double* __restrict__ A = (const double*)p.A + row0 * ld;
+  const double* __restrict__ B = (const double*)p.B + row0 * ld;
 
   double acc[C::MI][C::NI][2];
 #pragma unroll
@@ -251,15 +262,15 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
 #pragma unroll
     for (int ni = 0; ni < C::NI; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
 
-  const int KB = np / C::BK;
+  const int KB = nloc / C::BK;
   auto load = [&](int stage, int kb) {
     double* As = sm + stage * 2 * C::BK * C::LDS;
     double* Bs = As + C::BK * C::LDS;
     const int k0 = kb * C::BK;
     for (int c = tid; c < C::BK * BT / 2; c += C::NT) {
       const int row = c / (BT / 2), col = (c % (BT / 2)) * 2;
-      cp_async16(As + row * C::LDS + col, A + (size_t)(k0 + row) * np + i0 + col);
-      cp_async16(Bs + row * C::LDS + col, B + (size_t)(k0 + row) * np + j0 + col);
+      cp_async16(As + row * C::LDS + col, A + (size_t)(k0 + row) * ld + i0 + col);
+      cp_async16(Bs + row * C::LDS + col, B + (size_t)(k0 + row) * ld + j0 + col);
     }
   };
 #pragma unroll
@@ -294,8 +305,8 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
 
   // ---- epilogue: out = alpha*acc + beta*E, mirrored store, FP64 sums ----
   const bool diag = (bi == bj);
-  const double* __restrict__ E = (const double*)p.E;
-  double* __restrict__ out = (double*)p.out;
+  const double* __restrict__ E = (const double*)p.E + row0 * ld;
+  double* __restrict__ out = p.out ? (double*)p.out + row0 * ld : nullptr;
   double s[4] = {0.0, 0.0, 0.0, 0.0};  // ||out||^2, Tr out, ||E-acc||^2 (core rows), Tr acc
 #pragma unroll
   for (int mi = 0; mi < C::MI; ++mi) {
@@ -303,24 +314,24 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
     for (int ni = 0; ni < C::NI; ++ni) {
       const int r = i0 + wm * C::TM + mi * 8 + g;
       const int c = j0 + wn * C::TN + ni * 8 + 2 * t4;
-      const double2 e = *reinterpret_cast<const double2*>(E + (size_t)r * np + c);
+      const double2 e = *reinterpret_cast<const double2*>(E + (size_t)r * ld + c);
       const double a0 = acc[mi][ni][0], a1 = acc[mi][ni][1];
       const double v0 = alpha * a0 + beta * e.x;
       const double v1 = alpha * a1 + beta * e.y;
       const int w0 = sym_weight(diag, r, c), w1 = sym_weight(diag, r, c + 1);
       const double d0 = e.x - a0, d1 = e.y - a1;
       s[0] += w0 * v0 * v0 + w1 * v1 * v1;
-      s[2] += core_weight(w0, r, c, p.core) * d0 * d0 + core_weight(w1, r, c + 1, p.core) * d1 * d1;
+      s[2] += core_weight(w0, r, c, core) * d0 * d0 + core_weight(w1, r, c + 1, core) * d1 * d1;
       if (r == c) { s[1] += v0; s[3] += a0; }
       if (r == c + 1) { s[1] += v1; s[3] += a1; }
       if (out) {
         if (!diag) {
-          *reinterpret_cast<double2*>(out + (size_t)r * np + c) = make_double2(v0, v1);
-          out[(size_t)c * np + r] = v0;
-          out[(size_t)(c + 1) * np + r] = v1;
+          *reinterpret_cast<double2*>(out + (size_t)r * ld + c) = make_double2(v0, v1);
+          out[(size_t)c * ld + r] = v0;
+          out[(size_t)(c + 1) * ld + r] = v1;
         } else {
-          if (w0) { out[(size_t)r * np + c] = v0; out[(size_t)c * np + r] = v0; }
-          if (w1) { out[(size_t)r * np + c + 1] = v1; out[(size_t)(c + 1) * np + r] = v1; }
+          if (w0) { out[(size_t)r * ld + c] = v0; out[(size_t)c * ld + r] = v0; }
+          if (w1) { out[(size_t)r * ld + c + 1] = v1; out[(size_t)(c + 1) * ld + r] = v1; }
         }
       }
     }
@@ -338,24 +349,34 @@ int f64_ntiles(int np) {
   return t * (t + 1) / 2;
 }
 
-cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st) {
-  const int bt = f64_tile(a.np);
-  const int t = a.np / bt;
-  const int ntiles = t * (t + 1) / 2;
+static cudaError_t launch_f64_bt(const StepArgs& a, int bt, int ntiles, cudaStream_t st) {
   if (bt == 128) {
     using C = F64Cfg<128, 2, 4>;
     auto kern = k_sym_gemm_f64<128, 2, 4>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
-    note_launch();
   } else {
     using C = F64Cfg<64, 2, 2>;
     auto kern = k_sym_gemm_f64<64, 2, 2>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
-    note_launch();
   }
+  note_launch();
   return cudaGetLastError();
+}
+
+cudaError_t launch_sym_gemm_f64(const StepArgs& a0, cudaStream_t st) {
+  StepArgs a = a0;
+  a.tiles = nullptr;
+  if (a.ld == 0) a.ld = a.np;
+  const int bt = f64_tile(a.np);
+  const int t = a.np / bt;
+  return launch_f64_bt(a, bt, t * (t + 1) / 2, st);
+}
+
+cudaError_t launch_sym_gemm_f64_batched(const StepArgs& a, int bt, cudaStream_t st) {
+  if (!a.tiles || a.ntiles <= 0 || (bt != 64 && bt != 128)) return cudaErrorInvalidValue;
+  return launch_f64_bt(a, bt, a.ntiles, st);
 }
 
 }  // namespace sp2b

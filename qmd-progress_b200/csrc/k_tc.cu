@@ -176,10 +176,22 @@ __global__ void __launch_bounds__(128, 1)
     if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
     else { alpha = -1.0; beta = 2.0; }
   }
-  int bi, bj;
-  if (SYM) upper_tile(blockIdx.x, bi, bj);
-  else { bi = blockIdx.y; bj = blockIdx.x; }
+  int bi, bj, nloc = p.np, core = p.core, row0 = 0;
+  if (SYM && p.tiles) {
+    const int4 t = p.tiles[blockIdx.x];
+    row0 = t.x;
+    bi = t.y >> 16;
+    bj = t.y & 0xffff;
+    nloc = t.z;
+    core = t.w;
+  } else if (SYM) {
+    upper_tile(blockIdx.x, bi, bj);
+  } else {
+    bi = blockIdx.y;
+    bj = blockIdx.x;
+  }
   const int i0 = bi * tc::BM, j0 = bj * tc::BN;
+  const int ld = p.ld;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -200,7 +212,7 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
-  const int KB = p.np / tc::BK;
+  const int KB = nloc / tc::BK;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -215,10 +227,10 @@ __global__ void __launch_bounds__(128, 1)
         const uint32_t fb = smem_u32(&bar_full[s]);
         const uint32_t st = sbase + s * tc::STAGE_BYTES;
         mbar_expect_tx(fb, tc::STAGE_BYTES);
-        tma_load_2d(st + 0 * tc::TILE_BYTES, &tm_ahi, fb, kb * tc::BK, i0);
-        tma_load_2d(st + 1 * tc::TILE_BYTES, &tm_alo, fb, kb * tc::BK, i0);
-        tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_bhi, fb, kb * tc::BK, j0);
-        tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_blo, fb, kb * tc::BK, j0);
+        tma_load_2d(st + 0 * tc::TILE_BYTES, &tm_ahi, fb, kb * tc::BK, row0 + i0);
+        tma_load_2d(st + 1 * tc::TILE_BYTES, &tm_alo, fb, kb * tc::BK, row0 + i0);
+        tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_bhi, fb, kb * tc::BK, row0 + j0);
+        tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_blo, fb, kb * tc::BK, row0 + j0);
         issued_phase[s] = u & 1;
       }
       if (!ok) {
@@ -271,13 +283,13 @@ __global__ void __launch_bounds__(128, 1)
   if (good) {
     const int rl = warp * 32 + lane;
     const int r = i0 + rl;
-    const int np = p.np;
     const bool diag = SYM && (bi == bj);
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    const T* Ehi = (const T*)p.E;
-    const T* Elo = (const T*)p.E_lo;
-    T* Ohi = (T*)p.out;
-    T* Olo = (T*)p.out_lo;
+    const size_t base = (size_t)row0 * ld;  // the part's block inside the packed buffers
+    const T* Ehi = SYM ? (const T*)p.E + base : nullptr;
+    const T* Elo = SYM ? (const T*)p.E_lo + base : nullptr;
+    T* Ohi = (SYM && p.out) ? (T*)p.out + base : nullptr;
+    T* Olo = (SYM && p.out) ? (T*)p.out_lo + base : nullptr;
 #pragma unroll 1
     for (int cc = 0; cc < tc::BN / 32; ++cc) {
       uint32_t hh[32], xx[32];
@@ -298,8 +310,8 @@ __global__ void __launch_bounds__(128, 1)
       }
       alignas(16) T ehi[32], elo[32], nhi[32], nlo[32];
       {
-        const uint4* src_h = reinterpret_cast<const uint4*>(Ehi + (size_t)r * np + c0);
-        const uint4* src_l = reinterpret_cast<const uint4*>(Elo + (size_t)r * np + c0);
+        const uint4* src_h = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0);
+        const uint4* src_l = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0);
         uint4* dh = reinterpret_cast<uint4*>(ehi);
         uint4* dl = reinterpret_cast<uint4*>(elo);
 #pragma unroll
@@ -319,17 +331,17 @@ __global__ void __launch_bounds__(128, 1)
         const int w = sym_weight(diag, r, c);
         const double dres = x - P;
         sums[0] += w * vs * vs;
-        sums[2] += core_weight(w, r, c, p.core) * dres * dres;
+        sums[2] += core_weight(w, r, c, core) * dres * dres;
         if (r == c) { sums[1] += vs; sums[3] += P; }
         if (Ohi && w && r != c) {
-          Ohi[(size_t)c * np + r] = h;
-          Olo[(size_t)c * np + r] = l;
+          Ohi[(size_t)c * ld + r] = h;
+          Olo[(size_t)c * ld + r] = l;
         }
       }
       if (Ohi) {
         if (!diag) {
-          uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * np + c0);
-          uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * np + c0);
+          uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * ld + c0);
+          uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * ld + c0);
           const uint4* sh = reinterpret_cast<const uint4*>(nhi);
           const uint4* sl = reinterpret_cast<const uint4*>(nlo);
 #pragma unroll
@@ -337,8 +349,8 @@ __global__ void __launch_bounds__(128, 1)
         } else {
           for (int j = 0; j < 32; ++j)
             if (r <= c0 + j) {
-              Ohi[(size_t)r * np + c0 + j] = nhi[j];
-              Olo[(size_t)r * np + c0 + j] = nlo[j];
+              Ohi[(size_t)r * ld + c0 + j] = nhi[j];
+              Olo[(size_t)r * ld + c0 + j] = nlo[j];
             }
         }
       }
@@ -484,14 +496,14 @@ int tc_ntiles(int np) {
 }
 
 template <typename T, bool SYM>
-static cudaError_t launch_tc(const StepArgs& a, dim3 grid, float* plain_out, int plain_n,
-                             cudaStream_t st) {
+static cudaError_t launch_tc(const StepArgs& a, long long rows, dim3 grid, float* plain_out,
+                             int plain_n, cudaStream_t st) {
   const bool bf16 = std::is_same<T, __nv_bfloat16>::value;
   CUtensorMap m[4];
-  if (!make_tmap(&m[0], a.A, a.np, a.np, a.np, bf16) ||
-      !make_tmap(&m[1], a.A_lo, a.np, a.np, a.np, bf16) ||
-      !make_tmap(&m[2], a.B, a.np, a.np, a.np, bf16) ||
-      !make_tmap(&m[3], a.B_lo, a.np, a.np, a.np, bf16))
+  if (!make_tmap(&m[0], a.A, rows, a.ld, a.ld, bf16) ||
+      !make_tmap(&m[1], a.A_lo, rows, a.ld, a.ld, bf16) ||
+      !make_tmap(&m[2], a.B, rows, a.ld, a.ld, bf16) ||
+      !make_tmap(&m[3], a.B_lo, rows, a.ld, a.ld, bf16))
     return cudaErrorInvalidValue;
   auto kern = k_tc_gemm<T, SYM>;
   cudaError_t e =
@@ -502,11 +514,23 @@ static cudaError_t launch_tc(const StepArgs& a, dim3 grid, float* plain_out, int
   return cudaGetLastError();
 }
 
-cudaError_t launch_sym_gemm_tc(const StepArgs& a, int bf16, cudaStream_t st) {
-  if (a.np % tc::BM != 0) return cudaErrorInvalidValue;
+cudaError_t launch_sym_gemm_tc(const StepArgs& a0, int bf16, cudaStream_t st) {
+  if (a0.np % tc::BM != 0) return cudaErrorInvalidValue;
+  StepArgs a = a0;
+  a.tiles = nullptr;
+  a.ld = a.np;
   dim3 grid(tc_ntiles(a.np));
-  return bf16 ? launch_tc<__nv_bfloat16, true>(a, grid, nullptr, 0, st)
-              : launch_tc<__half, true>(a, grid, nullptr, 0, st);
+  return bf16 ? launch_tc<__nv_bfloat16, true>(a, a.np, grid, nullptr, 0, st)
+              : launch_tc<__half, true>(a, a.np, grid, nullptr, 0, st);
+}
+
+cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,
+                                       cudaStream_t st) {
+  if (!a.tiles || a.ntiles <= 0 || a.ld % tc::BM != 0 || rows % tc::BM != 0)
+    return cudaErrorInvalidValue;
+  dim3 grid(a.ntiles);
+  return bf16 ? launch_tc<__nv_bfloat16, true>(a, rows, grid, nullptr, 0, st)
+              : launch_tc<__half, true>(a, rows, grid, nullptr, 0, st);
 }
 
 cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,
@@ -519,9 +543,10 @@ cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* 
   a.B = bhi;
   a.B_lo = blo;
   a.np = np;
+  a.ld = np;
   a.err = err;
   dim3 grid(np / tc::BN, np / tc::BM);
-  return launch_tc<__half, false>(a, grid, c, n, st);
+  return launch_tc<__half, false>(a, np, grid, c, n, st);
 }
 
 static int ew_grid(size_t total) {

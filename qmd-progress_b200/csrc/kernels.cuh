@@ -28,8 +28,12 @@ struct StepArgs {
   void* out;            // nullptr: sums only
   const void* E_lo;     // split mode: lo half of E
   void* out_lo;         // split mode: lo half of out
-  int np;               // padded dimension (= leading dimension)
+  int np;               // padded dimension of a dense solve
+  int ld;               // row pitch of A/B/E/out (dense: np; batched parts: max padded size)
   int ntiles;
+  // Batched parts (tiles != nullptr): CTA b works on tile tiles[b] =
+  //   {x: first packed row of its part, y: (bi << 16) | bj, z: padded part size, w: core rows}
+  const int4* tiles;
   double alpha, beta;
   int core;             // > 0: residual sums over the first `core` rows only
   // SP2 control (control = 1)
@@ -59,6 +63,7 @@ cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const d
                                  double* x, double* partials, unsigned* counter, SP2Rec* rec0,
                                  double* norm_out, cudaStream_t st);
 cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st);
+cudaError_t launch_sym_gemm_f64_batched(const StepArgs& a, int bt, cudaStream_t st);
 cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, double* rho,
                               int ld, cudaStream_t st);
 cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,
@@ -71,6 +76,9 @@ cudaError_t launch_normalize_split(const double* h, int n, int ld, int np,
                                    double* partials, unsigned* counter, SP2Rec* rec0,
                                    double* norm_out, cudaStream_t st);
 cudaError_t launch_sym_gemm_tc(const StepArgs& a, int bf16, cudaStream_t st);
+// batched parts: A/B tensors are rows x ld packed buffers
+cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,
+                                       cudaStream_t st);
 cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int bf16,
                                 double* x, cudaStream_t st);
 cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,

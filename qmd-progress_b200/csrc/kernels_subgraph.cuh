@@ -1,0 +1,29 @@
+// Launch interfaces of the graph-partitioned SP2 path.
+#pragma once
+#include "kernels.cuh"
+
+namespace sp2b {
+
+// One core+halo part inside the packed buffers.
+struct PartDesc {
+  long long row0;   // first packed row
+  long long hoff;   // offset of its node list in the halo / sorted arrays
+  long long coff;   // offset of its ncore x n block in the packed core-row output
+  int n;            // core+halo size (lsize)
+  int np;           // n padded to 128
+  int ncore;        // core size (llsize)
+  int pad_;
+};
+
+cudaError_t launch_extract_csr(const long long* rp, const int* col, const double* val,
+                               const PartDesc* parts, int nparts, const int* halo,
+                               const int* skey, const int* sval, int ld, double* xs,
+                               cudaStream_t st);
+cudaError_t launch_norm_parts(double* xs, const int* row_part, const PartDesc* parts,
+                              long long rows, int ld, double emin, double emax, int prec,
+                              void* hi, void* lo, cudaStream_t st);
+cudaError_t launch_scatter_parts(const double* x64, const void* hi, const void* lo, int prec,
+                                 const PartDesc* parts, int nparts, const int* halo, int ld,
+                                 double* core_out, double* dense, long long n, cudaStream_t st);
+
+}  // namespace sp2b

@@ -1,0 +1,337 @@
+// Host side of the graph-partitioned SP2 path: prg_subgraphSP2Loop
+// (src/prg_subgraphloop_mod.F90:36-126) as one batched GPU solve.
+//
+// All parts share the branch sequence pp(1:maxIter) and the global bounds
+// (src/prg_subgraphloop_mod.F90:104-106), so every part advances in lock step: one
+// launch per SP2 iteration covers the upper tiles of every part (a ragged batch,
+// largest parts first), and the whole sequence normalise -> maxIter steps -> scatter
+// is captured once into a CUDA graph and replayed as one graph launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "kernels_subgraph.cuh"
+#include "sp2b_ctx.h"
+
+namespace sp2b {
+
+template <typename T>
+static cudaError_t grow_buf(T*& p, size_t& cap, size_t need) {
+  if (need <= cap && p) return cudaSuccess;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(need, 1) * sizeof(T));
+  if (e == cudaSuccess) cap = std::max<size_t>(need, 1);
+  return e;
+}
+
+struct SubBufs {
+  double* xs = nullptr;          size_t xs_cap = 0;     // FP64 packed (H_sub / FP64 iterate)
+  double* x2 = nullptr;          size_t x2_cap = 0;     // FP64 ping-pong partner
+  __half* hi[2] = {};            size_t hi_cap[2] = {};
+  __half* lo[2] = {};            size_t lo_cap[2] = {};
+  PartDesc* parts = nullptr;     size_t parts_cap = 0;
+  int4* tiles = nullptr;         size_t tiles_cap = 0;
+  int* row_part = nullptr;       size_t row_part_cap = 0;
+  int* halo = nullptr;           size_t halo_cap = 0;
+  int* skey = nullptr;           size_t skey_cap = 0;
+  int* sval = nullptr;           size_t sval_cap = 0;
+  long long* rp = nullptr;       size_t rp_cap = 0;
+  int* col = nullptr;            size_t col_cap = 0;
+  double* val = nullptr;         size_t val_cap = 0;
+  double* core = nullptr;        size_t core_cap = 0;
+  double* dense = nullptr;       size_t dense_cap = 0;
+  double* partials = nullptr;    size_t partials_cap = 0;
+  SP2Rec* rec = nullptr;         size_t rec_cap = 0;
+  int* pp = nullptr;             size_t pp_cap = 0;
+  double* vv = nullptr;          size_t vv_cap = 0;
+};
+static SubBufs g_sub[64];
+
+}  // namespace sp2b
+
+using namespace sp2b;
+
+extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
+                                      const double* h_val, int nparts, const long long* halo_ptr,
+                                      const int* halo_idx, const int* llsize, const int* pp,
+                                      int maxiter, double mineval, double maxeval,
+                                      double* rho_core, double* rho_dense, double* vv,
+                                      const sp2b_opts* opts) {
+  if (n <= 0 || nparts <= 0 || !h_row_ptr || !h_col || !h_val || !halo_ptr || !halo_idx ||
+      !llsize || maxiter < 0 || (maxiter > 0 && !pp) || !(maxeval - mineval > 0.0)) {
+    set_last_error("sp2b_subgraph_sp2_loop: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  sp2b_opts dflt;
+  sp2b_opts_default(&dflt);
+  dflt.precision = SP2B_PREC_MIXED_FP16;
+  if (!opts) opts = &dflt;
+  const int prec = opts->precision;
+  const bool dev = opts->device_ptrs != 0;
+  const bool split = prec != SP2B_PREC_FP64;
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  SubBufs& b = g_sub[c->dev];
+  cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : c->stream;
+
+  // ---- host-side layout (index lists are small; device inputs are fetched) ----
+  std::vector<long long> hp(nparts + 1);
+  std::vector<int> lls(nparts);
+  if (dev) {
+    SP2B_CUDA_TRY(cudaMemcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    SP2B_CUDA_TRY(cudaMemcpy(lls.data(), llsize, nparts * sizeof(int), cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long));
+    std::memcpy(lls.data(), llsize, nparts * sizeof(int));
+  }
+  const long long nhalo = hp[nparts];
+  std::vector<int> hidx(nhalo);
+  if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
+  else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
+
+  std::vector<PartDesc> P(nparts);
+  int ld = 0;
+  long long rows = 0, coff = 0;
+  for (int p = 0; p < nparts; ++p) {
+    const long long sz = hp[p + 1] - hp[p];
+    if (sz <= 0 || sz > 32768 || lls[p] < 0 || lls[p] > sz) {
+      set_last_error("part %d: bad sizes (lsize=%lld llsize=%d)", p, sz, lls[p]);
+      return SP2B_BAD_ARG;
+    }
+    PartDesc& d = P[p];
+    d.n = (int)sz;
+    d.np = padded(d.n);
+    d.ncore = lls[p];
+    d.hoff = hp[p];
+    d.row0 = rows;
+    d.coff = coff;
+    d.pad_ = 0;
+    rows += d.np;
+    coff += (long long)d.ncore * d.n;
+    ld = std::max(ld, d.np);
+  }
+  for (long long q = 0; q < nhalo; ++q)
+    if (hidx[q] < 0 || hidx[q] >= n) {
+      set_last_error("halo index out of range at %lld", q);
+      return SP2B_BAD_ARG;
+    }
+  // sorted node lists per part for the CSR column lookup
+  std::vector<int> skey(nhalo), sval(nhalo);
+  {
+    std::vector<int> ord;
+    for (int p = 0; p < nparts; ++p) {
+      const int m = P[p].n;
+      ord.resize(m);
+      std::iota(ord.begin(), ord.end(), 0);
+      const int* h = hidx.data() + P[p].hoff;
+      std::sort(ord.begin(), ord.end(), [h](int a, int b2) { return h[a] < h[b2]; });
+      for (int i = 0; i < m; ++i) {
+        skey[P[p].hoff + i] = h[ord[i]];
+        sval[P[p].hoff + i] = ord[i];
+      }
+    }
+  }
+  // row -> part map
+  std::vector<int> row_part(rows);
+  for (int p = 0; p < nparts; ++p)
+    std::fill(row_part.begin() + P[p].row0, row_part.begin() + P[p].row0 + P[p].np, p);
+  // tile list, most expensive parts first (cost of a tile ~ np)
+  const int bt = split ? 128 : 64;
+  std::vector<int> order(nparts);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return P[a].np > P[b2].np; });
+  std::vector<int4> tiles;
+  for (int p : order) {
+    const int T = P[p].np / bt;
+    for (int bj = 0; bj < T; ++bj)
+      for (int bi = 0; bi <= bj; ++bi)
+        tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj, P[p].np,
+                                  P[p].ncore > 0 ? P[p].ncore : -1));
+  }
+  if (rows > 0x7fffffffLL) {
+    set_last_error("packed parts exceed 2^31 rows");
+    return SP2B_BAD_ARG;
+  }
+  const int ntiles = (int)tiles.size();
+
+  // ---- device buffers ----
+  long long nnz;
+  if (dev) SP2B_CUDA_TRY(cudaMemcpy(&nnz, h_row_ptr + n, sizeof(long long), cudaMemcpyDeviceToHost));
+  else nnz = h_row_ptr[n];
+  const size_t packed = (size_t)rows * ld;
+  SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
+  if (split) {
+    for (int i = 0; i < 2; ++i) {
+      SP2B_CUDA_TRY(grow_buf(b.hi[i], b.hi_cap[i], packed));
+      SP2B_CUDA_TRY(grow_buf(b.lo[i], b.lo_cap[i], packed));
+    }
+  } else {
+    SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
+  }
+  SP2B_CUDA_TRY(grow_buf(b.parts, b.parts_cap, nparts));
+  SP2B_CUDA_TRY(grow_buf(b.tiles, b.tiles_cap, ntiles));
+  SP2B_CUDA_TRY(grow_buf(b.row_part, b.row_part_cap, rows));
+  SP2B_CUDA_TRY(grow_buf(b.halo, b.halo_cap, nhalo));
+  SP2B_CUDA_TRY(grow_buf(b.skey, b.skey_cap, nhalo));
+  SP2B_CUDA_TRY(grow_buf(b.sval, b.sval_cap, nhalo));
+  SP2B_CUDA_TRY(grow_buf(b.partials, b.partials_cap, 4 * (size_t)ntiles));
+  SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
+  SP2B_CUDA_TRY(grow_buf(b.pp, b.pp_cap, (size_t)maxiter + 1));
+  SP2B_CUDA_TRY(grow_buf(b.vv, b.vv_cap, (size_t)maxiter + 1));
+  const long long* rp_d = h_row_ptr;
+  const int* col_d = h_col;
+  const double* val_d = h_val;
+  if (!dev) {
+    SP2B_CUDA_TRY(grow_buf(b.rp, b.rp_cap, (size_t)n + 1));
+    SP2B_CUDA_TRY(grow_buf(b.col, b.col_cap, (size_t)nnz));
+    SP2B_CUDA_TRY(grow_buf(b.val, b.val_cap, (size_t)nnz));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.rp, h_row_ptr, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.col, h_col, nnz * sizeof(int), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.val, h_val, nnz * sizeof(double), cudaMemcpyHostToDevice, st));
+    rp_d = b.rp;
+    col_d = b.col;
+    val_d = b.val;
+  }
+  double* core_d = rho_core;
+  double* dense_d = rho_dense;
+  if (!dev) {
+    if (rho_core) {
+      SP2B_CUDA_TRY(grow_buf(b.core, b.core_cap, (size_t)coff));
+      core_d = b.core;
+    }
+    if (rho_dense) {
+      SP2B_CUDA_TRY(grow_buf(b.dense, b.dense_cap, (size_t)n * n));
+      dense_d = b.dense;
+    }
+  }
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.parts, P.data(), nparts * sizeof(PartDesc), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.tiles, tiles.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.row_part, row_part.data(), rows * sizeof(int), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.halo, hidx.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.skey, skey.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.sval, sval.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (maxiter > 0)
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, pp, maxiter * sizeof(int),
+                                  dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));  // host staging vectors go out of scope below
+
+  // ---- the batched solve, captured once into a graph ----
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.ld = ld;
+  a.np = ld;
+  a.ntiles = ntiles;
+  a.tiles = b.tiles;
+  a.control = 1;
+  a.ctl.algo = ALGO_SEQ;
+  a.ctl.icount = maxiter;
+  a.ctl.n = n;
+  a.rec = b.rec;
+  a.pp_in = b.pp;
+  a.pp_out = nullptr;
+  a.vv_out = b.vv;
+  a.vv_accumulate = 1;
+  a.sout = c->sout;
+  a.partials = b.partials;
+  a.counter = c->counter;
+  a.err = c->err;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  SP2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  auto body = [&]() -> cudaError_t {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(b.rec, 0, sizeof(SP2Rec), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(b.vv, 0, ((size_t)maxiter + 1) * sizeof(double), st)) != cudaSuccess) return e;
+    if (rho_dense && (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), st)) != cudaSuccess)
+      return e;
+    if ((e = launch_extract_csr(rp_d, col_d, val_d, b.parts, nparts, b.halo, b.skey, b.sval, ld,
+                                b.xs, st)) != cudaSuccess)
+      return e;
+    if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, mineval, maxeval, prec,
+                               split ? (void*)b.hi[0] : nullptr, split ? (void*)b.lo[0] : nullptr,
+                               st)) != cudaSuccess)
+      return e;
+    for (int k = 0; k < maxiter; ++k) {
+      a.k = k;
+      const int bin = k & 1, bout = (k + 1) & 1;
+      if (split) {
+        a.A = a.B = a.E = b.hi[bin];
+        a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
+        a.out = b.hi[bout];
+        a.out_lo = b.lo[bout];
+        e = launch_sym_gemm_tc_batched(a, rows, prec == SP2B_PREC_MIXED_BF16, st);
+      } else {
+        double* xin = bin ? b.x2 : b.xs;
+        double* xout = bout ? b.x2 : b.xs;
+        a.A = a.B = a.E = xin;
+        a.out = xout;
+        e = launch_sym_gemm_f64_batched(a, bt, st);
+      }
+      if (e != cudaSuccess) return e;
+    }
+    const int fb = maxiter & 1;
+    return launch_scatter_parts(fb ? b.x2 : b.xs, split ? (void*)b.hi[fb] : nullptr,
+                                split ? (void*)b.lo[fb] : nullptr, prec, b.parts, nparts, b.halo,
+                                ld, core_d, rho_dense ? dense_d : nullptr, n, st);
+  };
+  const cudaError_t be = body();
+  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  if (be != cudaSuccess || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    set_last_error("graph capture failed: %s / %s", cudaGetErrorString(be), cudaGetErrorString(ce));
+    return SP2B_CUDA_ERROR;
+  }
+  cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    set_last_error("graph instantiate failed: %s", cudaGetErrorString(ie));
+    return SP2B_CUDA_ERROR;
+  }
+  cudaError_t le = cudaGraphLaunch(exec, st);
+  if (le == cudaSuccess) le = cudaStreamSynchronize(st);
+  cudaGraphExecDestroy(exec);
+  note_launch(0);
+  if (le != cudaSuccess) {
+    set_last_error("graph launch failed: %s", cudaGetErrorString(le));
+    return SP2B_CUDA_ERROR;
+  }
+
+  // ---- outputs ----
+  std::vector<double> vvh(maxiter + 1, 0.0);
+  if (maxiter > 0)
+    SP2B_CUDA_TRY(cudaMemcpy(vvh.data(), b.vv, maxiter * sizeof(double), cudaMemcpyDeviceToHost));
+  int herr = 0;
+  SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (vv) {
+    for (int k = 0; k < maxiter; ++k) vvh[k] = std::sqrt(vvh[k]);  // prg_fnormGraph
+    if (dev) SP2B_CUDA_TRY(cudaMemcpy(vv, vvh.data(), maxiter * sizeof(double), cudaMemcpyHostToDevice));
+    else std::memcpy(vv, vvh.data(), maxiter * sizeof(double));
+  }
+  if (!dev) {
+    if (rho_core)
+      SP2B_CUDA_TRY(cudaMemcpy(rho_core, b.core, coff * sizeof(double), cudaMemcpyDeviceToHost));
+    if (rho_dense)
+      SP2B_CUDA_TRY(cudaMemcpy(rho_dense, b.dense, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  if (herr) {
+    set_last_error("a device-side wait timed out");
+    return SP2B_TIMEOUT;
+  }
+  for (int k = 0; k < maxiter; ++k)
+    if (!(vvh[k] == vvh[k])) {
+      set_last_error("non-finite values during sub-graph SP2");
+      return SP2B_BAD_INPUT;
+    }
+  return SP2B_OK;
+}

@@ -240,3 +240,75 @@ def equal_partition(nodes_per_part, nnodes):
     check(lib().sp2b_equal_partition(nodes_per_part, nnodes, C.byref(npart), _ptr(ptr), _ptr(nodes)),
           "equal_partition")
     return [nodes[ptr[i]:ptr[i + 1]].copy() for i in range(npart.value)]
+
+
+# ----------------------------------------------------------------------------------
+# Graph-partitioned SP2 (prg_subgraphSP2Loop, src/prg_subgraphloop_mod.F90:36-126)
+# ----------------------------------------------------------------------------------
+
+def dense_to_csr(a):
+    """CSR (row_ptr int64, col int32, val float64) of the nonzeros of a dense matrix."""
+    a = np.asarray(a)
+    r, c = np.nonzero(a)
+    rp = np.zeros(a.shape[0] + 1, dtype=np.int64)
+    np.add.at(rp, r + 1, 1)
+    return np.cumsum(rp), c.astype(np.int32), np.ascontiguousarray(a[r, c], dtype=np.float64)
+
+
+def subgraph_halos(n, g_csr, parts, h_csr=None, double_jump=True):
+    """Core+halo node lists (bml_matrix2submatrix_index at src/prg_subgraphloop_mod.F90:60).
+
+    Returns (halo_ptr int64 [nparts+1], halo_idx int32, lsize, llsize)."""
+    grp, gcol = np.ascontiguousarray(g_csr[0], np.int64), np.ascontiguousarray(g_csr[1], np.int32)
+    if h_csr is not None:
+        hrp, hcol = np.ascontiguousarray(h_csr[0], np.int64), np.ascontiguousarray(h_csr[1], np.int32)
+        hp_, hc_ = _ptr(hrp), _ptr(hcol)
+    else:
+        hp_, hc_ = None, None
+    nparts = len(parts)
+    pptr = np.zeros(nparts + 1, dtype=np.int32)
+    pptr[1:] = np.cumsum([len(p) for p in parts])
+    pn = np.ascontiguousarray(np.concatenate(parts), dtype=np.int32)
+    halo_ptr = np.zeros(nparts + 1, dtype=np.int64)
+    ls = np.zeros(nparts, dtype=np.int32)
+    lls = np.zeros(nparts, dtype=np.int32)
+    need = C.c_longlong(0)
+    cap = max(1, 4 * int(pptr[-1]))
+    while True:
+        idx = np.zeros(cap, dtype=np.int32)
+        st = lib().sp2b_subgraph_halos(n, _ptr(grp), _ptr(gcol), hp_, hc_, nparts, _ptr(pptr), _ptr(pn),
+                                       1 if double_jump else 0, _ptr(halo_ptr), _ptr(idx), cap,
+                                       C.byref(need), _ptr(ls), _ptr(lls))
+        if st == _lib.SP2B_OK:
+            return halo_ptr, idx[:need.value].copy(), ls, lls
+        if st == _lib.SP2B_BAD_ARG and need.value > cap:
+            cap = int(need.value)
+            continue
+        check(st, "subgraph_halos")
+
+
+def subgraph_sp2_loop(n, h_csr, halo_ptr, halo_idx, llsize, pp, maxiter, mineval, maxeval,
+                      precision=PREC_MIXED_FP16, dense=True, core=False):
+    """prg_subgraphSP2Loop: returns (rho_dense [n x n] or None, rho_core or None, vv).
+
+    rho_dense holds the core rows of every part (rest zero), indexed rho[i, j]; vv is
+    the per-iteration Frobenius norm over all parts' core rows (after prg_fnormGraph)."""
+    rp = np.ascontiguousarray(h_csr[0], np.int64)
+    col = np.ascontiguousarray(h_csr[1], np.int32)
+    val = np.ascontiguousarray(h_csr[2], np.float64)
+    hptr = np.ascontiguousarray(halo_ptr, np.int64)
+    hidx = np.ascontiguousarray(halo_idx, np.int32)
+    lls = np.ascontiguousarray(llsize, np.int32)
+    pp_a = np.ascontiguousarray(pp, np.int32) if maxiter > 0 else np.zeros(1, np.int32)
+    nparts = len(lls)
+    ls = np.diff(hptr)
+    rho_dense = np.zeros((n, n), order="F") if dense else None
+    rho_core = np.zeros(int(np.sum(lls.astype(np.int64) * ls))) if core else None
+    vv = np.zeros(max(maxiter, 1))
+    o = make_opts(precision=precision)
+    check(lib().sp2b_subgraph_sp2_loop(n, _ptr(rp), _ptr(col), _ptr(val), nparts, _ptr(hptr), _ptr(hidx),
+                                       _ptr(lls), _ptr(pp_a), maxiter, mineval, maxeval,
+                                       _ptr(rho_core) if core else None,
+                                       rho_dense.ctypes.data_as(C.c_void_p) if dense else None,
+                                       _ptr(vv), C.byref(o)), "subgraph_sp2_loop")
+    return rho_dense, rho_core, vv[:maxiter]

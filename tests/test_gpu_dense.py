@@ -27,8 +27,9 @@ def rel(a, b):
 @pytest.mark.parametrize("n", [2, 7, 33, 130, 256, 1024])
 def test_alg2_genseq_fp64_parity(cuda, n):
     h = M.two_band_1d(n, seed=n)
-    ref = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
-    got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    bndfil = (n // 2) / n          # integer occupancy (odd n included)
+    ref = O.sp2_alg2_genseq(h, bndfil, 0, 100, "None", 1e-10)
+    got = sp2b.sp2_alg2_genseq(h, bndfil, 0, 100, "None", 1e-10)
     assert got.pp == ref.pp
     assert got.icount == ref.icount
     assert rel(got.rho, ref.rho) <= FP64_TOL

@@ -1,0 +1,101 @@
+"""Graph-partitioned SP2 (prg_subgraphSP2Loop) on the GPU against the CPU oracle.
+
+FP64 batch: the core rows of every part match the oracle to 1e-10 and vv (after
+prg_fnormGraph) to 1e-9.  Mixed batch (FP16 hi+lo tcgen05): within 1e-6 per element.
+On poly.512.mtx with the reference test's settings (48 nodes per part, graph = rho
+thresholded at 1e-3, tests/src/main.F90:847-882) the result matches the recorded
+oracle output and passes the reference criterion (idempotency of rho/2 <= 1e-2).
+"""
+import numpy as np
+import pytest
+
+import sp2_oracle as O
+import sp2b
+from sp2b import modelham as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(n=240, per=40, seed=3):
+    h = M.two_band_1d(n, seed=seed)
+    g = (np.abs(h) > 0).astype(float)
+    parts = O.equal_partition(per, n)
+    emin, emax = O.gershgorin(h)
+    gs = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    eh, el, _ = O.homolumogap(gs.vv, gs.icount, gs.pp, emin, emax)
+    pp, maxiter = O.sp2sequence(emin, emax, eh, el, 1e-12)
+    return h, g, parts, emin, emax, pp, maxiter
+
+
+@pytest.mark.parametrize("double_jump", [True, False])
+def test_subgraph_fp64_parity(cuda, double_jump):
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    rho_ref, vv_ref, _ = O.subgraph_sp2_loop(h, g, parts, pp, maxiter, emin, emax, double_jump)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h),
+                                          double_jump)
+    rho, core, vv = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin,
+                                           emax, precision=sp2b.PREC_FP64, core=True)
+    assert np.linalg.norm(rho - rho_ref) / np.linalg.norm(rho_ref) < 1e-10
+    assert np.allclose(vv, O.fnorm_graph(vv_ref, maxiter), rtol=1e-9, atol=1e-12)
+    # packed core-row output agrees with the dense one
+    off = 0
+    for p in range(len(parts)):
+        idx = hi[hp[p]:hp[p + 1]]
+        blk = core[off:off + lls[p] * ls[p]].reshape(lls[p], ls[p])
+        assert np.array_equal(blk, rho[np.ix_(idx[:lls[p]], idx)])
+        off += lls[p] * ls[p]
+
+
+def test_subgraph_zero_iterations_and_ragged(cuda):
+    n = 130
+    h = M.two_band_1d(n, seed=9)
+    g = (np.abs(h) > 0).astype(float)
+    parts = [np.arange(0, 1), np.arange(1, 60), np.arange(60, 130)]   # ragged: 1, 59, 70 cores
+    emin, emax = O.gershgorin(h)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
+    for pp, mi in [([], 0), ([1, 0, 1], 3)]:
+        rho_ref, vv_ref, _ = O.subgraph_sp2_loop(h, g, parts, pp, mi, emin, emax)
+        rho, _, vv = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, mi, emin, emax,
+                                            precision=sp2b.PREC_FP64)
+        assert np.linalg.norm(rho - rho_ref) <= 1e-10 * np.linalg.norm(rho_ref)
+        assert np.allclose(vv, O.fnorm_graph(vv_ref, mi), rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec", [sp2b.PREC_MIXED_FP16, sp2b.PREC_MIXED_BF16])
+def test_subgraph_mixed_close_to_fp64(cuda, prec):
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    rho_ref, vv_ref, _ = O.subgraph_sp2_loop(h, g, parts, pp, maxiter, emin, emax)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
+    rho, _, vv = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin,
+                                        emax, precision=prec)
+    tol = 1e-6 if prec == sp2b.PREC_MIXED_FP16 else 1e-4
+    assert np.linalg.norm(rho - rho_ref) / n <= tol
+    assert np.allclose(vv, O.fnorm_graph(vv_ref, maxiter), rtol=1e-3, atol=tol)
+
+
+def _poly_parts(d):
+    n = int(d["n"])
+    g_csr = (d["g_row_ptr"], d["g_col"])
+    h_csr = sp2b.dense_to_csr(d["h"])
+    parts = O.equal_partition(48, n)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, g_csr, parts, h_csr, True)
+    return n, h_csr, hp, hi, ls, lls
+
+
+@pytest.mark.parametrize("prec", [sp2b.PREC_FP64, sp2b.PREC_MIXED_FP16])
+def test_poly512_subgraph_matches_fixture(cuda, poly512, prec):
+    d = poly512
+    n, h_csr, hp, hi, ls, lls = _poly_parts(d)
+    assert np.array_equal(ls, d["sg_lsize"])
+    rho, _, vv = sp2b.subgraph_sp2_loop(n, h_csr, hp, hi, lls, d["sg_pp"], int(d["sg_maxiter"]),
+                                        float(d["sg_mineval"]), float(d["sg_maxeval"]), precision=prec)
+    cols = d["sample_cols"]
+    atol = 1e-10 if prec == sp2b.PREC_FP64 else 1e-5
+    assert np.allclose(rho[:, cols], d["sg_rho_cols"], rtol=0, atol=atol)
+    assert np.allclose(vv, d["sg_vv"], rtol=1e-8 if prec == sp2b.PREC_FP64 else 1e-3, atol=atol)
+    assert abs(np.trace(rho) - float(d["sg_trace"])) < (1e-8 if prec == sp2b.PREC_FP64 else 1e-2)
+    half = rho / 2
+    idem = np.linalg.norm(half @ half - half)       # prg_check_idempotency of rho/2
+    assert idem <= 1e-2                             # tests/src/main.F90:876-881
