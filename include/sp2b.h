@@ -8,9 +8,11 @@
  * relies on H = H^T and returns an exactly symmetric density matrix.  rho is the
  * spin-summed density, 2x the idempotent projector (src/prg_sp2_mod.F90:375).
  *
- * Pointers are host pointers unless sp2b_opts.device_ptrs = 1, in which case they
- * are device pointers on the current CUDA device and the call is asynchronous on
- * sp2b_opts.stream up to its final status read.
+ * Matrix arguments (H, rho, the CSR arrays and halo lists of the sub-graph call) are
+ * host pointers unless sp2b_opts.device_ptrs = 1, in which case they are device
+ * pointers on the current CUDA device and the work runs on sp2b_opts.stream.  The
+ * short sequence arrays pp, vv and icount are host pointers in every mode.  Calls
+ * return after their results are complete.
  *
  * The PROGRESS-named exports (prg_sp2_alg2, ...) with the reference's exact C
  * signatures are declared in prg_sp2b.h.

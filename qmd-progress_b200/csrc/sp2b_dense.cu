@@ -188,15 +188,11 @@ int dense_solve(const DenseJob& j) {
                                        c->rec, norm_out, st));
 
   // ---- control inputs ----
-  if (j.ctl.algo == ALGO_SEQ && j.ctl.icount > 0) {
-    if (j.dev_ptrs)
-      SP2B_CUDA_TRY(cudaMemcpyAsync(c->pp_dev, j.pp_in, j.ctl.icount * sizeof(int), cudaMemcpyDeviceToDevice, st));
-    else
-      SP2B_CUDA_TRY(cudaMemcpyAsync(c->pp_dev, j.pp_in, j.ctl.icount * sizeof(int), cudaMemcpyHostToDevice, st));
-  }
+  // pp / vv / icount are host arrays in every mode (only matrices follow device_ptrs)
+  if (j.ctl.algo == ALGO_SEQ && j.ctl.icount > 0)
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->pp_dev, j.pp_in, j.ctl.icount * sizeof(int), cudaMemcpyHostToDevice, st));
   if (j.vv_out && j.vv_accumulate && maxlaunch > 0) {
-    SP2B_CUDA_TRY(cudaMemcpyAsync(c->vv_dev, j.vv_out, maxlaunch * sizeof(double),
-                                  j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(c->vv_dev, j.vv_out, maxlaunch * sizeof(double), cudaMemcpyHostToDevice, st));
   } else {
     SP2B_CUDA_TRY(cudaMemsetAsync(c->vv_dev, 0, (maxlaunch + 2) * sizeof(double), st));
   }
@@ -330,13 +326,11 @@ int dense_solve(const DenseJob& j) {
   // ---- sequence outputs ----
   const int iters = so.iter;
   if (j.pp_out && iters > 0)
-    SP2B_CUDA_TRY(cudaMemcpyAsync(j.pp_out, c->pp_dev, iters * sizeof(int),
-                                  j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(j.pp_out, c->pp_dev, iters * sizeof(int), cudaMemcpyDeviceToHost, st));
   if (j.vv_out) {
     const int nvv = j.vv_accumulate ? maxlaunch : (j.ctl.algo == ALGO_SEQ ? j.ctl.icount : iters);
     if (nvv > 0)
-      SP2B_CUDA_TRY(cudaMemcpyAsync(j.vv_out, c->vv_dev, nvv * sizeof(double),
-                                    j.dev_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(j.vv_out, c->vv_dev, nvv * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));
   if (j.icount_out) *j.icount_out = iters;

@@ -216,9 +216,8 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   SP2B_CUDA_TRY(cudaMemcpyAsync(b.halo, hidx.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
   SP2B_CUDA_TRY(cudaMemcpyAsync(b.skey, skey.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
   SP2B_CUDA_TRY(cudaMemcpyAsync(b.sval, sval.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
-  if (maxiter > 0)
-    SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, pp, maxiter * sizeof(int),
-                                  dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  if (maxiter > 0)  // pp and vv are host arrays in every mode
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));  // host staging vectors go out of scope below
 
   // ---- the batched solve, captured once into a graph ----
@@ -315,8 +314,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (vv) {
     for (int k = 0; k < maxiter; ++k) vvh[k] = std::sqrt(vvh[k]);  // prg_fnormGraph
-    if (dev) SP2B_CUDA_TRY(cudaMemcpy(vv, vvh.data(), maxiter * sizeof(double), cudaMemcpyHostToDevice));
-    else std::memcpy(vv, vvh.data(), maxiter * sizeof(double));
+    std::memcpy(vv, vvh.data(), maxiter * sizeof(double));
   }
   if (!dev) {
     if (rho_core)

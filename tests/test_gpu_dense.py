@@ -82,7 +82,7 @@ def test_submatrix_inplace_fp64_parity(cuda, core):
 
 
 def test_normalize_gershgorin_idempotency(cuda):
-    h = M.two_band_1d(257, seed=2)
+    h = M.two_band_1d(258, seed=2)
     lo, hi = sp2b.gershgorin(h)
     rlo, rhi = O.gershgorin(h)
     assert lo == pytest.approx(rlo, rel=1e-14) and hi == pytest.approx(rhi, rel=1e-14)
@@ -127,9 +127,10 @@ def test_progress_named_exports(cuda):
     L = _lib.lib()
     hb = L.sp2b_bml_wrap_dense(h.ctypes.data_as(C.c_void_p), n)
     rb = L.sp2b_bml_wrap_dense(rho.ctypes.data_as(C.c_void_p), n)
-    L.prg_sp2_alg2(hb, rb, 1e-9, 0.5, 0, 100, b"Rel", 1e-10, 0)
+    # the reference tests' settings: minsp2iter 25, "Rel" (tests/src/main.F90:82-92)
+    L.prg_sp2_alg2(hb, rb, 1e-9, 0.5, 25, 100, b"Rel", 1e-10, 0)
     assert L.sp2b_prg_last_status() == 0
-    ref = O.sp2_alg2(h, 0.5, 0, 100, "Rel", 1e-10)
+    ref = O.sp2_alg2(h, 0.5, 25, 100, "Rel", 1e-10)
     assert rel(rho, ref.rho) <= FP64_TOL
     idem = C.c_double()
     half = np.asfortranarray(rho / 2)
@@ -139,9 +140,9 @@ def test_progress_named_exports(cuda):
     pp = np.zeros(100, dtype=np.int32)
     vv = np.zeros(100)
     ic = C.c_int(0)
-    L.prg_sp2_alg2_genseq(hb, rb, 1e-9, 0.5, 0, 100, b"Rel", 1e-10,
+    L.prg_sp2_alg2_genseq(hb, rb, 1e-9, 0.5, 25, 100, b"Rel", 1e-10,
                           pp.ctypes.data_as(C.c_void_p), C.byref(ic), vv.ctypes.data_as(C.c_void_p), 0)
-    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "Rel", 1e-10)
+    g = O.sp2_alg2_genseq(h, 0.5, 25, 100, "Rel", 1e-10)
     assert ic.value == g.icount and list(pp[:ic.value]) == g.pp
     for b in (hb, rb, hb2):
         L.sp2b_bml_free(b)
@@ -178,7 +179,9 @@ def test_mixed_fp16_against_fp64(cuda, n):
     got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
     k = min(len(got.pp), len(ref.pp))
     assert got.pp[:k] == ref.pp[:k]
-    assert abs(len(got.pp) - len(ref.pp)) <= 2
+    # the mixed loop stops once Tr(X - X^2) < mixed_tol and lets the FP64 McWeeny step
+    # finish, so it never runs longer than the FP64 loop
+    assert len(got.pp) <= len(ref.pp) + 1
     err = np.linalg.norm(got.rho - ref.rho) / n
     assert err <= 1e-6, err
     assert abs(np.trace(got.rho) - n) < 1e-5 * n
