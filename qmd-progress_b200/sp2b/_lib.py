@@ -63,6 +63,7 @@ _SIGS = {
     "sp2b_sp2_basic": (_i, [_vp, _vp, _i, _d, _d, _i, _i, C.c_char_p, _d, _i, C.POINTER(Opts), _ip]),
     "sp2b_sp2_submatrix_inplace": (_i, [_vp, _i, _d, _vp, _i, _vp, _d, _d, _i, C.POINTER(Opts)]),
     "sp2b_sp2_submatrix": (_i, [_vp, _vp, _i, _d, _vp, _i, _vp, _d, _d, _i, C.POINTER(Opts)]),
+    "sp2b_sp2_submatrix_inplace_noalloc": (_i, [_vp, _i, _vp, _i, _vp, _d, _d, _i, _vp]),
     "sp2b_gershgorin": (_i, [_vp, _i, _dp, _dp, C.POINTER(Opts)]),
     "sp2b_normalize": (_i, [_vp, _i, _dp, _dp, C.POINTER(Opts)]),
     "sp2b_check_idempotency": (_i, [_vp, _i, _d, _dp, C.POINTER(Opts)]),
