@@ -6,6 +6,8 @@ namespace sp2b {
 
 // Counts kernel launches issued by the library (diagnostics / bench).
 void note_launch(int k = 1);
+long long launch_count();
+void set_launch_count(long long v);
 
 // Outcome of a dense solve, written by the device.
 struct SolveOut {

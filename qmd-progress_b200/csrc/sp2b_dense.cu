@@ -20,6 +20,8 @@ static double g_step_ms = 0.0;
 static long long g_step_timed = 0;
 
 void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(); }
+void set_launch_count(long long v) { g_launches.store(v); }
 
 void set_last_error(const char* fmt, ...) {
   va_list ap;

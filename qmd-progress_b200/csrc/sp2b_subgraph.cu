@@ -48,6 +48,16 @@ struct SubBufs {
   SP2Rec* rec = nullptr;         size_t rec_cap = 0;
   int* pp = nullptr;             size_t pp_cap = 0;
   double* vv = nullptr;          size_t vv_cap = 0;
+  // layout of the last call (reused when the part lists are unchanged)
+  std::vector<long long> last_hp;
+  std::vector<int> last_lls, last_hidx;
+  std::vector<PartDesc> P;
+  int ld = 0, ntiles = 0;
+  long long rows = 0, coff = 0;
+  bool layout_valid = false;
+  // instantiated graph of the last call and the inputs it was captured with
+  cudaGraphExec_t exec = nullptr;
+  std::vector<unsigned char> exec_key;
 };
 static SubBufs g_sub[64];
 
@@ -91,40 +101,48 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     std::memcpy(lls.data(), llsize, nparts * sizeof(int));
   }
   const long long nhalo = hp[nparts];
+  const int bt = split ? 128 : 64;  // tile edge of the step kernel
   std::vector<int> hidx(nhalo);
   if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
   else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
 
-  std::vector<PartDesc> P(nparts);
-  int ld = 0;
-  long long rows = 0, coff = 0;
-  for (int p = 0; p < nparts; ++p) {
-    const long long sz = hp[p + 1] - hp[p];
-    if (sz <= 0 || sz > 32768 || lls[p] < 0 || lls[p] > sz) {
-      set_last_error("part %d: bad sizes (lsize=%lld llsize=%d)", p, sz, lls[p]);
+  const bool same_layout = b.layout_valid && b.last_hp == hp && b.last_lls == lls &&
+                           b.last_hidx == hidx;
+  if (!same_layout) {
+    b.layout_valid = false;
+    std::vector<PartDesc>& P = b.P;
+    P.assign(nparts, PartDesc());
+    int ld = 0;
+    long long rows = 0, coff = 0;
+    for (int p = 0; p < nparts; ++p) {
+      const long long sz = hp[p + 1] - hp[p];
+      if (sz <= 0 || sz > 32768 || lls[p] < 0 || lls[p] > sz) {
+        set_last_error("part %d: bad sizes (lsize=%lld llsize=%d)", p, sz, lls[p]);
+        return SP2B_BAD_ARG;
+      }
+      PartDesc& d = P[p];
+      d.n = (int)sz;
+      d.np = padded(d.n);
+      d.ncore = lls[p];
+      d.hoff = hp[p];
+      d.row0 = rows;
+      d.coff = coff;
+      d.pad_ = 0;
+      rows += d.np;
+      coff += (long long)d.ncore * d.n;
+      ld = std::max(ld, d.np);
+    }
+    for (long long q = 0; q < nhalo; ++q)
+      if (hidx[q] < 0 || hidx[q] >= n) {
+        set_last_error("halo index out of range at %lld", q);
+        return SP2B_BAD_ARG;
+      }
+    if (rows > 0x7fffffffLL) {
+      set_last_error("packed parts exceed 2^31 rows");
       return SP2B_BAD_ARG;
     }
-    PartDesc& d = P[p];
-    d.n = (int)sz;
-    d.np = padded(d.n);
-    d.ncore = lls[p];
-    d.hoff = hp[p];
-    d.row0 = rows;
-    d.coff = coff;
-    d.pad_ = 0;
-    rows += d.np;
-    coff += (long long)d.ncore * d.n;
-    ld = std::max(ld, d.np);
-  }
-  for (long long q = 0; q < nhalo; ++q)
-    if (hidx[q] < 0 || hidx[q] >= n) {
-      set_last_error("halo index out of range at %lld", q);
-      return SP2B_BAD_ARG;
-    }
-  // sorted node lists per part for the CSR column lookup
-  std::vector<int> skey(nhalo), sval(nhalo);
-  {
-    std::vector<int> ord;
+    // sorted node lists per part for the CSR column lookup
+    std::vector<int> skey(nhalo), sval(nhalo), ord;
     for (int p = 0; p < nparts; ++p) {
       const int m = P[p].n;
       ord.resize(m);
@@ -136,29 +154,50 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         sval[P[p].hoff + i] = ord[i];
       }
     }
+    std::vector<int> row_part(rows);
+    for (int p = 0; p < nparts; ++p)
+      std::fill(row_part.begin() + P[p].row0, row_part.begin() + P[p].row0 + P[p].np, p);
+    // tile list, most expensive parts first (cost of a tile ~ np)
+    std::vector<int> order(nparts);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return P[a].np > P[b2].np; });
+    std::vector<int4> tiles;
+    for (int p : order) {
+      const int T = P[p].np / bt;
+      for (int bj = 0; bj < T; ++bj)
+        for (int bi = 0; bi <= bj; ++bi)
+          // K runs only to the part size rounded up to 64: the rest of the padded
+          // block is zero, so those k-blocks contribute nothing
+          tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj,
+                                    std::min(P[p].np, (P[p].n + 63) / 64 * 64),
+                                    P[p].ncore > 0 ? P[p].ncore : -1));
+    }
+    const int ntiles = (int)tiles.size();
+    SP2B_CUDA_TRY(grow_buf(b.parts, b.parts_cap, nparts));
+    SP2B_CUDA_TRY(grow_buf(b.tiles, b.tiles_cap, ntiles));
+    SP2B_CUDA_TRY(grow_buf(b.row_part, b.row_part_cap, rows));
+    SP2B_CUDA_TRY(grow_buf(b.halo, b.halo_cap, nhalo));
+    SP2B_CUDA_TRY(grow_buf(b.skey, b.skey_cap, nhalo));
+    SP2B_CUDA_TRY(grow_buf(b.sval, b.sval_cap, nhalo));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.parts, P.data(), nparts * sizeof(PartDesc), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.tiles, tiles.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.row_part, row_part.data(), rows * sizeof(int), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.halo, hidx.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.skey, skey.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.sval, sval.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));  // host staging vectors go out of scope
+    b.ld = ld;
+    b.rows = rows;
+    b.coff = coff;
+    b.ntiles = ntiles;
+    b.last_hp = hp;
+    b.last_lls = lls;
+    b.last_hidx = hidx;
+    b.layout_valid = true;
   }
-  // row -> part map
-  std::vector<int> row_part(rows);
-  for (int p = 0; p < nparts; ++p)
-    std::fill(row_part.begin() + P[p].row0, row_part.begin() + P[p].row0 + P[p].np, p);
-  // tile list, most expensive parts first (cost of a tile ~ np)
-  const int bt = split ? 128 : 64;
-  std::vector<int> order(nparts);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return P[a].np > P[b2].np; });
-  std::vector<int4> tiles;
-  for (int p : order) {
-    const int T = P[p].np / bt;
-    for (int bj = 0; bj < T; ++bj)
-      for (int bi = 0; bi <= bj; ++bi)
-        tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj, P[p].np,
-                                  P[p].ncore > 0 ? P[p].ncore : -1));
-  }
-  if (rows > 0x7fffffffLL) {
-    set_last_error("packed parts exceed 2^31 rows");
-    return SP2B_BAD_ARG;
-  }
-  const int ntiles = (int)tiles.size();
+  const int ld = b.ld;
+  const long long rows = b.rows, coff = b.coff;
+  const int ntiles = b.ntiles;
 
   // ---- device buffers ----
   long long nnz;
@@ -174,12 +213,6 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   } else {
     SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
   }
-  SP2B_CUDA_TRY(grow_buf(b.parts, b.parts_cap, nparts));
-  SP2B_CUDA_TRY(grow_buf(b.tiles, b.tiles_cap, ntiles));
-  SP2B_CUDA_TRY(grow_buf(b.row_part, b.row_part_cap, rows));
-  SP2B_CUDA_TRY(grow_buf(b.halo, b.halo_cap, nhalo));
-  SP2B_CUDA_TRY(grow_buf(b.skey, b.skey_cap, nhalo));
-  SP2B_CUDA_TRY(grow_buf(b.sval, b.sval_cap, nhalo));
   SP2B_CUDA_TRY(grow_buf(b.partials, b.partials_cap, 4 * (size_t)ntiles));
   SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
   SP2B_CUDA_TRY(grow_buf(b.pp, b.pp_cap, (size_t)maxiter + 1));
@@ -210,15 +243,8 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
       dense_d = b.dense;
     }
   }
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.parts, P.data(), nparts * sizeof(PartDesc), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.tiles, tiles.data(), ntiles * sizeof(int4), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.row_part, row_part.data(), rows * sizeof(int), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.halo, hidx.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.skey, skey.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaMemcpyAsync(b.sval, sval.data(), nhalo * sizeof(int), cudaMemcpyHostToDevice, st));
   if (maxiter > 0)  // pp and vv are host arrays in every mode
     SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
-  SP2B_CUDA_TRY(cudaStreamSynchronize(st));  // host staging vectors go out of scope below
 
   // ---- the batched solve, captured once into a graph ----
   StepArgs a;
@@ -241,8 +267,32 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   a.counter = c->counter;
   a.err = c->err;
 
+  // The captured graph bakes in every pointer, size and scalar it launches with;
+  // reuse it when all of them are unchanged.
+  struct Key {
+    const void* p[21];
+    long long q[8];
+    double d[2];
+  } key;
+  memset(&key, 0, sizeof(key));
+  const void* ptrs[21] = {rp_d, col_d, val_d, core_d, dense_d, b.xs, b.x2, b.hi[0], b.hi[1],
+                          b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
+                          b.sval, b.partials, b.rec, b.pp, (const void*)st};
+  memcpy(key.p, ptrs, sizeof(ptrs));
+  const long long qs[8] = {n, nparts, rows, ld, maxiter, prec, ntiles, (long long)(size_t)b.vv};
+  memcpy(key.q, qs, sizeof(qs));
+  key.d[0] = mineval;
+  key.d[1] = maxeval;
+  std::vector<unsigned char> kbytes((unsigned char*)&key, (unsigned char*)&key + sizeof(key));
+  const bool reuse = b.exec && b.exec_key == kbytes;
   cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraphExec_t exec = reuse ? b.exec : nullptr;
+  if (!reuse) {
+  if (b.exec) {
+    cudaGraphExecDestroy(b.exec);
+    b.exec = nullptr;
+  }
+  const long long launches_before = launch_count();  // captured launches do not run yet
   SP2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   auto body = [&]() -> cudaError_t {
     cudaError_t e;
@@ -286,6 +336,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   };
   const cudaError_t be = body();
   const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  set_launch_count(launches_before);
   if (be != cudaSuccess || ce != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
     set_last_error("graph capture failed: %s / %s", cudaGetErrorString(be), cudaGetErrorString(ce));
@@ -297,10 +348,12 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     set_last_error("graph instantiate failed: %s", cudaGetErrorString(ie));
     return SP2B_CUDA_ERROR;
   }
+  b.exec = exec;
+  b.exec_key = kbytes;
+  }
   cudaError_t le = cudaGraphLaunch(exec, st);
   if (le == cudaSuccess) le = cudaStreamSynchronize(st);
-  cudaGraphExecDestroy(exec);
-  note_launch(0);
+  note_launch(maxiter + 3);  // extract, normalise, maxiter steps, scatter
   if (le != cudaSuccess) {
     set_last_error("graph launch failed: %s", cudaGetErrorString(le));
     return SP2B_CUDA_ERROR;
