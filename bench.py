@@ -388,7 +388,16 @@ def run_subgraph(args, rank, world, local):
     torch.cuda.empty_cache()
     full_iters = ic.value
     eh, el, egap = sp2b.homolumogap(vv[:full_iters], full_iters, pp[:full_iters], emin, emax)
-    seq, maxiter = sp2b.sp2sequence(emin, emax, eh, el, 1e-12)
+    if egap > 0.0 and emin < eh < el < emax:
+        seq, maxiter = sp2b.sp2sequence(emin, emax, eh, el, 1e-12)
+        seq_source = "prg_sp2sequence(homolumogap)"
+    else:
+        # no usable gap estimate (the full-system ||X - X^2||_F never fell below the
+        # prg_homolumogap threshold on this near-gapless lattice): the parts replay the
+        # branch sequence the full-system genseq took
+        seq, maxiter = [int(x) for x in pp[:full_iters]], full_iters
+        seq_source = "full-system genseq pp"
+
     g_csr = G.thresholded_square_graph((rp, col, val), n, 0.6)
     parts = G.rcb_partition(G.lattice_coords(L), args.parts, seed=0, lo=0.4, hi=0.6)
     hp, hidx, ls, lls = sp2b.subgraph_halos(n, g_csr, parts, None, double_jump=False)
@@ -452,7 +461,8 @@ def run_subgraph(args, rank, world, local):
                           "n": n, "parts": len(parts), "lsize_min": int(ls.min()),
                           "lsize_max": int(ls.max()), "lsize_mean": float(ls.mean()),
                           "maxiter": maxiter, "full_genseq_iters": full_iters,
-                          "homo": eh, "lumo": el, "graph": "|H^2| > 0.6", "halo": "one jump",
+                          "homo": eh, "lumo": el, "sequence": seq_source,
+                          "graph": "|H^2| > 0.6", "halo": "one jump",
                           "partition": "RCB U[0.4,0.6]", "setup_s": setup_s},
                "tflops": value * flops / 1e12, "flops_per_solve": flops,
                "fp64": {"solves_per_s": world * max(1, args.fp64_steps) / (t64 / 1e3),

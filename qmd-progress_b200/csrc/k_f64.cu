@@ -262,7 +262,9 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
 #pragma unroll
     for (int ni = 0; ni < C::NI; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
 
-  const int KB = nloc / C::BK;
+  // every valid tile starts inside its part; anything else contributes nothing
+  const bool tile_ok = !p.tiles || (i0 < nloc && j0 < nloc);
+  const int KB = tile_ok ? nloc / C::BK : 0;
   auto load = [&](int stage, int kb) {
     double* As = sm + stage * 2 * C::BK * C::LDS;
     double* Bs = As + C::BK * C::LDS;
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
   double* __restrict__ out = p.out ? (double*)p.out + row0 * ld : nullptr;
   double s[4] = {0.0, 0.0, 0.0, 0.0};  // ||out||^2, Tr out, ||E-acc||^2 (core rows), Tr acc
 #pragma unroll
-  for (int mi = 0; mi < C::MI; ++mi) {
+  for (int mi = 0; mi < (tile_ok ? C::MI : 0); ++mi) {
 #pragma unroll
     for (int ni = 0; ni < C::NI; ++ni) {
       const int r = i0 + wm * C::TM + mi * 8 + g;

@@ -192,6 +192,9 @@ __global__ void __launch_bounds__(128, 1)
   }
   const int i0 = bi * tc::BM, j0 = bj * tc::BN;
   const int ld = p.ld;
+  // every valid tile starts inside its part (i0, j0 < part size <= K extent); anything
+  // else is skipped (no loads, no stores, zero partials) instead of addressing outside
+  const bool tile_ok = !(SYM && p.tiles) || (i0 < nloc && j0 < nloc);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(128, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
-  const int KB = nloc / tc::BK;
+  const int KB = tile_ok ? nloc / tc::BK : 0;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(128, 1)
   const bool good = mbar_wait(smem_u32(&bar_done), 0, &s_abort) && !s_abort;
   tc_fence_after();
   double sums[4] = {0.0, 0.0, 0.0, 0.0};
-  if (good) {
+  if (good && tile_ok) {
     const int rl = warp * 32 + lane;
     const int r = i0 + rl;
     const bool diag = SYM && (bi == bj);

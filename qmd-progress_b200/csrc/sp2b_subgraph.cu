@@ -52,7 +52,7 @@ struct SubBufs {
   std::vector<long long> last_hp;
   std::vector<int> last_lls, last_hidx;
   std::vector<PartDesc> P;
-  int ld = 0, ntiles = 0;
+  int ld = 0, ntiles = 0, layout_bt = 0;
   long long rows = 0, coff = 0;
   bool layout_valid = false;
   // instantiated graph of the last call and the inputs it was captured with
@@ -106,8 +106,9 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
   else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
 
-  const bool same_layout = b.layout_valid && b.last_hp == hp && b.last_lls == lls &&
-                           b.last_hidx == hidx;
+  // the tile list depends on the tile edge of the step kernel (128 split, 64 FP64)
+  const bool same_layout = b.layout_valid && b.layout_bt == bt && b.last_hp == hp &&
+                           b.last_lls == lls && b.last_hidx == hidx;
   if (!same_layout) {
     b.layout_valid = false;
     std::vector<PartDesc>& P = b.P;
@@ -193,6 +194,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     b.last_hp = hp;
     b.last_lls = lls;
     b.last_hidx = hidx;
+    b.layout_bt = bt;
     b.layout_valid = true;
   }
   const int ld = b.ld;

@@ -99,3 +99,20 @@ def test_poly512_subgraph_matches_fixture(cuda, poly512, prec):
     half = rho / 2
     idem = np.linalg.norm(half @ half - half)       # prg_check_idempotency of rho/2
     assert idem <= 1e-2                             # tests/src/main.F90:876-881
+
+
+def test_subgraph_precision_switch_reuses_layout_safely(cuda):
+    """The cached part layout and CUDA graph must follow the precision: the split and
+    FP64 step kernels use different tile edges (128 and 64)."""
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    rho_ref, _, _ = O.subgraph_sp2_loop(h, g, parts, pp, maxiter, emin, emax)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
+    for prec in [sp2b.PREC_FP64, sp2b.PREC_MIXED_FP16, sp2b.PREC_FP64, sp2b.PREC_MIXED_FP16,
+                 sp2b.PREC_MIXED_FP16]:
+        rho, _, _ = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin,
+                                           emax, precision=prec)
+        if prec == sp2b.PREC_FP64:
+            assert np.linalg.norm(rho - rho_ref) / np.linalg.norm(rho_ref) < 1e-10
+        else:
+            assert np.linalg.norm(rho - rho_ref) / n <= 1e-6
