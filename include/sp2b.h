@@ -199,6 +199,20 @@ int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
  * computed as hi/lo FP16 tcgen05 products with FP32 accumulation. */
 int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* c, int n, void* stream);
 
+/* Differentiable SP2 (the autograd path), device FP32 n x n arrays on `stream`.  These
+ * have no single counterpart in the reference: they are the pieces of a reverse-mode
+ * derivative of the SP2 recursion whose forward-mode form is prg_compute_response_SP2
+ * (src/prg_response_mod.F90:653-782).
+ *   normalize:    x = (maxeval I - h)/(maxeval - mineval)
+ *   sp2_step:     y = x^2 (branch 1) or 2x - x^2 (branch 0), split-precision products
+ *   adjoint_step: g_out = {g, x} (branch 1) or 2g - {g, x} (branch 0), {g,x} = gx + xg,
+ *                 `work` is an n x n scratch array. */
+int sp2b_dev_normalize_f32(const float* h, float* x, int n, double mineval, double maxeval,
+                           void* stream);
+int sp2b_dev_sp2_step_f32(const float* x, float* y, int n, int branch, void* stream);
+int sp2b_dev_adjoint_step_f32(const float* g, const float* x, float* g_out, float* work, int n,
+                              int branch, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------------------ */
 
 /* State of the last dense solve on the current device: SP2 step launches issued by

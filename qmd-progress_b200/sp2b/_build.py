@@ -24,6 +24,7 @@ SOURCES = [
     "sp2b_dense.cu",
     "sp2b_subgraph.cu",
     "sp2b_noalloc.cu",
+    "sp2b_adjoint.cu",
     "sp2b_host.cpp",
     "sp2b_prg.cpp",
 ]

@@ -75,6 +75,9 @@ _SIGS = {
     "sp2b_subgraph_sp2_loop": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _i, _d, _d, _vp, _vp,
                                     _vp, C.POINTER(Opts)]),
     "sp2b_dev_sym_gemm_f32": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "sp2b_dev_normalize_f32": (_i, [_vp, _vp, _i, _d, _d, _vp]),
+    "sp2b_dev_sp2_step_f32": (_i, [_vp, _vp, _i, _i, _vp]),
+    "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_set_step_timing": (_i, [_i]),

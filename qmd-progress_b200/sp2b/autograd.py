@@ -1,0 +1,117 @@
+"""Differentiable SP2: a hand-written adjoint of the SP2 recursion behind
+torch.autograd.Function, giving d(Tr D A)/dH for response and force workloads.
+
+Forward (replaying a branch sequence pp with fixed bounds, like prg_sp2_alg2_seq,
+src/prg_sp2_mod.F90:543-627):  X_0 = (e_max I - H)/(e_max - e_min),
+X_{k+1} = X_k^2 (pp_k = 1) or 2 X_k - X_k^2 (pp_k = 0), D = 2 X_K.
+FP32 storage, squarings as FP16 hi+lo split products on the tensor cores.
+
+Backward: G_K = dL/dX_K = 2 sym(dL/dD); G_k = {G_{k+1}, X_k} or 2 G_{k+1} - {G_{k+1}, X_k};
+dL/dH = -G_0/(e_max - e_min).  The forward keeps X_k every `checkpoint` steps; the
+backward recomputes each segment from its checkpoint.  The Gershgorin bounds and the
+branch sequence are held fixed (they are piecewise constant in H), which is what the
+reference's density-matrix perturbation theory does (prg_compute_response_SP2,
+src/prg_response_mod.F90:653-782, propagates a perturbation through the same
+recursion with the same branch decisions).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _step(x: torch.Tensor, y: torch.Tensor, branch: int):
+    _lib.check(_lib.lib().sp2b_dev_sp2_step_f32(x.data_ptr(), y.data_ptr(), x.shape[0], int(branch),
+                                                _stream()), "sp2_step_f32")
+
+
+def _adjoint(g: torch.Tensor, x: torch.Tensor, out: torch.Tensor, work: torch.Tensor, branch: int):
+    _lib.check(_lib.lib().sp2b_dev_adjoint_step_f32(g.data_ptr(), x.data_ptr(), out.data_ptr(),
+                                                    work.data_ptr(), x.shape[0], int(branch),
+                                                    _stream()), "adjoint_step_f32")
+
+
+def _check_input(h: torch.Tensor):
+    if not (h.is_cuda and h.dtype == torch.float32 and h.dim() == 2 and h.shape[0] == h.shape[1]):
+        raise ValueError("H must be a square float32 CUDA tensor")
+    return h.contiguous()
+
+
+class SP2Density(torch.autograd.Function):
+    """D = SP2(H) with a fixed branch sequence and fixed bounds; see the module docstring."""
+
+    @staticmethod
+    def forward(ctx, h, pp, mineval, maxeval, checkpoint=4):
+        h = _check_input(h)
+        n = h.shape[0]
+        pp = [int(b) for b in pp]
+        x = torch.empty_like(h)
+        _lib.check(_lib.lib().sp2b_dev_normalize_f32(h.data_ptr(), x.data_ptr(), n, float(mineval),
+                                                     float(maxeval), _stream()), "normalize_f32")
+        ckpts = [x.clone()]
+        y = torch.empty_like(h)
+        for k, b in enumerate(pp):
+            _step(x, y, b)
+            x, y = y, x
+            if (k + 1) % checkpoint == 0 and k + 1 < len(pp):
+                ckpts.append(x.clone())
+        ctx.save_for_backward(*ckpts)
+        ctx.pp = pp
+        ctx.scale = -1.0 / (float(maxeval) - float(mineval))
+        ctx.checkpoint = checkpoint
+        return 2.0 * x
+
+    @staticmethod
+    def backward(ctx, grad_d):
+        ckpts = ctx.saved_tensors
+        pp, c = ctx.pp, ctx.checkpoint
+        K = len(pp)
+        g = (grad_d + grad_d.transpose(0, 1)).contiguous().float()   # dL/dX_K = 2 sym(dL/dD)
+        work = torch.empty_like(g)
+        gout = torch.empty_like(g)
+        nseg = (K + c - 1) // c
+        for s in range(nseg - 1, -1, -1):
+            k0, k1 = s * c, min((s + 1) * c, K)
+            xs = [ckpts[s]]
+            for k in range(k0, k1 - 1):            # X_{k0+1} .. X_{k1-1} from the checkpoint
+                y = torch.empty_like(g)
+                _step(xs[-1], y, pp[k])
+                xs.append(y)
+            for k in range(k1 - 1, k0 - 1, -1):
+                _adjoint(g, xs[k - k0], gout, work, pp[k])
+                g, gout = gout, g
+        return ctx.scale * g, None, None, None, None
+
+
+def sp2_density(h: torch.Tensor, pp, mineval: float, maxeval: float, checkpoint: int = 4):
+    """Differentiable D(H) for a given branch sequence and bounds."""
+    return SP2Density.apply(h, pp, mineval, maxeval, checkpoint)
+
+
+def sequence_and_bounds(h: torch.Tensor, bndfil: float, maxsp2iter: int = 100,
+                        precision: int = _lib.PREC_FP64):
+    """Branch sequence and Gershgorin bounds of H from the library's genseq solve
+    (prg_sp2_alg2_genseq, src/prg_sp2_mod.F90:395-533) on an FP64 copy of H."""
+    n = h.shape[0]
+    h64 = h.detach().double().contiguous()
+    rho = torch.empty_like(h64)
+    pp = np.zeros(maxsp2iter + 2, dtype=np.int32)
+    vv = np.zeros(maxsp2iter + 2)
+    ic = C.c_int(0)
+    o = _lib.make_opts(precision=precision, device_ptrs=True, stream=_stream())
+    L = _lib.lib()
+    _lib.check(L.sp2b_sp2_alg2_genseq(h64.data_ptr(), rho.data_ptr(), n, 0.0, bndfil, 0, maxsp2iter,
+                                      b"None", 1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
+                                      C.byref(o)), "genseq")
+    lo, hi = C.c_double(), C.c_double()
+    _lib.check(L.sp2b_gershgorin(h64.data_ptr(), n, C.byref(lo), C.byref(hi), C.byref(o)),
+               "gershgorin")
+    return [int(b) for b in pp[:ic.value]], lo.value, hi.value

@@ -116,3 +116,23 @@ def test_subgraph_precision_switch_reuses_layout_safely(cuda):
             assert np.linalg.norm(rho - rho_ref) / np.linalg.norm(rho_ref) < 1e-10
         else:
             assert np.linalg.norm(rho - rho_ref) / n <= 1e-6
+
+
+def test_distributed_path_single_rank_gpu_solver(cuda, tmp_path):
+    """sp2b.dist with the GPU per-rank solver (one rank, gloo) equals the local call."""
+    import torch.distributed as dist
+    from sp2b import dist as D
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
+    rho_loc, _, vv_loc = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter,
+                                                emin, emax, precision=sp2b.PREC_FP64)
+    dist.init_process_group("gloo", init_method=f"file://{tmp_path}/pg", rank=0, world_size=1)
+    try:
+        rho, vv, owner = D.subgraph_sp2_loop_distributed(
+            n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin, emax,
+            D.gpu_solver(sp2b.PREC_FP64))
+    finally:
+        dist.destroy_process_group()
+    assert np.array_equal(rho, rho_loc)
+    assert np.allclose(vv, vv_loc, rtol=1e-12, atol=0)
