@@ -83,7 +83,8 @@ int sp2b_dev_normalize_f32(const float* h, float* x, int n, double mineval, doub
   int status = SP2B_OK;
   Ctx* c = get_ctx(&status);
   if (!c) return status;
-  k_normalize_f32<<<grid1d((size_t)n * n), 256, 0, stream ? (cudaStream_t)stream : c->stream>>>(
+  (void)c;
+  k_normalize_f32<<<grid1d((size_t)n * n), 256, 0, (cudaStream_t)stream>>>(
       h, n, (float)(-1.0 / mm), (float)(maxeval / mm), x);
   note_launch();
   SP2B_CUDA_TRY(cudaGetLastError());
@@ -99,7 +100,7 @@ int sp2b_dev_sp2_step_f32(const float* x, float* y, int n, int branch, void* str
   Ctx* c = get_ctx(&status);
   if (!c) return status;
   std::lock_guard<std::mutex> lk(c->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // device arrays: NULL = the default stream
   const int np = padded(n);
   SP2B_CUDA_TRY(c->ensure_split(np));
   SP2B_CUDA_TRY(c->ensure_common(0, np, 1, n));
@@ -133,7 +134,8 @@ int sp2b_dev_adjoint_step_f32(const float* g, const float* x, float* g_out, floa
   int status = SP2B_OK;
   Ctx* c = get_ctx(&status);
   if (!c) return status;
-  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;  // one stream for both
+  (void)c;
+  cudaStream_t st = (cudaStream_t)stream;  // NULL = the default stream, for both kernels
   int s = sp2b_dev_sym_gemm_f32(g, x, work, n, st);  // M = G X
   if (s != SP2B_OK) return s;
   dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);

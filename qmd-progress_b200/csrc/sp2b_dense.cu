@@ -124,8 +124,12 @@ static int parse_conv(const char* s) {
   return CONV_NONE;
 }
 
+// Device-pointer calls run on the caller's stream, and a NULL stream there means the
+// CUDA default stream (the caller's data is ordered on it); host-pointer calls, whose
+// data movement is the library's own, run on the library stream unless one is given.
 static cudaStream_t pick_stream(const sp2b_opts* o, Ctx* c) {
-  return (o && o->stream) ? (cudaStream_t)o->stream : c->stream;
+  if (o && o->stream) return (cudaStream_t)o->stream;
+  return (o && o->device_ptrs) ? (cudaStream_t)0 : c->stream;
 }
 
 int dense_solve(const DenseJob& j) {
@@ -149,7 +153,7 @@ int dense_solve(const DenseJob& j) {
   Ctx* c = get_ctx(&status);
   if (!c) return status;
   std::lock_guard<std::mutex> lk(c->mu);
-  cudaStream_t st = j.stream ? j.stream : c->stream;
+  cudaStream_t st = j.stream ? j.stream : (j.dev_ptrs ? (cudaStream_t)0 : c->stream);
   const int n = j.n, np = padded(n);
   const bool split = j.prec != SP2B_PREC_FP64;
   const int bf16 = j.prec == SP2B_PREC_MIXED_BF16;
@@ -720,7 +724,7 @@ int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* cout, int n, vo
   Ctx* c = get_ctx(&status);
   if (!c) return status;
   std::lock_guard<std::mutex> lk(c->mu);
-  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  cudaStream_t st = (cudaStream_t)stream;  // device arrays: NULL = the default stream
   const int np = padded(n);
   SP2B_CUDA_TRY(c->ensure_split(np));
   SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));

@@ -88,7 +88,10 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   if (!c) return status;
   std::lock_guard<std::mutex> lk(c->mu);
   SubBufs& b = g_sub[c->dev];
-  cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : c->stream;
+  // work is ordered on the caller's stream (device pointers: NULL = the default
+  // stream); the CUDA graph is captured on the library stream and launched on `st`
+  cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : (dev ? (cudaStream_t)0 : c->stream);
+  cudaStream_t cap = c->stream;
 
   // ---- host-side layout (index lists are small; device inputs are fetched) ----
   std::vector<long long> hp(nparts + 1);
@@ -279,7 +282,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   memset(&key, 0, sizeof(key));
   const void* ptrs[21] = {rp_d, col_d, val_d, core_d, dense_d, b.xs, b.x2, b.hi[0], b.hi[1],
                           b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
-                          b.sval, b.partials, b.rec, b.pp, (const void*)st};
+                          b.sval, b.partials, b.rec, b.pp, (const void*)cap};
   memcpy(key.p, ptrs, sizeof(ptrs));
   const long long qs[8] = {n, nparts, rows, ld, maxiter, prec, ntiles, (long long)(size_t)b.vv};
   memcpy(key.q, qs, sizeof(qs));
@@ -295,23 +298,23 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     b.exec = nullptr;
   }
   const long long launches_before = launch_count();  // captured launches do not run yet
-  SP2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  SP2B_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   auto body = [&]() -> cudaError_t {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(b.rec, 0, sizeof(SP2Rec), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(b.vv, 0, ((size_t)maxiter + 1) * sizeof(double), st)) != cudaSuccess) return e;
-    if (rho_dense && (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), st)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), cap)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), cap)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), cap)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), cap)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(b.rec, 0, sizeof(SP2Rec), cap)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(b.vv, 0, ((size_t)maxiter + 1) * sizeof(double), cap)) != cudaSuccess) return e;
+    if (rho_dense && (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
       return e;
     if ((e = launch_extract_csr(rp_d, col_d, val_d, b.parts, nparts, b.halo, b.skey, b.sval, ld,
-                                b.xs, st)) != cudaSuccess)
+                                b.xs, cap)) != cudaSuccess)
       return e;
     if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, mineval, maxeval, prec,
                                split ? (void*)b.hi[0] : nullptr, split ? (void*)b.lo[0] : nullptr,
-                               st)) != cudaSuccess)
+                               cap)) != cudaSuccess)
       return e;
     for (int k = 0; k < maxiter; ++k) {
       a.k = k;
@@ -321,23 +324,23 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
         a.out = b.hi[bout];
         a.out_lo = b.lo[bout];
-        e = launch_sym_gemm_tc_batched(a, rows, prec == SP2B_PREC_MIXED_BF16, st);
+        e = launch_sym_gemm_tc_batched(a, rows, prec == SP2B_PREC_MIXED_BF16, cap);
       } else {
         double* xin = bin ? b.x2 : b.xs;
         double* xout = bout ? b.x2 : b.xs;
         a.A = a.B = a.E = xin;
         a.out = xout;
-        e = launch_sym_gemm_f64_batched(a, bt, st);
+        e = launch_sym_gemm_f64_batched(a, bt, cap);
       }
       if (e != cudaSuccess) return e;
     }
     const int fb = maxiter & 1;
     return launch_scatter_parts(fb ? b.x2 : b.xs, split ? (void*)b.hi[fb] : nullptr,
                                 split ? (void*)b.lo[fb] : nullptr, prec, b.parts, nparts, b.halo,
-                                ld, core_d, rho_dense ? dense_d : nullptr, n, st);
+                                ld, core_d, rho_dense ? dense_d : nullptr, n, cap);
   };
   const cudaError_t be = body();
-  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
   set_launch_count(launches_before);
   if (be != cudaSuccess || ce != cudaSuccess) {
     if (graph) cudaGraphDestroy(graph);
