@@ -370,6 +370,290 @@ __global__ void __launch_bounds__(128, 1)
 }
 
 // ---------------------------------------------------------------------------------
+// Persistent, warp-specialised SP2 step (the kernel used for every symmetric launch).
+//   warp 0: TMA producer; warp 1: TMEM owner + MMA issuer; warps 2..9: epilogue.
+// Each CTA walks its tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (a fixed
+// assignment, so its partial sums are reproducible).  TMEM holds two accumulator
+// sets (hi*hi and cross, 128 columns each, x2 = 512 columns): the MMAs of tile t+1 run
+// while the epilogue drains tile t.  Each lane quarter of TMEM is read by two
+// epilogue warps, one per 64-column half.
+// ---------------------------------------------------------------------------------
+namespace tcp {
+constexpr int NWARP = 10;
+constexpr int NTHR = NWARP * 32;
+constexpr int EPI_WARPS = 8;
+constexpr int TMEM_COLS = 512;
+constexpr int CHUNK = 16;  // columns per tcgen05.ld
+}  // namespace tcp
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+struct TileInfo {
+  int row0, i0, j0, kb, core;
+  bool ok, diag;
+};
+
+__device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
+  TileInfo ti;
+  int bi, bj, nloc = p.np;
+  ti.core = p.core;
+  ti.row0 = 0;
+  if (p.tiles) {
+    const int4 v = p.tiles[t];
+    ti.row0 = v.x;
+    bi = v.y >> 16;
+    bj = v.y & 0xffff;
+    nloc = v.z;
+    ti.core = v.w;
+  } else {
+    upper_tile(t, bi, bj);
+  }
+  ti.i0 = bi * tc::BM;
+  ti.j0 = bj * tc::BN;
+  // a valid tile starts inside its part; anything else is skipped
+  ti.ok = !p.tiles || (ti.i0 < nloc && ti.j0 < nloc);
+  ti.kb = ti.ok ? nloc / tc::BK : 0;
+  ti.diag = bi == bj;
+  return ti;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(tcp::NTHR, 1)
+    k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                 const StepArgs p, int ntiles) {
+  using TR = SplitTraits<T>;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full[tc::ST];
+  __shared__ __align__(8) uint64_t bar_empty[tc::ST];
+  __shared__ __align__(8) uint64_t bar_tfull[2];
+  __shared__ __align__(8) uint64_t bar_tempty[2];
+  __shared__ __align__(8) uint64_t bar_final;
+  __shared__ uint32_t tmem_holder;
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+  __shared__ volatile int s_abort;
+
+  double alpha = p.alpha, beta = p.beta;
+  if (p.control) {
+    const int br = control_prologue(p);
+    if (br < 0) return;
+    if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
+    else { alpha = -1.0; beta = 2.0; }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = smem_u32(smem);
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < tc::ST; ++s) {
+      mbar_init(smem_u32(&bar_full[s]), 1);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(smem_u32(&bar_tfull[a]), 1);
+      mbar_init(smem_u32(&bar_tempty[a]), tcp::EPI_WARPS);
+    }
+    mbar_init(smem_u32(&bar_final), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), tcp::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_holder;
+  double sums[4] = {0.0, 0.0, 0.0, 0.0};
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer ----------------
+      int issued_phase[tc::ST];
+      for (int s = 0; s < tc::ST; ++s) issued_phase[s] = -1;
+      bool ok = true;
+      uint32_t g = 0;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const TileInfo ti = persist_tile(p, t);
+        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+          const int s = g % tc::ST;
+          const uint32_t u = g / tc::ST;
+          if (g >= (uint32_t)tc::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&bar_full[s]);
+          const uint32_t st = sbase + s * tc::STAGE_BYTES;
+          mbar_expect_tx(fb, tc::STAGE_BYTES);
+          tma_load_2d(st + 0 * tc::TILE_BYTES, &tm_hi, fb, kb * tc::BK, ti.row0 + ti.i0);
+          tma_load_2d(st + 1 * tc::TILE_BYTES, &tm_lo, fb, kb * tc::BK, ti.row0 + ti.i0);
+          tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_hi, fb, kb * tc::BK, ti.row0 + ti.j0);
+          tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_lo, fb, kb * tc::BK, ti.row0 + ti.j0);
+          issued_phase[s] = u & 1;
+        }
+      }
+      if (!ok) {  // abort: wait (bounded) for this CTA's copies still in flight
+        for (int s = 0; s < tc::ST; ++s)
+          if (issued_phase[s] >= 0)
+            for (uint32_t i = 0; i < kSpinLimit; ++i)
+              if (mbar_try(smem_u32(&bar_full[s]), issued_phase[s])) break;
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer ----------------
+      constexpr uint32_t idesc = make_idesc(TR::kFmt, tc::BM, tc::BN);
+      bool ok = true;
+      uint32_t g = 0, tl = 0;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tl) {
+        const TileInfo ti = persist_tile(p, t);
+        const int a = tl & 1;
+        const uint32_t v = tl >> 1;
+        if (tl >= 2 && !mbar_wait(smem_u32(&bar_tempty[a]), (v - 1) & 1, &s_abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc_hh = tmem + a * 256, acc_x = tmem + a * 256 + tc::BN;
+        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+          const int s = g % tc::ST;
+          if (!mbar_wait(smem_u32(&bar_full[s]), (g / tc::ST) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + s * tc::STAGE_BYTES;
+          const uint64_t d_ahi = sw128_desc(st + 0 * tc::TILE_BYTES);
+          const uint64_t d_alo = sw128_desc(st + 1 * tc::TILE_BYTES);
+          const uint64_t d_bhi = sw128_desc(st + 2 * tc::TILE_BYTES);
+          const uint64_t d_blo = sw128_desc(st + 3 * tc::TILE_BYTES);
+#pragma unroll
+          for (int kk = 0; kk < tc::BK / tc::UK; ++kk) {
+            const uint64_t off = (uint64_t)((kk * tc::UK * 2) >> 4);
+            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+            umma_f16(acc_hh, d_ahi + off, d_bhi + off, idesc, acc);
+            umma_f16(acc_x, d_ahi + off, d_blo + off, idesc, acc);
+            umma_f16(acc_x, d_alo + off, d_bhi + off, idesc, 1u);
+          }
+          umma_commit(smem_u32(&bar_empty[s]));
+        }
+        if (!ok) break;
+        umma_commit(smem_u32(&bar_tfull[a]));  // accumulators of this tile are complete
+      }
+      // every MMA issued by this thread has retired once this arrives
+      umma_commit(smem_u32(&bar_final));
+      for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try(smem_u32(&bar_final), 0)) break;
+      if (!ok) s_abort = 1;
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (8 warps) ----------------
+    const int q = warp & 3;             // TMEM lane quarter of this warp
+    const int half = (warp - 2) >> 2;   // 64-column half of the tile
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const int ld = p.ld;
+    uint32_t tl = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
+      const TileInfo ti = persist_tile(p, t);
+      const int a = tl & 1;
+      if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
+      tc_fence_after();
+      if (ti.ok) {
+        const int r = ti.i0 + q * 32 + lane;  // row inside the part
+        const size_t base = (size_t)ti.row0 * ld;
+        const T* Ehi = (const T*)p.E + base;
+        const T* Elo = (const T*)p.E_lo + base;
+        T* Ohi = p.out ? (T*)p.out + base : nullptr;
+        T* Olo = p.out ? (T*)p.out_lo + base : nullptr;
+#pragma unroll 1
+        for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
+          const int cl = half * 64 + cc * tcp::CHUNK;
+          uint32_t hh[16], xx[16];
+          tmem_ld16(tmem + lane_base + a * 256 + cl, hh);
+          tmem_ld16(tmem + lane_base + a * 256 + tc::BN + cl, xx);
+          tmem_wait_ld();
+          const int c0 = ti.j0 + cl;
+          alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
+          {
+            const uint4* sh = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0);
+            const uint4* sl = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0);
+            uint4* dh = reinterpret_cast<uint4*>(ehi);
+            uint4* dl = reinterpret_cast<uint4*>(elo);
+            dh[0] = sh[0];
+            dh[1] = sh[1];
+            dl[0] = sl[0];
+            dl[1] = sl[1];
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + j;
+            const double P =
+                (double)__uint_as_float(hh[j]) + TR::kInv * (double)__uint_as_float(xx[j]);
+            const double x = TR::to_d(ehi[j]) + TR::kInv * TR::to_d(elo[j]);
+            const double val = alpha * P + beta * x;
+            const T h = TR::from_d(val);
+            const T l = TR::from_d((val - TR::to_d(h)) * TR::kScale);
+            const double vs = TR::to_d(h) + TR::kInv * TR::to_d(l);
+            nhi[j] = h;
+            nlo[j] = l;
+            const int w = sym_weight(ti.diag, r, c);
+            const double dres = x - P;
+            sums[0] += w * vs * vs;
+            sums[2] += core_weight(w, r, c, ti.core) * dres * dres;
+            if (r == c) {
+              sums[1] += vs;
+              sums[3] += P;
+            }
+            if (Ohi && w && r != c) {
+              Ohi[(size_t)c * ld + r] = h;
+              Olo[(size_t)c * ld + r] = l;
+            }
+          }
+          if (Ohi) {
+            if (!ti.diag) {
+              uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * ld + c0);
+              uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * ld + c0);
+              const uint4* sh = reinterpret_cast<const uint4*>(nhi);
+              const uint4* sl = reinterpret_cast<const uint4*>(nlo);
+              dh[0] = sh[0];
+              dh[1] = sh[1];
+              dl[0] = sl[0];
+              dl[1] = sl[1];
+            } else {
+              for (int j = 0; j < 16; ++j)
+                if (r <= c0 + j) {
+                  Ohi[(size_t)r * ld + c0 + j] = nhi[j];
+                  Olo[(size_t)r * ld + c0 + j] = nlo[j];
+                }
+            }
+          }
+        }
+      }
+      tc_fence_before();  // our TMEM reads are ordered before the release below
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tmem_dealloc(tmem, tcp::TMEM_COLS);
+  if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+  if (p.out) __threadfence();
+  publish_and_finalize(p, sums, red, &s_flag);
+}
+
+// ---------------------------------------------------------------------------------
 // Elementwise kernels of the split path
 // ---------------------------------------------------------------------------------
 template <typename T>
@@ -517,23 +801,53 @@ static cudaError_t launch_tc(const StepArgs& a, long long rows, dim3 grid, float
   return cudaGetLastError();
 }
 
+static int num_sms() {
+  static int sms = 0;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+      sms = v;
+    if (sms <= 0) sms = 148;
+  });
+  return sms;
+}
+
+template <typename T>
+static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles, cudaStream_t st) {
+  const bool bf16 = std::is_same<T, __nv_bfloat16>::value;
+  CUtensorMap m[2];
+  if (!make_tmap(&m[0], a.A, rows, a.ld, a.ld, bf16) || !make_tmap(&m[1], a.A_lo, rows, a.ld, a.ld, bf16))
+    return cudaErrorInvalidValue;
+  auto kern = k_tc_persist<T>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  const int grid = std::min(ntiles, num_sms());
+  kern<<<grid, tcp::NTHR, tc::SMEM_BYTES, st>>>(m[0], m[1], a, ntiles);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// Symmetric launches: A = B (the iterate), so one pair of tensor maps serves both.
 cudaError_t launch_sym_gemm_tc(const StepArgs& a0, int bf16, cudaStream_t st) {
-  if (a0.np % tc::BM != 0) return cudaErrorInvalidValue;
+  if (a0.np % tc::BM != 0 || a0.A != a0.B || a0.A_lo != a0.B_lo) return cudaErrorInvalidValue;
   StepArgs a = a0;
   a.tiles = nullptr;
   a.ld = a.np;
-  dim3 grid(tc_ntiles(a.np));
-  return bf16 ? launch_tc<__nv_bfloat16, true>(a, a.np, grid, nullptr, 0, st)
-              : launch_tc<__half, true>(a, a.np, grid, nullptr, 0, st);
+  const int nt = tc_ntiles(a.np);
+  return bf16 ? launch_persist<__nv_bfloat16>(a, a.np, nt, st)
+              : launch_persist<__half>(a, a.np, nt, st);
 }
 
 cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,
                                        cudaStream_t st) {
-  if (!a.tiles || a.ntiles <= 0 || a.ld % tc::BM != 0 || rows % tc::BM != 0)
+  if (!a.tiles || a.ntiles <= 0 || a.ld % tc::BM != 0 || rows % tc::BM != 0 || a.A != a.B ||
+      a.A_lo != a.B_lo)
     return cudaErrorInvalidValue;
-  dim3 grid(a.ntiles);
-  return bf16 ? launch_tc<__nv_bfloat16, true>(a, rows, grid, nullptr, 0, st)
-              : launch_tc<__half, true>(a, rows, grid, nullptr, 0, st);
+  return bf16 ? launch_persist<__nv_bfloat16>(a, rows, a.ntiles, st)
+              : launch_persist<__half>(a, rows, a.ntiles, st);
 }
 
 cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,
