@@ -35,6 +35,8 @@ struct SplitTraits<__half> {
   static constexpr double kScale = 2048.0, kInv = 1.0 / 2048.0;
   __device__ static double to_d(__half h) { return (double)__half2float(h); }
   __device__ static __half from_d(double v) { return __double2half(v); }
+  __device__ static float to_f(__half h) { return __half2float(h); }
+  __device__ static __half from_f(float v) { return __float2half_rn(v); }
 };
 template <>
 struct SplitTraits<__nv_bfloat16> {
@@ -42,6 +44,8 @@ struct SplitTraits<__nv_bfloat16> {
   static constexpr double kScale = 256.0, kInv = 1.0 / 256.0;
   __device__ static double to_d(__nv_bfloat16 h) { return (double)__bfloat162float(h); }
   __device__ static __nv_bfloat16 from_d(double v) { return __double2bfloat16(v); }
+  __device__ static float to_f(__nv_bfloat16 h) { return __bfloat162float(h); }
+  __device__ static __nv_bfloat16 from_f(float v) { return __float2bfloat16_rn(v); }
 };
 
 // ---------------------------------------------------------------------------------
@@ -595,25 +599,29 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
             dl[0] = sl[0];
             dl[1] = sl[1];
           }
+          // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
+          // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
+          // (or 2 x 8) bits; only the sums that drive the branch rule are FP64.
+          const float kInvF = (float)TR::kInv, kScaleF = (float)TR::kScale;
+          const float af = (float)alpha, bf = (float)beta;  // 1/0 or -1/2: exact
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int c = c0 + j;
-            const double P =
-                (double)__uint_as_float(hh[j]) + TR::kInv * (double)__uint_as_float(xx[j]);
-            const double x = TR::to_d(ehi[j]) + TR::kInv * TR::to_d(elo[j]);
-            const double val = alpha * P + beta * x;
-            const T h = TR::from_d(val);
-            const T l = TR::from_d((val - TR::to_d(h)) * TR::kScale);
-            const double vs = TR::to_d(h) + TR::kInv * TR::to_d(l);
+            const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
+            const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
+            const float val = fmaf(af, P, bf * x);
+            const T h = TR::from_f(val);
+            const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
+            const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
             nhi[j] = h;
             nlo[j] = l;
             const int w = sym_weight(ti.diag, r, c);
-            const double dres = x - P;
-            sums[0] += w * vs * vs;
-            sums[2] += core_weight(w, r, c, ti.core) * dres * dres;
+            const double dres = (double)x - (double)P;
+            sums[0] = fma((double)w * vs, vs, sums[0]);
+            sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
             if (r == c) {
               sums[1] += vs;
-              sums[3] += P;
+              sums[3] += (double)P;
             }
             if (Ohi && w && r != c) {
               Ohi[(size_t)c * ld + r] = h;
