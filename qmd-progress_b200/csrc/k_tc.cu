@@ -616,12 +616,15 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
             nhi[j] = h;
             nlo[j] = l;
             const int w = sym_weight(ti.diag, r, c);
-            const double dres = (double)x - (double)P;
+            // the residual X - X^2 (vv) needs the product at accumulator precision
+            const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
+                                  (double)__uint_as_float(hh[j]));
+            const double dres = (double)x - Pd;
             sums[0] = fma((double)w * vs, vs, sums[0]);
             sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
             if (r == c) {
               sums[1] += vs;
-              sums[3] += (double)P;
+              sums[3] += Pd;
             }
             if (Ohi && w && r != c) {
               Ohi[(size_t)c * ld + r] = h;
