@@ -94,7 +94,10 @@ def test_poly512_subgraph_matches_fixture(cuda, poly512, prec):
     cols = d["sample_cols"]
     atol = 1e-10 if prec == sp2b.PREC_FP64 else 1e-5
     assert np.allclose(rho[:, cols], d["sg_rho_cols"], rtol=0, atol=atol)
-    assert np.allclose(vv, d["sg_vv"], rtol=1e-8 if prec == sp2b.PREC_FP64 else 1e-3, atol=atol)
+    # vv = ||X - X^2||_F per step; in the split form it bottoms out at the noise floor
+    # of the 2 x 11-bit iterate (~1e-5 summed over all core rows here)
+    assert np.allclose(vv, d["sg_vv"], rtol=1e-8 if prec == sp2b.PREC_FP64 else 1e-3,
+                       atol=atol if prec == sp2b.PREC_FP64 else 5e-5)
     assert abs(np.trace(rho) - float(d["sg_trace"])) < (1e-8 if prec == sp2b.PREC_FP64 else 1e-2)
     half = rho / 2
     idem = np.linalg.norm(half @ half - half)       # prg_check_idempotency of rho/2
