@@ -46,8 +46,9 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="two_band", choices=["two_band", "subgraph"],
-                    help="two_band: dense config (default); subgraph: 32^3 lattice, 256 parts")
+    ap.add_argument("--workload", default="two_band", choices=["two_band", "subgraph", "cubic_dense"],
+                    help="two_band: dense config (default); subgraph: 32^3 lattice, 256 parts; "
+                         "cubic_dense: the 32^3 lattice solved densely (N=32768)")
     ap.add_argument("--L", type=int, default=32, help="subgraph: lattice edge")
     ap.add_argument("--parts", type=int, default=256, help="subgraph: number of parts")
     return ap.parse_args()
@@ -186,6 +187,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "subgraph":
         return run_subgraph(args, rank, world, local)
+    if args.workload == "cubic_dense":
+        return run_cubic_dense(args, rank, local)
 
     import numpy as np
     import torch
@@ -473,6 +476,66 @@ def run_subgraph(args, rank, world, local):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_cubic_dense(args, rank, local):
+    """Dense mixed SP2 of the L^3 lattice Hamiltonian (N = L^3), FP64 solve beside it."""
+    import numpy as np
+    import torch
+    from sp2b import _lib, modelham as M
+    torch.cuda.set_device(local)
+    L = args.L
+    n = L ** 3
+    rp, col, val = M.cubic_3d_csr(L, seed=rank, threshold=1e-5)
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    h = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    h[torch.from_numpy(rows).cuda(), torch.from_numpy(col.astype(np.int64)).cuda()] = \
+        torch.from_numpy(val).cuda()
+    rho = torch.empty_like(h)
+    pp = np.zeros(130, dtype=np.int32)
+    vv = np.zeros(130)
+    ic = C.c_int(0)
+    Lb = _lib.lib()
+    stream = torch.cuda.current_stream()
+
+    def solve(prec):
+        o = _lib.make_opts(precision=prec, device_ptrs=True, stream=stream.cuda_stream)
+        _lib.check(Lb.sp2b_sp2_alg2_genseq(h.data_ptr(), rho.data_ptr(), n, 0.0, 0.5, 0, 120, b"None",
+                                           1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
+                                           C.byref(o)), "genseq")
+        return ic.value
+
+    prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
+            "fp64": _lib.PREC_FP64}[args.precision]
+    for _ in range(args.warmup):
+        solve(prec)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            iters = solve(prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / args.steps
+    rho_m = rho.clone()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    it64 = solve(_lib.PREC_FP64)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t64 = f0.elapsed_time(f1)
+    err = float((rho_m - rho).norm().item())
+    out = {"metric": f"dense SP2 solves/s ({L}^3 lattice, N={n})", "value": 1e3 / t,
+           "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": args.precision, "data": "synthetic",
+           "config": {"workload": f"cubic{L}_dense_{args.precision}", "n": n, "sp2_iters": iters},
+           "tflops": (2.0 * n ** 3 * iters + 4.0 * n ** 3) / (t / 1e3) / 1e12,
+           "fp64": {"ms_per_solve": t64, "iters": it64, "solves_per_s": 1e3 / t64},
+           "err_vs_fp64": {"fro_over_n": err / n, "rel_fro": err / float(rho.norm().item())},
+           "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":

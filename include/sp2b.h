@@ -226,6 +226,12 @@ int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, doubl
  * the device time of the SP2 step kernels recorded with CUDA events when
  * sp2b_set_step_timing(1) is on (ms, number of timed launches). */
 long long sp2b_launch_count(void);
+
+/* Failure-path self-test (no counterpart in the reference): runs the library's bounded
+ * device wait on a barrier that nothing arrives at, limited to spin_limit polls.
+ * Returns SP2B_TIMEOUT when the wait ran out and the kernel returned normally, which
+ * is the expected outcome; the device stays usable. */
+int sp2b_selftest_wait_timeout(int spin_limit);
 int sp2b_set_step_timing(int enable);
 int sp2b_step_timing(double* ms, long long* launches);
 

@@ -72,15 +72,19 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up (returns false and raises the CTA abort flag) after
-// kSpinLimit polls, or early once another thread of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+// Bounded wait: gives up (returns false and raises the CTA abort flag) after `limit`
+// polls, or early once another thread of the CTA has aborted.
+__device__ __forceinline__ bool mbar_wait_limit(uint32_t a, uint32_t parity,
+                                                volatile int* abort_flag, uint32_t limit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_try(a, parity)) return true;
     if ((i & 255u) == 255u && *abort_flag) return false;
   }
   *abort_flag = 1;
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
+  return mbar_wait_limit(a, parity, abort_flag, kSpinLimit);
 }
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
                                             int x, int y) {
@@ -662,6 +666,29 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
   if (p.out) __threadfence();
   publish_and_finalize(p, sums, red, &s_flag);
+}
+
+// Failure-path self-test: every thread waits, with the same bounded wait the step
+// kernels use, on an mbarrier that nothing ever arrives at.  The wait runs out after
+// `limit` polls, the kernel records SP2B_TIMEOUT and returns normally.
+__global__ void k_wait_selftest(uint32_t limit, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ volatile int abort_flag;
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    mbar_init(smem_u32(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_limit(smem_u32(&bar), 0, &abort_flag, limit);
+  __syncthreads();
+  if (!ok && threadIdx.x == 0) atomicExch(err, SP2B_TIMEOUT);
+}
+
+cudaError_t launch_wait_selftest(uint32_t limit, int* err, cudaStream_t st) {
+  k_wait_selftest<<<1, 64, 0, st>>>(limit, err);
+  note_launch();
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------

@@ -83,6 +83,7 @@ cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf
                                        cudaStream_t st);
 cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int bf16,
                                 double* x, cudaStream_t st);
+cudaError_t launch_wait_selftest(uint32_t limit, int* err, cudaStream_t st);
 cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
                                 cudaStream_t st);
 cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,

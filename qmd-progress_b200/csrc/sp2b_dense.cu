@@ -672,6 +672,27 @@ int sp2b_check_idempotency(const double* a, int n, double threshold, double* ide
   return SP2B_OK;
 }
 
+int sp2b_selftest_wait_timeout(int spin_limit) {
+  if (spin_limit < 1) {
+    set_last_error("spin_limit must be positive");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), c->stream));
+  SP2B_CUDA_TRY(launch_wait_selftest((uint32_t)spin_limit, c->err, c->stream));
+  int herr = 0;
+  SP2B_CUDA_TRY(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (herr != 0) {
+    set_last_error("self-test: a bounded device wait ran out after %d polls", spin_limit);
+    return SP2B_TIMEOUT;
+  }
+  return SP2B_OK;
+}
+
 long long sp2b_launch_count(void) { return g_launches.load(); }
 
 int sp2b_set_step_timing(int enable) {

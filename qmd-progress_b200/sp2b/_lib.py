@@ -80,6 +80,7 @@ _SIGS = {
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
+    "sp2b_selftest_wait_timeout": (_i, [_i]),
     "sp2b_set_step_timing": (_i, [_i]),
     "sp2b_step_timing": (_i, [_dp, _llp]),
     # PROGRESS-named exports

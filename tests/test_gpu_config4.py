@@ -1,0 +1,78 @@
+"""Large dense mixed-precision SP2 on the 3D lattice Hamiltonian (no partitioning).
+
+N = 32768 (32^3 sites, dense FP64 H of 8.6 GB on the device): FP16 hi+lo tcgen05
+products, FP64 traces, FP64 McWeeny step, against the FP64 GPU SP2 of the same H
+(itself checked against the eigendecomposition on the smaller lattice below).  The
+lattice is nearly gapless, so SP2 needs ~50 steps and amplifies rounding by roughly
+1/gap; the bounds below are what the 2 x 11-bit split reaches on it.
+At 16^3 (4096) both forms are compared with numpy eigh (prg_build_density_T0) on 8
+random columns.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import sp2_oracle as O
+from sp2b import _lib, modelham as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense_on_device(torch, L, seed=0):
+    rp, col, val = M.cubic_3d_csr(L, seed=seed, threshold=1e-5)
+    n = L ** 3
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    h = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+    h[torch.from_numpy(rows).cuda(), torch.from_numpy(col.astype(np.int64)).cuda()] = \
+        torch.from_numpy(val).cuda()
+    return h
+
+
+def _genseq(torch, h, prec):
+    n = h.shape[0]
+    rho = torch.empty_like(h)
+    pp = np.zeros(130, dtype=np.int32)
+    vv = np.zeros(130)
+    ic = C.c_int(0)
+    o = _lib.make_opts(precision=prec, device_ptrs=True,
+                       stream=torch.cuda.current_stream().cuda_stream)
+    _lib.check(_lib.lib().sp2b_sp2_alg2_genseq(h.data_ptr(), rho.data_ptr(), n, 0.0, 0.5, 0, 120,
+                                                b"None", 1e-10, pp.ctypes.data, C.byref(ic),
+                                                vv.ctypes.data, 0, C.byref(o)), "genseq")
+    return rho, [int(x) for x in pp[:ic.value]]
+
+
+def test_cubic16_columns_against_eigh(cuda):
+    torch = cuda
+    L = 16
+    n = L ** 3
+    h = _dense_on_device(torch, L)
+    d_ref, _ = O.build_density_t0(h.cpu().numpy(), 0.5)
+    rng = np.random.default_rng(0)
+    cols = rng.choice(n, 8, replace=False)
+    for prec, tol in [(_lib.PREC_FP64, 1e-9), (_lib.PREC_MIXED_FP16, 1e-4)]:
+        rho, pp = _genseq(torch, h, prec)
+        got = rho[:, torch.from_numpy(cols).cuda()].cpu().numpy()
+        err = np.linalg.norm(got - d_ref[:, cols]) / np.linalg.norm(d_ref[:, cols])
+        assert err <= tol, (prec, err)
+
+
+def test_cubic32_dense_mixed_against_fp64(cuda):
+    torch = cuda
+    L = 32
+    n = L ** 3
+    h = _dense_on_device(torch, L)
+    rho_m, pp_m = _genseq(torch, h, _lib.PREC_MIXED_FP16)
+    tr_m = float(torch.trace(rho_m).item())
+    rho_f, pp_f = _genseq(torch, h, _lib.PREC_FP64)
+    k = min(len(pp_m), len(pp_f))
+    assert pp_m[:k] == pp_f[:k]
+    assert abs(float(torch.trace(rho_f).item()) - n) < 1e-6 * n
+    assert abs(tr_m - n) < 1e-3 * n
+    diff = rho_m.sub_(rho_f)
+    err_over_n = float(diff.norm().item()) / n
+    rel = float(diff.norm().item() / rho_f.norm().item())
+    print(f"config4: {len(pp_m)} mixed / {len(pp_f)} FP64 steps, ||dD||_F/N = {err_over_n:.3e}, "
+          f"relative {rel:.3e}")
+    assert err_over_n <= 1e-5

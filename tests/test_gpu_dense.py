@@ -211,3 +211,14 @@ def test_dev_sym_gemm_f32(cuda):
         ref = a.double() @ b.double()
         err = ((c.double() - ref).norm() / ref.norm()).item()
         assert err < 2e-6, (n, err)
+
+
+def test_bounded_device_wait_times_out_and_device_stays_usable(cuda):
+    """Failure detection without a fault: a wait on a flag nothing sets runs out."""
+    L = _lib.lib()
+    assert L.sp2b_selftest_wait_timeout(4096) == _lib.SP2B_TIMEOUT
+    assert "ran out" in _lib.last_error()
+    h = M.two_band_1d(256, seed=3)
+    ok = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
+    ref = O.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10)
+    assert np.linalg.norm(ok.rho - ref.rho) / 256 <= 1e-6
