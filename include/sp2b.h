@@ -39,6 +39,12 @@ extern "C" {
                                    FP64 traces, final FP64 McWeeny step */
 #define SP2B_PREC_MIXED_BF16 2  /* same with BF16 hi+lo operands */
 
+/* Products of the McWeeny refinement that ends a mixed solve. */
+#define SP2B_MCW_INT8 0  /* X^2 exact from INT8 residue products (tcgen05 kind::i8) and CRT,
+                            rounded to 2^-S with S ~ 35; correction X (X^2 - X) split
+                            precision.  Used for mcweeny = 1 (default). */
+#define SP2B_MCW_FP64 1  /* both products FP64 (DMMA).  Always used for mcweeny > 1. */
+
 typedef struct sp2b_opts {
   int precision;     /* SP2B_PREC_* (default FP64) */
   int mcweeny;       /* mixed only: FP64 McWeeny steps after the loop (default 1) */
@@ -46,6 +52,7 @@ typedef struct sp2b_opts {
   int device_ptrs;   /* 1: matrix arguments are device pointers */
   void* stream;      /* cudaStream_t to run on (NULL: the per-library stream) */
   int verbose;
+  int mcweeny_products; /* mixed only: SP2B_MCW_* (default SP2B_MCW_INT8) */
 } sp2b_opts;
 
 /* Fill opts with defaults (FP64, host pointers). */
@@ -226,6 +233,11 @@ int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, doubl
  * the device time of the SP2 step kernels recorded with CUDA events when
  * sp2b_set_step_timing(1) is on (ms, number of timed launches). */
 long long sp2b_launch_count(void);
+
+/* Scale exponent S and largest squared row norm of X of the last INT8 McWeeny
+ * refinement on the current device (the residue products are exact for
+ * (2^S sqrt(r2max) + sqrt(np)/2)^2 < prod(moduli)/2). */
+int sp2b_last_refinement_info(int* scale_exp, double* r2max);
 
 /* Failure-path self-test (no counterpart in the reference): runs the library's bounded
  * device wait on a barrier that nothing arrives at, limited to spin_limit polls.

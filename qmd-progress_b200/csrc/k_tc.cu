@@ -13,6 +13,7 @@
 #include <mutex>
 
 #include "reduce.cuh"
+#include "tc_ptx.cuh"
 
 namespace sp2b {
 namespace tc {
@@ -47,116 +48,6 @@ struct SplitTraits<__nv_bfloat16> {
   __device__ static float to_f(__nv_bfloat16 h) { return __bfloat162float(h); }
   __device__ static __nv_bfloat16 from_f(float v) { return __float2bfloat16_rn(v); }
 };
-
-// ---------------------------------------------------------------------------------
-// PTX wrappers
-// ---------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t cnt) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(cnt) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: gives up (returns false and raises the CTA abort flag) after `limit`
-// polls, or early once another thread of the CTA has aborted.
-__device__ __forceinline__ bool mbar_wait_limit(uint32_t a, uint32_t parity,
-                                                volatile int* abort_flag, uint32_t limit) {
-  for (uint32_t i = 0; i < limit; ++i) {
-    if (mbar_try(a, parity)) return true;
-    if ((i & 255u) == 255u && *abort_flag) return false;
-  }
-  *abort_flag = 1;
-  return false;
-}
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
-  return mbar_wait_limit(a, parity, abort_flag, kSpinLimit);
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
-                                            int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(mbar), "r"(x), "r"(y)
-      : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
-               "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   mbar)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-        "=r"(v[31])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// K-major operand tile, 128-byte swizzle, 8-row groups 1024 bytes apart (SBO), LBO
-// unused for swizzled K-major (1), descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(1024u >> 4) << 32;
-  d |= (uint64_t)1u << 46;
-  d |= (uint64_t)2u << 61;
-  return d;
-}
-// kind::f16 instruction descriptor: FP32 accumulate, A/B K-major, M x N.
-__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, int M, int N) {
-  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
 
 // ---------------------------------------------------------------------------------
 // The kernel.  SYM: one CTA per upper 128x128 tile with the SP2 epilogue.
@@ -394,19 +285,6 @@ constexpr int TMEM_COLS = 512;
 constexpr int CHUNK = 16;  // columns per tcgen05.ld
 }  // namespace tcp
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t a) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
-}
-
 struct TileInfo {
   int row0, i0, j0, kb, core;
   bool ok, diag;
@@ -436,10 +314,14 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
   return ti;
 }
 
-template <typename T>
+// EPI 0: SP2 step epilogue (A = B = E = X_k).  EPI 1: McWeeny combine of the INT8
+// refinement, D = 2 X^2 - acc with acc = X (4R) (A = X, B = 4R = 4(X^2 - X), E = X^2 in
+// FP64), written to the n_out x n_out density (row pitch ld_out) and mirrored.
+template <typename T, int EPI>
 __global__ void __launch_bounds__(tcp::NTHR, 1)
     k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
-                 const StepArgs p, int ntiles) {
+                 const __grid_constant__ CUtensorMap tm_bhi,
+                 const __grid_constant__ CUtensorMap tm_blo, const StepArgs p, int ntiles) {
   using TR = SplitTraits<T>;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[tc::ST];
@@ -504,8 +386,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
           mbar_expect_tx(fb, tc::STAGE_BYTES);
           tma_load_2d(st + 0 * tc::TILE_BYTES, &tm_hi, fb, kb * tc::BK, ti.row0 + ti.i0);
           tma_load_2d(st + 1 * tc::TILE_BYTES, &tm_lo, fb, kb * tc::BK, ti.row0 + ti.i0);
-          tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_hi, fb, kb * tc::BK, ti.row0 + ti.j0);
-          tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_lo, fb, kb * tc::BK, ti.row0 + ti.j0);
+          tma_load_2d(st + 2 * tc::TILE_BYTES, &tm_bhi, fb, kb * tc::BK, ti.row0 + ti.j0);
+          tma_load_2d(st + 3 * tc::TILE_BYTES, &tm_blo, fb, kb * tc::BK, ti.row0 + ti.j0);
           issued_phase[s] = u & 1;
         }
       }
@@ -577,7 +459,7 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       const int a = tl & 1;
       if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
-      if (ti.ok) {
+      if (EPI == 0 && ti.ok) {
         const int r = ti.i0 + q * 32 + lane;  // row inside the part
         const size_t base = (size_t)ti.row0 * ld;
         const T* Ehi = (const T*)p.E + base;
@@ -651,6 +533,45 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
                   Ohi[(size_t)r * ld + c0 + j] = nhi[j];
                   Olo[(size_t)r * ld + c0 + j] = nlo[j];
                 }
+            }
+          }
+        }
+      }
+      if (EPI == 1 && ti.ok) {
+        // D = 2 X^2 - X (4R): X^2 exact to the INT8 refinement's grid (FP64), the
+        // correction X (4R) small, so its split-precision product is far below it.
+        const int r = ti.i0 + q * 32 + lane;
+        const double* X2 = (const double*)p.E;
+        double* D = (double*)p.out;
+        const int nout = p.n_out, ldo = p.ld_out;
+#pragma unroll 1
+        for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
+          const int cl = half * 64 + cc * tcp::CHUNK;
+          uint32_t hh[16], xx[16];
+          tmem_ld16(tmem + lane_base + a * 256 + cl, hh);
+          tmem_ld16(tmem + lane_base + a * 256 + tc::BN + cl, xx);
+          tmem_wait_ld();
+          const int c0 = ti.j0 + cl;
+          double x2[16];
+          const double2* src = reinterpret_cast<const double2*>(X2 + (size_t)r * ld + c0);
+#pragma unroll
+          for (int h2 = 0; h2 < 8; ++h2) {
+            const double2 v2 = src[h2];
+            x2[2 * h2] = v2.x;
+            x2[2 * h2 + 1] = v2.y;
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + j;
+            const double acc = fma(TR::kInv, (double)__uint_as_float(xx[j]),
+                                   (double)__uint_as_float(hh[j]));
+            const double d = 2.0 * x2[j] - acc;
+            const int w = sym_weight(ti.diag, r, c);
+            if (w && r < nout && c < nout) {
+              D[(size_t)r * ldo + c] = d;
+              if (r != c) D[(size_t)c * ldo + r] = d;
+              sums[0] = fma((double)w * d, d, sums[0]);
+              if (r == c) sums[1] += d;
             }
           }
         }
@@ -785,36 +706,6 @@ __global__ void k_f32_to_split(const float* __restrict__ a, int n, int np, __hal
 // ---------------------------------------------------------------------------------
 // Host side: tensor maps and launches
 // ---------------------------------------------------------------------------------
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    cudaDriverEntryPointQueryResult q;
-    void* ptr = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-  });
-  return fn;
-}
-
-// rows x cols (cols contiguous, row pitch ld elements) 16-bit matrix; box 64 x 128.
-static bool make_tmap(CUtensorMap* tm, const void* base, long long rows, long long cols,
-                      long long ld, bool bf16) {
-  auto fn = encode_fn();
-  if (!fn) return false;
-  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
-  cuuint32_t es[2] = {1, 1};
-  CUresult r = fn(tm, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
-                  const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS;
-}
-
 int tc_ntiles(int np) {
   const int t = np / tc::BM;
   return t * (t + 1) / 2;
@@ -852,18 +743,25 @@ static int num_sms() {
   return sms;
 }
 
-template <typename T>
+template <typename T, int EPI>
 static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles, cudaStream_t st) {
   const bool bf16 = std::is_same<T, __nv_bfloat16>::value;
-  CUtensorMap m[2];
+  CUtensorMap m[4];
   if (!make_tmap(&m[0], a.A, rows, a.ld, a.ld, bf16) || !make_tmap(&m[1], a.A_lo, rows, a.ld, a.ld, bf16))
     return cudaErrorInvalidValue;
-  auto kern = k_tc_persist<T>;
+  if (a.B == a.A && a.B_lo == a.A_lo) {
+    m[2] = m[0];
+    m[3] = m[1];
+  } else if (!make_tmap(&m[2], a.B, rows, a.ld, a.ld, bf16) ||
+             !make_tmap(&m[3], a.B_lo, rows, a.ld, a.ld, bf16)) {
+    return cudaErrorInvalidValue;
+  }
+  auto kern = k_tc_persist<T, EPI>;
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   const int grid = std::min(ntiles, num_sms());
-  kern<<<grid, tcp::NTHR, tc::SMEM_BYTES, st>>>(m[0], m[1], a, ntiles);
+  kern<<<grid, tcp::NTHR, tc::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
   note_launch();
   return cudaGetLastError();
 }
@@ -875,8 +773,8 @@ cudaError_t launch_sym_gemm_tc(const StepArgs& a0, int bf16, cudaStream_t st) {
   a.tiles = nullptr;
   a.ld = a.np;
   const int nt = tc_ntiles(a.np);
-  return bf16 ? launch_persist<__nv_bfloat16>(a, a.np, nt, st)
-              : launch_persist<__half>(a, a.np, nt, st);
+  return bf16 ? launch_persist<__nv_bfloat16, 0>(a, a.np, nt, st)
+              : launch_persist<__half, 0>(a, a.np, nt, st);
 }
 
 cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,
@@ -884,8 +782,35 @@ cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf
   if (!a.tiles || a.ntiles <= 0 || a.ld % tc::BM != 0 || rows % tc::BM != 0 || a.A != a.B ||
       a.A_lo != a.B_lo)
     return cudaErrorInvalidValue;
-  return bf16 ? launch_persist<__nv_bfloat16>(a, rows, a.ntiles, st)
-              : launch_persist<__half>(a, rows, a.ntiles, st);
+  return bf16 ? launch_persist<__nv_bfloat16, 0>(a, rows, a.ntiles, st)
+              : launch_persist<__half, 0>(a, rows, a.ntiles, st);
+}
+
+// McWeeny combine of the INT8 refinement: D = 2 X^2 - X (4R), upper tiles, mirrored.
+cudaError_t launch_mcweeny_tc(const __half* xhi, const __half* xlo, const __half* rhi,
+                              const __half* rlo, const double* x2, int np, int bf16, double* d,
+                              int n, int ldd, double* partials, unsigned* counter,
+                              double* sums_out, int* err, cudaStream_t st) {
+  if (np % tc::BM != 0 || n > np) return cudaErrorInvalidValue;
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.A = xhi;
+  a.A_lo = xlo;
+  a.B = rhi;
+  a.B_lo = rlo;
+  a.E = x2;
+  a.out = d;
+  a.np = np;
+  a.ld = np;
+  a.n_out = n;
+  a.ld_out = ldd;
+  a.partials = partials;
+  a.counter = counter;
+  a.sums_out = sums_out;
+  a.err = err;
+  const int nt = tc_ntiles(np);
+  return bf16 ? launch_persist<__nv_bfloat16, 1>(a, np, nt, st)
+              : launch_persist<__half, 1>(a, np, nt, st);
 }
 
 cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,

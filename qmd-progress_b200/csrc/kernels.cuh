@@ -1,5 +1,7 @@
 // Launch interfaces shared by the sp2b translation units.
 #pragma once
+#include <vector>
+
 #include "sp2b_common.cuh"
 
 namespace sp2b {
@@ -53,6 +55,7 @@ struct StepArgs {
   unsigned* counter;
   double* sums_out;     // non-control: the 4 totals {||out||^2, Tr out, ||E-acc||^2, Tr acc}
   int* err;             // device error word (timeouts)
+  int n_out, ld_out;    // McWeeny combine: the n_out x n_out density and its row pitch
 };
 
 // FP64 path ---------------------------------------------------------------------------
@@ -86,6 +89,22 @@ cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int 
 cudaError_t launch_wait_selftest(uint32_t limit, int* err, cudaStream_t st);
 cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
                                 cudaStream_t st);
+cudaError_t launch_mcweeny_tc(const __half* xhi, const __half* xlo, const __half* rhi,
+                              const __half* rlo, const double* x2, int np, int bf16, double* d,
+                              int n, int ldd, double* partials, unsigned* counter,
+                              double* sums_out, int* err, cudaStream_t st);
+
+// INT8 (Ozaki residue) refinement products -------------------------------------------
+int oz_nmod();
+size_t oz_scale_bytes();
+void oz_tile_list(int np, std::vector<int2>& out);
+cudaError_t launch_oz_products(const __half* xhi, const __half* xlo, int np, int bf16,
+                               void* scale, int8_t* res, uint8_t* qout, const int2* tiles,
+                               int ntiles, int* err, cudaStream_t st);
+cudaError_t launch_oz_crt(const uint8_t* q, const __half* xhi, const __half* xlo, int np,
+                          int bf16, const void* scale, double* x2, __half* rhi, __half* rlo,
+                          cudaStream_t st);
+cudaError_t oz_read_scale(const void* scale, int* S, double* r2max, cudaStream_t st);
 cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* bhi,
                             const __half* blo, int np, float* c, int n, cudaStream_t st,
                             int* err);

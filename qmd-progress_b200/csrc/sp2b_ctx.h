@@ -40,12 +40,22 @@ struct Ctx {
   SolveOut* sout = nullptr;
   SolveOut* h_sout = nullptr;   // pinned
   int* err = nullptr;
+  // INT8 refinement: residue planes, reduced product planes, tile list, scale state
+  int8_t* oz_res = nullptr;
+  uint8_t* oz_q = nullptr;
+  size_t oz_cap = 0;
+  int2* oz_tiles = nullptr;
+  int oz_tiles_np = 0, oz_ntiles = 0;
+  void* oz_scale = nullptr;
+  int oz_last_S = 0;            // scale exponent of the last INT8 refinement
+  double oz_last_r2max = 0.0;   // its largest squared row norm
   int last_launches = 0;            // SP2 step launches of the last dense solve
   std::vector<cudaEvent_t> ev;      // step timing events (pairs)
 
   cudaError_t ensure_f64(int np, int nbuf);
   cudaError_t ensure_split(int np);
   cudaError_t ensure_common(size_t nin, int np, int maxlaunch, int n);
+  cudaError_t ensure_oz(int np, cudaStream_t st);
 };
 
 Ctx* get_ctx(int* status);
@@ -70,6 +80,7 @@ struct DenseJob {
   int* iters_out;
   double* bounds_out;
   int mcweeny;
+  int mcweeny_products;  // SP2B_MCW_INT8 or SP2B_MCW_FP64
 };
 
 int dense_solve(const DenseJob& j);

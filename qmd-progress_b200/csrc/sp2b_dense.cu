@@ -111,6 +111,37 @@ cudaError_t Ctx::ensure_common(size_t nin, int np, int maxlaunch, int n) {
   return cudaSuccess;
 }
 
+cudaError_t Ctx::ensure_oz(int np, cudaStream_t st) {
+  const size_t need = (size_t)oz_nmod() * np * np;
+  cudaError_t e;
+  if (need > oz_cap || !oz_res) {
+    if (oz_res) cudaFree(oz_res);
+    if (oz_q) cudaFree(oz_q);
+    oz_res = nullptr;
+    oz_q = nullptr;
+    oz_cap = 0;
+    if ((e = cudaMalloc((void**)&oz_res, need)) != cudaSuccess) return e;
+    if ((e = cudaMalloc((void**)&oz_q, need)) != cudaSuccess) return e;
+    oz_cap = need;
+  }
+  if (!oz_scale && (e = cudaMalloc(&oz_scale, oz_scale_bytes())) != cudaSuccess) return e;
+  if (oz_tiles_np != np) {
+    std::vector<int2> t;
+    oz_tile_list(np, t);
+    if (oz_tiles) cudaFree(oz_tiles);
+    oz_tiles = nullptr;
+    oz_tiles_np = 0;
+    if ((e = cudaMalloc((void**)&oz_tiles, t.size() * sizeof(int2))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(oz_tiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                             st)) != cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    oz_ntiles = (int)t.size();
+    oz_tiles_np = np;
+  }
+  return cudaSuccess;
+}
+
 // ------------------------------------------------------------------------------------
 // Dense solve
 // ------------------------------------------------------------------------------------
@@ -162,10 +193,14 @@ int dense_solve(const DenseJob& j) {
   else if (j.ctl.algo == ALGO_BASIC) maxlaunch = j.ctl.maxit + 1;
   else maxlaunch = j.ctl.maxit;
 
+  // one McWeeny step of a split solve runs on the INT8 tensor cores (exact residue
+  // products); more steps, or the FP64 choice, use FP64 DMMA products
+  const bool oz = split && j.mcweeny == 1 && j.mcweeny_products == SP2B_MCW_INT8 && np <= 65536;
   const size_t nn = (size_t)n * n;
   SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
-  SP2B_CUDA_TRY(c->ensure_f64(np, split ? 3 : 2));
+  SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : 2));
   if (split) SP2B_CUDA_TRY(c->ensure_split(np));
+  if (oz) SP2B_CUDA_TRY(c->ensure_oz(np, st));
 
   // ---- input ----
   const double* hsrc = j.inplace ? j.rho : j.h;
@@ -289,45 +324,76 @@ int dense_solve(const DenseJob& j) {
     return SP2B_CUDA_ERROR;
   }
 
-  // ---- final density: D = 2 X (FP64) or FP64 McWeeny refinement of the split iterate ----
+  // ---- final density: D = 2 X (FP64) or McWeeny refinement of the split iterate ----
   const int fb = so.nupd & 1;
-  double* xfin;
-  if (split) {
-    SP2B_CUDA_TRY(launch_split_to_f64(c->hi[fb], c->lo[fb], np, bf16, c->x64[0], st));
-    double* X = c->x64[0];
-    double* P = c->x64[1];
-    double* D = c->x64[2];
-    for (int m = 0; m < j.mcweeny; ++m) {
-      StepArgs q;
-      memset(&q, 0, sizeof(q));
-      q.np = np;
-      q.partials = c->partials;
-      q.counter = c->counter;
-      q.sums_out = c->small + 16;
-      // P = X X
-      q.A = q.B = q.E = X;
-      q.out = P;
-      q.alpha = 1.0;
-      q.beta = 0.0;
-      SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
-      // D = 3 P - 2 P X   (McWeeny: 3X^2 - 2X^3)
-      q.A = P;
-      q.B = X;
-      q.E = P;
-      q.out = D;
-      q.alpha = -2.0;
-      q.beta = 3.0;
-      SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
-      std::swap(X, D);
-    }
-    xfin = X;
-  } else {
-    xfin = c->x64[fb];
-  }
   double* rho_dev = j.dev_ptrs ? j.rho : c->hin;
-  SP2B_CUDA_TRY(launch_finish_f64(xfin, np, n, 2.0, rho_dev, n, st));
+  if (oz) {
+    // D = 3X^2 - 2X^3 (times 2) = 2X^2 - 4X(X^2 - X): X^2 from exact INT8 residue
+    // products, the small correction X (4R) from one split-precision product.
+    const int ob = 1 - fb;
+    SP2B_CUDA_TRY(launch_oz_products(c->hi[fb], c->lo[fb], np, bf16, c->oz_scale, c->oz_res,
+                                     c->oz_q, c->oz_tiles, c->oz_ntiles, c->err, st));
+    SP2B_CUDA_TRY(launch_oz_crt(c->oz_q, c->hi[fb], c->lo[fb], np, bf16, c->oz_scale, c->x64[0],
+                                c->hi[ob], c->lo[ob], st));
+    SP2B_CUDA_TRY(launch_mcweeny_tc(c->hi[fb], c->lo[fb], c->hi[ob], c->lo[ob], c->x64[0], np,
+                                    bf16, rho_dev, n, n, c->partials, c->counter, c->small + 16,
+                                    c->err, st));
+  } else {
+    double* xfin;
+    if (split) {
+      SP2B_CUDA_TRY(launch_split_to_f64(c->hi[fb], c->lo[fb], np, bf16, c->x64[0], st));
+      double* X = c->x64[0];
+      double* P = c->x64[1];
+      double* D = c->x64[2];
+      for (int m = 0; m < j.mcweeny; ++m) {
+        StepArgs q;
+        memset(&q, 0, sizeof(q));
+        q.np = np;
+        q.partials = c->partials;
+        q.counter = c->counter;
+        q.sums_out = c->small + 16;
+        // P = X X
+        q.A = q.B = q.E = X;
+        q.out = P;
+        q.alpha = 1.0;
+        q.beta = 0.0;
+        SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+        // D = 3 P - 2 P X   (McWeeny: 3X^2 - 2X^3)
+        q.A = P;
+        q.B = X;
+        q.E = P;
+        q.out = D;
+        q.alpha = -2.0;
+        q.beta = 3.0;
+        SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+        std::swap(X, D);
+      }
+      xfin = X;
+    } else {
+      xfin = c->x64[fb];
+    }
+    SP2B_CUDA_TRY(launch_finish_f64(xfin, np, n, 2.0, rho_dev, n, st));
+  }
   if (!j.dev_ptrs)
     SP2B_CUDA_TRY(cudaMemcpyAsync(j.rho, rho_dev, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (oz) {
+    int S = 0;
+    double r2max = 0.0;
+    SP2B_CUDA_TRY(oz_read_scale(c->oz_scale, &S, &r2max, st));
+    c->oz_last_S = S;
+    c->oz_last_r2max = r2max;
+    int herr = 0;
+    SP2B_CUDA_TRY(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+      set_last_error("a device-side wait timed out in the INT8 McWeeny refinement");
+      return SP2B_TIMEOUT;
+    }
+    if (S < 0) {
+      set_last_error("INT8 McWeeny refinement: no valid scale (largest row norm^2 %g)", r2max);
+      return SP2B_BAD_INPUT;
+    }
+  }
 
   // ---- sequence outputs ----
   const int iters = so.iter;
@@ -368,12 +434,23 @@ extern "C" {
 
 const char* sp2b_last_error(void) { return g_err; }
 
+int sp2b_last_refinement_info(int* scale_exp, double* r2max) {
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (scale_exp) *scale_exp = c->oz_last_S;
+  if (r2max) *r2max = c->oz_last_r2max;
+  return SP2B_OK;
+}
+
 int sp2b_opts_default(sp2b_opts* o) {
   if (!o) return SP2B_BAD_ARG;
   memset(o, 0, sizeof(*o));
   o->precision = SP2B_PREC_FP64;
   o->mcweeny = 1;
   o->mixed_tol = 1e-3;
+  o->mcweeny_products = SP2B_MCW_INT8;
   return SP2B_OK;
 }
 
@@ -420,6 +497,7 @@ static DenseJob base_job(const double* h, double* rho, int n, const sp2b_opts* o
   j.dev_ptrs = o->device_ptrs != 0;
   j.stream = (cudaStream_t)o->stream;
   j.mcweeny = o->mcweeny;
+  j.mcweeny_products = o->mcweeny_products;
   j.ctl.n = n;
   j.ctl.mixed_tol = o->mixed_tol;
   j.ctl.icount = 0;

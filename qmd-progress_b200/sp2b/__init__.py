@@ -15,14 +15,15 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (PREC_FP64, PREC_MIXED_BF16, PREC_MIXED_FP16, SP2Error, check, lib,
-                   make_opts)
+from ._lib import (MCW_FP64, MCW_INT8, PREC_FP64, PREC_MIXED_BF16, PREC_MIXED_FP16, SP2Error,
+                   check, lib, make_opts)
 
 __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq",
            "sp2_alg2_seq_inplace", "sp2_alg1", "sp2_alg1_genseq", "sp2_alg1_seq",
            "sp2_alg1_seq_inplace", "sp2_basic", "sp2_submatrix_inplace", "sp2_submatrix",
            "gershgorin", "normalize", "check_idempotency", "sp2sequence", "homolumogap",
-           "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16"]
+           "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "MCW_INT8",
+           "MCW_FP64", "last_refinement_info"]
 
 
 @dataclass
@@ -45,8 +46,16 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def _opts(precision, mcweeny, mixed_tol):
-    return make_opts(precision=precision, mcweeny=mcweeny, mixed_tol=mixed_tol)
+def _opts(precision, mcweeny, mixed_tol, mcweeny_products=_lib.MCW_INT8):
+    return make_opts(precision=precision, mcweeny=mcweeny, mixed_tol=mixed_tol,
+                     mcweeny_products=mcweeny_products)
+
+
+def last_refinement_info():
+    """(S, r2max) of the last INT8 McWeeny refinement on the current device."""
+    S, r2 = C.c_int(0), C.c_double(0.0)
+    check(lib().sp2b_last_refinement_info(C.byref(S), C.byref(r2)), "last_refinement_info")
+    return S.value, r2.value
 
 
 def _conv(s):
@@ -54,20 +63,22 @@ def _conv(s):
 
 
 def sp2_alg2(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
-             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3,
+             mcweeny_products=_lib.MCW_INT8):
     """prg_sp2_alg2 (src/prg_sp2_mod.F90:263-380)."""
     h = _f64(h)
     n = h.shape[0]
     rho = np.empty_like(h)
     it = C.c_int(0)
-    o = _opts(precision, mcweeny, mixed_tol)
+    o = _opts(precision, mcweeny, mixed_tol, mcweeny_products)
     check(lib().sp2b_sp2_alg2(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter, maxsp2iter,
                               _conv(sp2conv), idemtol, 0, C.byref(o), C.byref(it)), "sp2_alg2")
     return SP2Result(rho=rho, iters=it.value, icount=it.value)
 
 
 def sp2_alg2_genseq(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
-                    threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+                    threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3,
+                    mcweeny_products=_lib.MCW_INT8):
     """prg_sp2_alg2_genseq (src/prg_sp2_mod.F90:395-533): also pp, icount, vv."""
     h = _f64(h)
     n = h.shape[0]
@@ -75,7 +86,7 @@ def sp2_alg2_genseq(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idem
     pp = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.int32)
     vv = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.float64)
     ic = C.c_int(0)
-    o = _opts(precision, mcweeny, mixed_tol)
+    o = _opts(precision, mcweeny, mixed_tol, mcweeny_products)
     check(lib().sp2b_sp2_alg2_genseq(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter,
                                      maxsp2iter, _conv(sp2conv), idemtol, _ptr(pp), C.byref(ic),
                                      _ptr(vv), 0, C.byref(o)), "sp2_alg2_genseq")
@@ -116,13 +127,14 @@ def sp2_alg2_seq_inplace(rho, pp, icount, mineval, maxeval, precision=PREC_FP64)
 
 
 def sp2_alg1(h, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel", idemtol=1e-10,
-             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3):
+             threshold=0.0, precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3,
+             mcweeny_products=_lib.MCW_INT8):
     """prg_sp2_alg1 (src/prg_sp2_mod.F90:734-864)."""
     h = _f64(h)
     n = h.shape[0]
     rho = np.empty_like(h)
     it = C.c_int(0)
-    o = _opts(precision, mcweeny, mixed_tol)
+    o = _opts(precision, mcweeny, mixed_tol, mcweeny_products)
     check(lib().sp2b_sp2_alg1(_ptr(h), _ptr(rho), n, threshold, bndfil, minsp2iter, maxsp2iter,
                               _conv(sp2conv), idemtol, 0, C.byref(o), C.byref(it)), "sp2_alg1")
     return SP2Result(rho=rho, iters=it.value, icount=it.value)

@@ -20,6 +20,7 @@ LIB = os.path.join(HERE, "libsp2b.so")
 SOURCES = [
     "k_f64.cu",
     "k_tc.cu",
+    "k_ozaki.cu",
     "k_subgraph.cu",
     "sp2b_dense.cu",
     "sp2b_subgraph.cu",

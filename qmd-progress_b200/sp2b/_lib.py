@@ -22,6 +22,8 @@ SP2B_NO_DEVICE = 6
 PREC_FP64 = 0
 PREC_MIXED_FP16 = 1
 PREC_MIXED_BF16 = 2
+MCW_INT8 = 0
+MCW_FP64 = 1
 
 STATUS_NAMES = {0: "SP2B_OK", 1: "SP2B_NOT_CONVERGED", 2: "SP2B_BAD_ARG", 3: "SP2B_CUDA_ERROR",
                 4: "SP2B_TIMEOUT", 5: "SP2B_BAD_INPUT", 6: "SP2B_NO_DEVICE"}
@@ -29,7 +31,8 @@ STATUS_NAMES = {0: "SP2B_OK", 1: "SP2B_NOT_CONVERGED", 2: "SP2B_BAD_ARG", 3: "SP
 
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("mcweeny", C.c_int), ("mixed_tol", C.c_double),
-                ("device_ptrs", C.c_int), ("stream", C.c_void_p), ("verbose", C.c_int)]
+                ("device_ptrs", C.c_int), ("stream", C.c_void_p), ("verbose", C.c_int),
+                ("mcweeny_products", C.c_int)]
 
 
 class SP2Error(RuntimeError):
@@ -80,6 +83,7 @@ _SIGS = {
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
+    "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_selftest_wait_timeout": (_i, [_i]),
     "sp2b_set_step_timing": (_i, [_i]),
     "sp2b_step_timing": (_i, [_dp, _llp]),
@@ -140,11 +144,13 @@ def check(status: int, where: str):
         raise SP2Error(status, where, last_error())
 
 
-def make_opts(precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3, device_ptrs=False, stream=None):
+def make_opts(precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3, device_ptrs=False, stream=None,
+              mcweeny_products=MCW_INT8):
     o = Opts()
     lib().sp2b_opts_default(C.byref(o))
     o.precision = precision
     o.mcweeny = mcweeny
+    o.mcweeny_products = mcweeny_products
     o.mixed_tol = mixed_tol
     o.device_ptrs = 1 if device_ptrs else 0
     o.stream = stream

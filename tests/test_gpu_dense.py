@@ -222,3 +222,36 @@ def test_bounded_device_wait_times_out_and_device_stays_usable(cuda):
     ok = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
     ref = O.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10)
     assert np.linalg.norm(ok.rho - ref.rho) / 256 <= 1e-6
+
+
+# ---- McWeeny refinement on the INT8 tensor cores (exact residue products + CRT) ----
+@pytest.mark.parametrize("n,prec", [(100, sp2b.PREC_MIXED_FP16), (200, sp2b.PREC_MIXED_FP16),
+                                    (1000, sp2b.PREC_MIXED_FP16), (2048, sp2b.PREC_MIXED_FP16),
+                                    (640, sp2b.PREC_MIXED_BF16)])
+def test_int8_mcweeny_matches_fp64_mcweeny(cuda, n, prec):
+    """The refinement from INT8 residue products agrees with the same step done with
+    FP64 DMMA products (both start from the same split iterate): X^2 is exact up to the
+    2^-S rounding of X, the correction product is small."""
+    h = M.two_band_1d(n, seed=n + 11)
+    a = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10, precision=prec)
+    S, r2max = sp2b.last_refinement_info()
+    b = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10, precision=prec,
+                             mcweeny_products=sp2b.MCW_FP64)
+    assert a.pp == b.pp
+    assert 30 <= S <= 40 and 0.0 < r2max < 1.5, (S, r2max)
+    assert rel(a.rho, b.rho) <= 1e-10, rel(a.rho, b.rho)
+    assert np.array_equal(a.rho, a.rho.T)
+    ref = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    assert np.linalg.norm(a.rho - ref.rho) / n <= (1e-6 if prec == sp2b.PREC_MIXED_FP16 else 1e-5)
+
+
+def test_int8_mcweeny_against_eigh(cuda):
+    """Config-1-like check at N = 1536 against the FP64 diagonalisation oracle
+    (prg_build_density_T0): ||D - D_ref||_F / N, |Tr D - N_occ|, ||D^2/4 - D/2||_F."""
+    n = 1536
+    h = M.two_band_1d(n, seed=5)
+    got = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
+    d_ref, _ = O.build_density_t0(h, 0.5)
+    assert np.linalg.norm(got.rho - d_ref) / n <= 1e-6
+    assert abs(np.trace(got.rho) - n) <= 1e-6 * n
+    assert O.check_idempotency(got.rho / 2.0) <= 1e-6
