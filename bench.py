@@ -3,7 +3,8 @@
 
 Workload (default): the two-band 1D model Hamiltonian at N=8192 (seeded), solved by the
 alg2 branch rule with FP16 hi+lo split products on the tcgen05 tensor cores, FP32
-accumulation, FP64 traces and one final FP64 McWeeny step.  A "step" is one complete
+accumulation, FP64 traces and one final McWeeny step whose X^2 is exact (nine INT8
+residue products on the tensor cores, CRT in FP64).  A "step" is one complete
 solve H -> D.  Inputs (8192^2 FP64 = 512 MiB) are larger than L2 (126 MB), so no L2
 flush is needed between steps.
 
@@ -64,7 +65,7 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed regions."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -78,7 +79,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -242,20 +243,22 @@ def main():
     launches0 = L.sp2b_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            iters = solve_dev(prec)
-        ev1.record(stream)
-        barrier()
+    clk = ClockSampler(local).__enter__()   # covers every timed region below
+    ev0.record(stream)
+    for _ in range(args.steps):
+        iters = solve_dev(prec)
+    ev1.record(stream)
+    barrier()
     launches = L.sp2b_launch_count() - launches0
     step_ms = C.c_double(0)
     step_n = C.c_longlong(0)
     L.sp2b_step_timing(C.byref(step_ms), C.byref(step_n))
+    ref_ms = (C.c_double * 4)()
+    ref_n = C.c_longlong(0)
+    L.sp2b_refinement_timing(ref_ms, C.byref(ref_n))
     L.sp2b_set_step_timing(0)
     t_ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = world * args.steps / (t_ms / 1e3)
-    clocks = clk.summary()
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
@@ -296,6 +299,9 @@ def main():
                 "ms_per_solve": tf / args.fp64_steps,
                 "tflops": world * args.fp64_steps * 2.0 * n ** 3 * it64 / (tf / 1e3) / 1e12}
 
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+
     # ---- roofline of the dominant kernel (the SP2 step) ----
     peaks, src = load_peaks()
     step_avg_ms = step_ms.value / max(step_n.value, 1)
@@ -311,11 +317,31 @@ def main():
         ent = tj.get(f"sp2_step_{args.precision}_n{n}")
         if ent:
             traffic = ent.get("bytes_per_launch")
+    # executed tensor work: upper 128 x 128 tiles (incl. the diagonal), three 16-bit
+    # products each (hi*hi, hi*lo, lo*hi) over the padded K
+    npad = -(-n // 128) * 128
+    nb = npad // 128
+    exec_flops = 3 * 2.0 * 128 * 128 * npad * (nb * (nb + 1) // 2) if prec != _lib.PREC_FP64 else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "peak_source": f"{src} {peak_key}", "kernel": "k_tc_gemm (SP2 step)",
+                "peak_source": f"{src} {peak_key}", "kernel": "k_tc_persist (SP2 step)",
                 "avg_launch_ms": step_avg_ms, "launches_timed": step_n.value,
-                "flops_per_launch": flops_launch}
+                "flops_per_launch": flops_launch,
+                "executed_tflops": (exec_flops / (step_avg_ms / 1e3) / 1e12) if exec_flops else None,
+                "executed_frac": (exec_flops / (step_avg_ms / 1e3) / 1e12 / peak) if exec_flops and peak else None}
+    refinement = None
+    if ref_n.value > 0:
+        per = [ref_ms[i] / ref_n.value for i in range(4)]
+        nbp = -(-npad // 256)
+        oz_tiles = sum(nbp - bi // 2 for bi in range(nb))
+        int8_ops = 9 * 2.0 * 128 * 256 * npad * oz_tiles       # executed, 9 residue products
+        refinement = {"ms_per_solve": sum(per),
+                      "phases_ms": {"residue_planes": per[0], "int8_products": per[1], "crt": per[2],
+                                    "combine_product": per[3]},
+                      "kernel": "k_oz_gemm (9 INT8 residue products, upper 128x256 tiles)",
+                      "int8_tops_executed": int8_ops / (per[1] / 1e3) / 1e12,
+                      "int8_peak_nominal_tops": 4500.0,
+                      "int8_frac_of_nominal": int8_ops / (per[1] / 1e3) / 1e12 / 4500.0}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(n, iters, max_seconds=20.0)
@@ -331,8 +357,8 @@ def main():
                           "parallelism": f"replicas{world}", "l2": "inputs 512 MiB > L2, no flush"},
                # algorithmic: 2N^3 per SP2 step + 4N^3 for the McWeeny step (mixed)
                "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
-               "fp64": fp64, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-               "clocks": clocks, "gpu_launches": launches}
+               "fp64": fp64, "e2e": e2e, "roofline": roofline, "refinement": refinement,
+               "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

@@ -246,6 +246,9 @@ int sp2b_last_refinement_info(int* scale_exp, double* r2max);
 int sp2b_selftest_wait_timeout(int spin_limit);
 int sp2b_set_step_timing(int enable);
 int sp2b_step_timing(double* ms, long long* launches);
+/* With step timing on: summed device time of the INT8 McWeeny refinement phases over
+ * the timed solves, ms4 = {residue planes, INT8 products, CRT, combine product}. */
+int sp2b_refinement_timing(double* ms4, long long* solves);
 
 #ifdef __cplusplus
 }

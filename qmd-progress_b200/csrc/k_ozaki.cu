@@ -465,12 +465,18 @@ int oz_nmod() { return oz::T; }
 size_t oz_scale_bytes() { return sizeof(OzScale); }
 
 // Upper 128 x 256 tiles of an np x np product: rows of block bi, columns of the 256-wide
-// block bjp, for every bjp that reaches the diagonal or beyond (2 bjp + 1 >= bi).
+// block bjp, for every bjp that reaches the diagonal or beyond (2 bjp + 1 >= bi).  Ordered
+// in panels of kOzPanel column blocks, row blocks top to bottom inside a panel, so one wave
+// of the persistent grid shares few operand row blocks (their K-slices stay in L2).
+constexpr int kOzPanel = 6;
 void oz_tile_list(int np, std::vector<int2>& out) {
   out.clear();
   const int nb = np / oz::BM, nbp = (np + oz::BN - 1) / oz::BN;
-  for (int bi = 0; bi < nb; ++bi)
-    for (int bjp = bi / 2; bjp < nbp; ++bjp) out.push_back(make_int2(bi, bjp));
+  for (int p0 = 0; p0 < nbp; p0 += kOzPanel) {
+    const int p1 = std::min(nbp, p0 + kOzPanel);
+    for (int bi = 0; bi < nb && bi <= 2 * p1 - 1; ++bi)
+      for (int bjp = std::max(p0, bi / 2); bjp < p1; ++bjp) out.push_back(make_int2(bi, bjp));
+  }
 }
 
 static int oz_sms() {
@@ -481,10 +487,9 @@ static int oz_sms() {
   return v;
 }
 
-cudaError_t launch_oz_products(const __half* xhi, const __half* xlo, int np, int bf16,
-                               void* scale, int8_t* res, uint8_t* qout, const int2* tiles,
-                               int ntiles, int* err, cudaStream_t st) {
-  if (np % oz::BM != 0 || np > 65536 || ntiles <= 0) return cudaErrorInvalidValue;
+cudaError_t launch_oz_planes(const __half* xhi, const __half* xlo, int np, int bf16,
+                             void* scale, int8_t* res, cudaStream_t st) {
+  if (np % oz::BM != 0 || np > 65536) return cudaErrorInvalidValue;
   OzScale* sc = (OzScale*)scale;
   cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(OzScale), st);
   if (e != cudaSuccess) return e;
@@ -503,12 +508,17 @@ cudaError_t launch_oz_products(const __half* xhi, const __half* xlo, int np, int
   else
     k_oz_residues<__half><<<g, 256, 0, st>>>(xhi, xlo, np, sc, res);
   note_launch(3);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_oz_gemm(const int8_t* res, int np, uint8_t* qout, const int2* tiles,
+                           int ntiles, int* err, cudaStream_t st) {
+  if (np % oz::BM != 0 || np > 65536 || ntiles <= 0) return cudaErrorInvalidValue;
   CUtensorMap tm;
   if (!make_tmap_box(&tm, res, (long long)oz::T * np, np, np, TMAP_U8, oz::BM))
     return cudaErrorInvalidValue;
-  e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           oz::SMEM_BYTES);
+  cudaError_t e = cudaFuncSetAttribute(k_oz_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       oz::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   OzGemmArgs a;
   a.np = np;

@@ -15,6 +15,10 @@
 #include "reduce.cuh"
 #include "tc_ptx.cuh"
 
+#include <map>
+#include <utility>
+#include <vector>
+
 namespace sp2b {
 namespace tc {
 constexpr int BM = 128;  // UMMA M (TMEM lanes)
@@ -301,7 +305,7 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
     bi = v.y >> 16;
     bj = v.y & 0xffff;
     nloc = v.z;
-    ti.core = v.w;
+    ti.core = v.w == -2 ? p.core : v.w;   // -2: the launch's own core count
   } else {
     upper_tile(t, bi, bj);
   }
@@ -312,6 +316,134 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
   ti.kb = ti.ok ? nloc / tc::BK : 0;
   ti.diag = bi == bj;
   return ti;
+}
+
+// Epilogue of one 128 x 128 accumulator tile for the warp that owns TMEM lane quarter q
+// and 64-column half `half`; tacc is the TMEM address of its lanes' hi*hi accumulator
+// (the cross accumulator follows at + BN columns).
+template <typename T, int EPI>
+__device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
+                                         int q, int half, int lane, double alpha, double beta,
+                                         double (&sums)[4]) {
+  using TR = SplitTraits<T>;
+  const int ld = p.ld;
+  if (EPI == 0 && ti.ok) {
+    const int r = ti.i0 + q * 32 + lane;  // row inside the part
+    const size_t base = (size_t)ti.row0 * ld;
+    const T* Ehi = (const T*)p.E + base;
+    const T* Elo = (const T*)p.E_lo + base;
+    T* Ohi = p.out ? (T*)p.out + base : nullptr;
+    T* Olo = p.out ? (T*)p.out_lo + base : nullptr;
+#pragma unroll 1
+    for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
+      const int cl = half * 64 + cc * tcp::CHUNK;
+      uint32_t hh[16], xx[16];
+      tmem_ld16(tacc + cl, hh);
+      tmem_ld16(tacc + tc::BN + cl, xx);
+      tmem_wait_ld();
+      const int c0 = ti.j0 + cl;
+      alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
+      {
+        const uint4* sh = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0);
+        const uint4* sl = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0);
+        uint4* dh = reinterpret_cast<uint4*>(ehi);
+        uint4* dl = reinterpret_cast<uint4*>(elo);
+        dh[0] = sh[0];
+        dh[1] = sh[1];
+        dl[0] = sl[0];
+        dl[1] = sl[1];
+      }
+      // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
+      // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
+      // (or 2 x 8) bits; only the sums that drive the branch rule are FP64.
+      const float kInvF = (float)TR::kInv, kScaleF = (float)TR::kScale;
+      const float af = (float)alpha, bf = (float)beta;  // 1/0 or -1/2: exact
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = c0 + j;
+        const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
+        const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
+        const float val = fmaf(af, P, bf * x);
+        const T h = TR::from_f(val);
+        const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
+        const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
+        nhi[j] = h;
+        nlo[j] = l;
+        const int w = sym_weight(ti.diag, r, c);
+        // the residual X - X^2 (vv) needs the product at accumulator precision
+        const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
+                              (double)__uint_as_float(hh[j]));
+        const double dres = (double)x - Pd;
+        sums[0] = fma((double)w * vs, vs, sums[0]);
+        sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
+        if (r == c) {
+          sums[1] += vs;
+          sums[3] += Pd;
+        }
+        if (Ohi && w && r != c) {
+          Ohi[(size_t)c * ld + r] = h;
+          Olo[(size_t)c * ld + r] = l;
+        }
+      }
+      if (Ohi) {
+        if (!ti.diag) {
+          uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * ld + c0);
+          uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * ld + c0);
+          const uint4* sh = reinterpret_cast<const uint4*>(nhi);
+          const uint4* sl = reinterpret_cast<const uint4*>(nlo);
+          dh[0] = sh[0];
+          dh[1] = sh[1];
+          dl[0] = sl[0];
+          dl[1] = sl[1];
+        } else {
+          for (int j = 0; j < 16; ++j)
+            if (r <= c0 + j) {
+              Ohi[(size_t)r * ld + c0 + j] = nhi[j];
+              Olo[(size_t)r * ld + c0 + j] = nlo[j];
+            }
+        }
+      }
+    }
+  }
+  if (EPI == 1 && ti.ok) {
+    // D = 2 X^2 - X (4R): X^2 exact to the INT8 refinement's grid (FP64), the
+    // correction X (4R) small, so its split-precision product is far below it.
+    const int r = ti.i0 + q * 32 + lane;
+    const double* X2 = (const double*)p.E;
+    double* D = (double*)p.out;
+    const int nout = p.n_out, ldo = p.ld_out;
+#pragma unroll 1
+    for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
+      const int cl = half * 64 + cc * tcp::CHUNK;
+      uint32_t hh[16], xx[16];
+      tmem_ld16(tacc + cl, hh);
+      tmem_ld16(tacc + tc::BN + cl, xx);
+      tmem_wait_ld();
+      const int c0 = ti.j0 + cl;
+      double x2[16];
+      const double2* src = reinterpret_cast<const double2*>(X2 + (size_t)r * ld + c0);
+#pragma unroll
+      for (int h2 = 0; h2 < 8; ++h2) {
+        const double2 v2 = src[h2];
+        x2[2 * h2] = v2.x;
+        x2[2 * h2 + 1] = v2.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = c0 + j;
+        const double acc = fma(TR::kInv, (double)__uint_as_float(xx[j]),
+                               (double)__uint_as_float(hh[j]));
+        const double d = 2.0 * x2[j] - acc;
+        const int w = sym_weight(ti.diag, r, c);
+        if (w && r < nout && c < nout) {
+          D[(size_t)r * ldo + c] = d;
+          if (r != c) D[(size_t)c * ldo + r] = d;
+          sums[0] = fma((double)w * d, d, sums[0]);
+          if (r == c) sums[1] += d;
+        }
+      }
+    }
+  }
 }
 
 // EPI 0: SP2 step epilogue (A = B = E = X_k).  EPI 1: McWeeny combine of the INT8
@@ -452,130 +584,13 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     const int q = warp & 3;             // TMEM lane quarter of this warp
     const int half = (warp - 2) >> 2;   // 64-column half of the tile
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    const int ld = p.ld;
     uint32_t tl = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
       const TileInfo ti = persist_tile(p, t);
       const int a = tl & 1;
       if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
-      if (EPI == 0 && ti.ok) {
-        const int r = ti.i0 + q * 32 + lane;  // row inside the part
-        const size_t base = (size_t)ti.row0 * ld;
-        const T* Ehi = (const T*)p.E + base;
-        const T* Elo = (const T*)p.E_lo + base;
-        T* Ohi = p.out ? (T*)p.out + base : nullptr;
-        T* Olo = p.out ? (T*)p.out_lo + base : nullptr;
-#pragma unroll 1
-        for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
-          const int cl = half * 64 + cc * tcp::CHUNK;
-          uint32_t hh[16], xx[16];
-          tmem_ld16(tmem + lane_base + a * 256 + cl, hh);
-          tmem_ld16(tmem + lane_base + a * 256 + tc::BN + cl, xx);
-          tmem_wait_ld();
-          const int c0 = ti.j0 + cl;
-          alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
-          {
-            const uint4* sh = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0);
-            const uint4* sl = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0);
-            uint4* dh = reinterpret_cast<uint4*>(ehi);
-            uint4* dl = reinterpret_cast<uint4*>(elo);
-            dh[0] = sh[0];
-            dh[1] = sh[1];
-            dl[0] = sl[0];
-            dl[1] = sl[1];
-          }
-          // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
-          // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
-          // (or 2 x 8) bits; only the sums that drive the branch rule are FP64.
-          const float kInvF = (float)TR::kInv, kScaleF = (float)TR::kScale;
-          const float af = (float)alpha, bf = (float)beta;  // 1/0 or -1/2: exact
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int c = c0 + j;
-            const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
-            const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
-            const float val = fmaf(af, P, bf * x);
-            const T h = TR::from_f(val);
-            const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
-            const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
-            nhi[j] = h;
-            nlo[j] = l;
-            const int w = sym_weight(ti.diag, r, c);
-            // the residual X - X^2 (vv) needs the product at accumulator precision
-            const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
-                                  (double)__uint_as_float(hh[j]));
-            const double dres = (double)x - Pd;
-            sums[0] = fma((double)w * vs, vs, sums[0]);
-            sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
-            if (r == c) {
-              sums[1] += vs;
-              sums[3] += Pd;
-            }
-            if (Ohi && w && r != c) {
-              Ohi[(size_t)c * ld + r] = h;
-              Olo[(size_t)c * ld + r] = l;
-            }
-          }
-          if (Ohi) {
-            if (!ti.diag) {
-              uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * ld + c0);
-              uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * ld + c0);
-              const uint4* sh = reinterpret_cast<const uint4*>(nhi);
-              const uint4* sl = reinterpret_cast<const uint4*>(nlo);
-              dh[0] = sh[0];
-              dh[1] = sh[1];
-              dl[0] = sl[0];
-              dl[1] = sl[1];
-            } else {
-              for (int j = 0; j < 16; ++j)
-                if (r <= c0 + j) {
-                  Ohi[(size_t)r * ld + c0 + j] = nhi[j];
-                  Olo[(size_t)r * ld + c0 + j] = nlo[j];
-                }
-            }
-          }
-        }
-      }
-      if (EPI == 1 && ti.ok) {
-        // D = 2 X^2 - X (4R): X^2 exact to the INT8 refinement's grid (FP64), the
-        // correction X (4R) small, so its split-precision product is far below it.
-        const int r = ti.i0 + q * 32 + lane;
-        const double* X2 = (const double*)p.E;
-        double* D = (double*)p.out;
-        const int nout = p.n_out, ldo = p.ld_out;
-#pragma unroll 1
-        for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
-          const int cl = half * 64 + cc * tcp::CHUNK;
-          uint32_t hh[16], xx[16];
-          tmem_ld16(tmem + lane_base + a * 256 + cl, hh);
-          tmem_ld16(tmem + lane_base + a * 256 + tc::BN + cl, xx);
-          tmem_wait_ld();
-          const int c0 = ti.j0 + cl;
-          double x2[16];
-          const double2* src = reinterpret_cast<const double2*>(X2 + (size_t)r * ld + c0);
-#pragma unroll
-          for (int h2 = 0; h2 < 8; ++h2) {
-            const double2 v2 = src[h2];
-            x2[2 * h2] = v2.x;
-            x2[2 * h2 + 1] = v2.y;
-          }
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int c = c0 + j;
-            const double acc = fma(TR::kInv, (double)__uint_as_float(xx[j]),
-                                   (double)__uint_as_float(hh[j]));
-            const double d = 2.0 * x2[j] - acc;
-            const int w = sym_weight(ti.diag, r, c);
-            if (w && r < nout && c < nout) {
-              D[(size_t)r * ldo + c] = d;
-              if (r != c) D[(size_t)c * ldo + r] = d;
-              sums[0] = fma((double)w * d, d, sums[0]);
-              if (r == c) sums[1] += d;
-            }
-          }
-        }
-      }
+      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums);
       tc_fence_before();  // our TMEM reads are ordered before the release below
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
@@ -584,6 +599,190 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   tc_fence_before();
   __syncthreads();
   if (warp == 1) tmem_dealloc(tmem, tcp::TMEM_COLS);
+  if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+  if (p.out) __threadfence();
+  publish_and_finalize(p, sums, red, &s_flag);
+}
+
+// ---------------------------------------------------------------------------------
+// Paired-CTA SP2 step (cta_group::2) for dense sizes that are multiples of 256.
+// A cluster of two CTAs computes one 256 x 128 output tile per work item with M = 256
+// MMAs: each CTA stages its own 128 rows of A and one 64-row half of B, so a CTA moves
+// 48 KB per 64-wide k-block instead of 64 KB and its MMAs read 6 KB of shared memory per
+// 128 x 128 x 16 slice instead of 8 KB.  CTA 0 of the pair issues the MMAs and owns the
+// operand-full barriers (both CTAs' tile loads complete on them); the MMA commits arrive
+// on the stage-free and accumulator-full barriers of both CTAs; the epilogue warps of
+// both CTAs arrive on CTA 0's accumulator-empty barrier.  Each CTA runs the same
+// epilogue as the single-CTA kernel on its own 128 x 128 block (TMEM double-buffered).
+// Work item w = {bi2, bj}: rows 256 bi2 .. +255, columns 128 bj .. +127, bj >= 2 bi2; the
+// block of CTA 1 is skipped by its epilogue when it lies below the diagonal.
+// ---------------------------------------------------------------------------------
+namespace tcq {
+constexpr int BH = 64;                                  // B rows staged per CTA (N / 2)
+constexpr int A_BYTES = tc::BM * tc::BK * 2;            // 16 KB
+constexpr int BH_BYTES = BH * tc::BK * 2;               // 8 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * BH_BYTES; // 48 KB
+constexpr int ST = 4;
+constexpr int SMEM_BYTES = ST * STAGE_BYTES + 1024;
+}  // namespace tcq
+
+template <typename T, int EPI>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
+    k_tc_pair(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
+              const __grid_constant__ CUtensorMap tm_bhi, const __grid_constant__ CUtensorMap tm_blo,
+              const StepArgs p, const int2* __restrict__ ptiles, int ntiles) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full[tcq::ST];
+  __shared__ __align__(8) uint64_t bar_empty[tcq::ST];
+  __shared__ __align__(8) uint64_t bar_tfull[2];
+  __shared__ __align__(8) uint64_t bar_tempty[2];
+  __shared__ __align__(8) uint64_t bar_final;
+  __shared__ uint32_t tmem_holder;
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+  __shared__ volatile int s_abort;
+
+  double alpha = p.alpha, beta = p.beta;
+  if (EPI == 0 && p.control) {
+    // the decision is the same in every CTA, so both CTAs of a pair leave together
+    const int br = control_prologue(p);
+    if (br < 0) return;
+    if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
+    else { alpha = -1.0; beta = 2.0; }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = smem_u32(smem);
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < tcq::ST; ++s) {
+      mbar_init(smem_u32(&bar_full[s]), 1);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(smem_u32(&bar_tfull[a]), 1);
+      mbar_init(smem_u32(&bar_tempty[a]), 2 * tcp::EPI_WARPS);
+    }
+    mbar_init(smem_u32(&bar_final), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc_pair(smem_u32(&tmem_holder), tcp::TMEM_COLS);
+  tc_fence_before();
+  cluster_sync();   // barriers and TMEM of both CTAs exist before either uses the other's
+  tc_fence_after();
+  const uint32_t tmem = tmem_holder;
+  const int KB = p.np / tc::BK;
+  double sums[4] = {0.0, 0.0, 0.0, 0.0};
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer (both CTAs) ----------------
+      bool ok = true;
+      uint32_t g = 0;
+      for (int w = pair; w < ntiles && ok; w += npairs) {
+        const int2 tile = ptiles[w];
+        const int ra = tile.x * 2 * tc::BM + (int)rank * tc::BM;
+        const int rb = tile.y * tc::BN + (int)rank * tcq::BH;
+        for (int kb = 0; kb < KB; ++kb, ++g) {
+          const int s = g % tcq::ST;
+          const uint32_t u = g / tcq::ST;
+          if (g >= (uint32_t)tcq::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb0 = map_to_rank(smem_u32(&bar_full[s]), 0);
+          if (rank == 0) mbar_expect_tx(smem_u32(&bar_full[s]), 2 * tcq::STAGE_BYTES);
+          const uint32_t st = sbase + s * tcq::STAGE_BYTES;
+          tma_load_2d_pair(st, &tm_ahi, fb0, kb * tc::BK, ra);
+          tma_load_2d_pair(st + tcq::A_BYTES, &tm_alo, fb0, kb * tc::BK, ra);
+          tma_load_2d_pair(st + 2 * tcq::A_BYTES, &tm_bhi, fb0, kb * tc::BK, rb);
+          tma_load_2d_pair(st + 2 * tcq::A_BYTES + tcq::BH_BYTES, &tm_blo, fb0, kb * tc::BK, rb);
+        }
+      }
+      if (!ok) s_abort = 1;
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      // ---------------- MMA issuer (CTA 0 of the pair) ----------------
+      constexpr uint32_t idesc = make_idesc(SplitTraits<T>::kFmt, 2 * tc::BM, tc::BN);
+      bool ok = true;
+      uint32_t g = 0, tl = 0;
+      for (int w = pair; w < ntiles && ok; w += npairs, ++tl) {
+        const int a = tl & 1;
+        const uint32_t v = tl >> 1;
+        if (tl >= 2 && !mbar_wait(smem_u32(&bar_tempty[a]), (v - 1) & 1, &s_abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc_hh = tmem + a * 256, acc_x = tmem + a * 256 + tc::BN;
+        for (int kb = 0; kb < KB; ++kb, ++g) {
+          const int s = g % tcq::ST;
+          if (!mbar_wait(smem_u32(&bar_full[s]), (g / tcq::ST) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + s * tcq::STAGE_BYTES;
+          const uint64_t d_ahi = sw128_desc(st);
+          const uint64_t d_alo = sw128_desc(st + tcq::A_BYTES);
+          const uint64_t d_bhi = sw128_desc(st + 2 * tcq::A_BYTES);
+          const uint64_t d_blo = sw128_desc(st + 2 * tcq::A_BYTES + tcq::BH_BYTES);
+#pragma unroll
+          for (int kk = 0; kk < tc::BK / tc::UK; ++kk) {
+            const uint64_t off = (uint64_t)((kk * tc::UK * 2) >> 4);
+            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+            umma_f16_pair(acc_hh, d_ahi + off, d_bhi + off, idesc, acc);
+            umma_f16_pair(acc_x, d_ahi + off, d_blo + off, idesc, acc);
+            umma_f16_pair(acc_x, d_alo + off, d_bhi + off, idesc, 1u);
+          }
+          umma_commit_pair_mc(smem_u32(&bar_empty[s]), (uint16_t)0x3);
+        }
+        if (!ok) break;
+        umma_commit_pair_mc(smem_u32(&bar_tfull[a]), (uint16_t)0x3);
+      }
+      umma_commit_pair(smem_u32(&bar_final));
+      for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try(smem_u32(&bar_final), 0)) break;
+      if (!ok) s_abort = 1;
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (8 warps in each CTA) ----------------
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const uint32_t tempty0[2] = {map_to_rank(smem_u32(&bar_tempty[0]), 0),
+                                 map_to_rank(smem_u32(&bar_tempty[1]), 0)};
+    uint32_t tl = 0;
+    for (int w = pair; w < ntiles; w += npairs, ++tl) {
+      const int2 tile = ptiles[w];
+      const int a = tl & 1;
+      if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
+      tc_fence_after();
+      TileInfo ti;
+      const int brow = tile.x * 2 + (int)rank;
+      ti.row0 = 0;
+      ti.i0 = brow * tc::BM;
+      ti.j0 = tile.y * tc::BN;
+      ti.kb = KB;
+      ti.core = p.core;
+      ti.ok = brow <= tile.y;        // CTA 1's block of a diagonal pair lies below it
+      ti.diag = brow == tile.y;
+      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(tempty0[a]);
+    }
+  }
+  tc_fence_before();
+  cluster_sync();   // every MMA retired (CTA 0 waited), every epilogue done in both CTAs
+  tc_fence_after();
+  if (warp == 1) tmem_dealloc_pair(tmem, tcp::TMEM_COLS);
   if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
   if (p.out) __threadfence();
   publish_and_finalize(p, sums, red, &s_flag);
@@ -766,12 +965,147 @@ static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles,
   return cudaGetLastError();
 }
 
+// Upper 128 x 128 tiles of an np x np product in panels of kPanel tile columns; inside a
+// panel the row blocks run top to bottom.  The ~148 tiles of one wave of the persistent
+// grid then share ~148/kPanel row blocks of A and kPanel of B, whose K-slices stay in L2,
+// where the plain column order touches every row block of X in each wave.  One list per
+// (device, np), built on first use; none while the stream is being captured.
+constexpr int kPanel = 12;
+void panel_tile_order(int nb, int panel, std::vector<int2>& out) {
+  out.clear();
+  for (int p0 = 0; p0 < nb; p0 += panel) {
+    const int p1 = std::min(nb, p0 + panel);
+    for (int bi = 0; bi < p1; ++bi)
+      for (int bj = std::max(bi, p0); bj < p1; ++bj) out.push_back(make_int2(bi, bj));
+  }
+}
+
+static const int4* dense_tiles(int np, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int4*> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({dev, np});
+  if (it != cache.end()) return it->second;
+  std::vector<int2> order;
+  panel_tile_order(np / tc::BM, kPanel, order);
+  std::vector<int4> t(order.size());
+  for (size_t i = 0; i < order.size(); ++i)
+    t[i] = make_int4(0, (order[i].x << 16) | order[i].y, np, -2);
+  int4* d = nullptr;
+  if (cudaMalloc((void**)&d, t.size() * sizeof(int4)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  cache[{dev, np}] = d;
+  return d;
+}
+
+// Work items of the paired kernel, {bi2, bj} with bj >= 2 bi2, in panels of kPanel column
+// blocks (row pairs top to bottom inside a panel).  Cached per (device, np).
+void pair_tile_order(int nb, int panel, std::vector<int2>& out) {
+  out.clear();
+  for (int p0 = 0; p0 < nb; p0 += panel) {
+    const int p1 = std::min(nb, p0 + panel);
+    for (int bi2 = 0; 2 * bi2 < p1; ++bi2)
+      for (int bj = std::max(2 * bi2, p0); bj < p1; ++bj) out.push_back(make_int2(bi2, bj));
+  }
+}
+
+static const int2* pair_tiles(int np, cudaStream_t st, int* count) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, std::pair<int2*, int>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({dev, np});
+  if (it != cache.end()) {
+    *count = it->second.second;
+    return it->second.first;
+  }
+  std::vector<int2> t;
+  pair_tile_order(np / tc::BM, kPanel, t);
+  int2* d = nullptr;
+  if (cudaMalloc((void**)&d, t.size() * sizeof(int2)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  cache[{dev, np}] = {d, (int)t.size()};
+  *count = (int)t.size();
+  return d;
+}
+
+// Clusters of the paired kernel that can be resident at once (one CTA per SM).
+template <typename T, int EPI>
+static int pair_clusters() {
+  static int per_dev[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return num_sms() / 2;
+  if (per_dev[dev] > 0) return per_dev[dev];
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(num_sms() & ~1, 1, 1);
+  cfg.blockDim = dim3(tcp::NTHR, 1, 1);
+  cfg.dynamicSmemBytes = tcq::SMEM_BYTES;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (void*)k_tc_pair<T, EPI>, &cfg) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    n = num_sms() / 2;
+  }
+  per_dev[dev] = n;
+  return n;
+}
+
+// Paired-CTA launch for np a multiple of 256; returns cudaErrorNotSupported when the
+// caller should use the single-CTA kernel instead.
+template <typename T, int EPI>
+static cudaError_t launch_pair(const StepArgs& a, cudaStream_t st) {
+  if (a.np % (2 * tc::BM) != 0 || a.ld != a.np) return cudaErrorNotSupported;
+  int ntiles = 0;
+  const int2* tl = pair_tiles(a.np, st, &ntiles);
+  if (!tl || ntiles <= 0) return cudaErrorNotSupported;
+  const int type = std::is_same<T, __nv_bfloat16>::value ? TMAP_BF16 : TMAP_F16;
+  CUtensorMap m[4];
+  if (!make_tmap_box(&m[0], a.A, a.np, a.np, a.np, type, tc::BM) ||
+      !make_tmap_box(&m[1], a.A_lo, a.np, a.np, a.np, type, tc::BM) ||
+      !make_tmap_box(&m[2], a.B, a.np, a.np, a.np, type, tcq::BH) ||
+      !make_tmap_box(&m[3], a.B_lo, a.np, a.np, a.np, type, tcq::BH))
+    return cudaErrorInvalidValue;
+  auto kern = k_tc_pair<T, EPI>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tcq::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  const int clusters = std::min(ntiles, pair_clusters<T, EPI>());
+  kern<<<2 * clusters, tcp::NTHR, tcq::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, tl, ntiles);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // Symmetric launches: A = B (the iterate), so one pair of tensor maps serves both.
 cudaError_t launch_sym_gemm_tc(const StepArgs& a0, int bf16, cudaStream_t st) {
   if (a0.np % tc::BM != 0 || a0.A != a0.B || a0.A_lo != a0.B_lo) return cudaErrorInvalidValue;
   StepArgs a = a0;
   a.tiles = nullptr;
   a.ld = a.np;
+  cudaError_t e = bf16 ? launch_pair<__nv_bfloat16, 0>(a, st) : launch_pair<__half, 0>(a, st);
+  if (e != cudaErrorNotSupported) return e;
+  a.tiles = dense_tiles(a.np, st);   // nullptr: plain column order
   const int nt = tc_ntiles(a.np);
   return bf16 ? launch_persist<__nv_bfloat16, 0>(a, a.np, nt, st)
               : launch_persist<__half, 0>(a, a.np, nt, st);
@@ -808,6 +1142,9 @@ cudaError_t launch_mcweeny_tc(const __half* xhi, const __half* xlo, const __half
   a.counter = counter;
   a.sums_out = sums_out;
   a.err = err;
+  cudaError_t e = bf16 ? launch_pair<__nv_bfloat16, 1>(a, st) : launch_pair<__half, 1>(a, st);
+  if (e != cudaErrorNotSupported) return e;
+  a.tiles = dense_tiles(np, st);
   const int nt = tc_ntiles(np);
   return bf16 ? launch_persist<__nv_bfloat16, 1>(a, np, nt, st)
               : launch_persist<__half, 1>(a, np, nt, st);

@@ -98,9 +98,10 @@ cudaError_t launch_mcweeny_tc(const __half* xhi, const __half* xlo, const __half
 int oz_nmod();
 size_t oz_scale_bytes();
 void oz_tile_list(int np, std::vector<int2>& out);
-cudaError_t launch_oz_products(const __half* xhi, const __half* xlo, int np, int bf16,
-                               void* scale, int8_t* res, uint8_t* qout, const int2* tiles,
-                               int ntiles, int* err, cudaStream_t st);
+cudaError_t launch_oz_planes(const __half* xhi, const __half* xlo, int np, int bf16,
+                             void* scale, int8_t* res, cudaStream_t st);
+cudaError_t launch_oz_gemm(const int8_t* res, int np, uint8_t* qout, const int2* tiles,
+                           int ntiles, int* err, cudaStream_t st);
 cudaError_t launch_oz_crt(const uint8_t* q, const __half* xhi, const __half* xlo, int np,
                           int bf16, const void* scale, double* x2, __half* rhi, __half* rlo,
                           cudaStream_t st);

@@ -51,6 +51,7 @@ struct Ctx {
   double oz_last_r2max = 0.0;   // its largest squared row norm
   int last_launches = 0;            // SP2 step launches of the last dense solve
   std::vector<cudaEvent_t> ev;      // step timing events (pairs)
+  std::vector<cudaEvent_t> ev_ref;  // INT8 refinement phase boundaries
 
   cudaError_t ensure_f64(int np, int nbuf);
   cudaError_t ensure_split(int np);

@@ -18,6 +18,8 @@ static std::atomic<int> g_step_timing{0};
 static std::mutex g_timing_mu;
 static double g_step_ms = 0.0;
 static long long g_step_timed = 0;
+static double g_ref_ms[4] = {0.0, 0.0, 0.0, 0.0};  // INT8 refinement phases
+static long long g_ref_timed = 0;
 
 void note_launch(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(); }
@@ -331,13 +333,25 @@ int dense_solve(const DenseJob& j) {
     // D = 3X^2 - 2X^3 (times 2) = 2X^2 - 4X(X^2 - X): X^2 from exact INT8 residue
     // products, the small correction X (4R) from one split-precision product.
     const int ob = 1 - fb;
-    SP2B_CUDA_TRY(launch_oz_products(c->hi[fb], c->lo[fb], np, bf16, c->oz_scale, c->oz_res,
-                                     c->oz_q, c->oz_tiles, c->oz_ntiles, c->err, st));
+    if (timing) {
+      while ((int)c->ev_ref.size() < 5) {
+        cudaEvent_t e;
+        SP2B_CUDA_TRY(cudaEventCreate(&e));
+        c->ev_ref.push_back(e);
+      }
+      SP2B_CUDA_TRY(cudaEventRecord(c->ev_ref[0], st));
+    }
+    SP2B_CUDA_TRY(launch_oz_planes(c->hi[fb], c->lo[fb], np, bf16, c->oz_scale, c->oz_res, st));
+    if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev_ref[1], st));
+    SP2B_CUDA_TRY(launch_oz_gemm(c->oz_res, np, c->oz_q, c->oz_tiles, c->oz_ntiles, c->err, st));
+    if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev_ref[2], st));
     SP2B_CUDA_TRY(launch_oz_crt(c->oz_q, c->hi[fb], c->lo[fb], np, bf16, c->oz_scale, c->x64[0],
                                 c->hi[ob], c->lo[ob], st));
+    if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev_ref[3], st));
     SP2B_CUDA_TRY(launch_mcweeny_tc(c->hi[fb], c->lo[fb], c->hi[ob], c->lo[ob], c->x64[0], np,
                                     bf16, rho_dev, n, n, c->partials, c->counter, c->small + 16,
                                     c->err, st));
+    if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev_ref[4], st));
   } else {
     double* xfin;
     if (split) {
@@ -382,6 +396,15 @@ int dense_solve(const DenseJob& j) {
     SP2B_CUDA_TRY(oz_read_scale(c->oz_scale, &S, &r2max, st));
     c->oz_last_S = S;
     c->oz_last_r2max = r2max;
+    if (timing) {
+      std::lock_guard<std::mutex> lk2(g_timing_mu);
+      for (int ph = 0; ph < 4; ++ph) {
+        float t = 0.f;
+        SP2B_CUDA_TRY(cudaEventElapsedTime(&t, c->ev_ref[ph], c->ev_ref[ph + 1]));
+        g_ref_ms[ph] += t;
+      }
+      ++g_ref_timed;
+    }
     int herr = 0;
     SP2B_CUDA_TRY(cudaMemcpyAsync(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SP2B_CUDA_TRY(cudaStreamSynchronize(st));
@@ -778,6 +801,16 @@ int sp2b_set_step_timing(int enable) {
   g_step_timing.store(enable ? 1 : 0);
   g_step_ms = 0.0;
   g_step_timed = 0;
+  for (double& v : g_ref_ms) v = 0.0;
+  g_ref_timed = 0;
+  return SP2B_OK;
+}
+
+int sp2b_refinement_timing(double* ms4, long long* solves) {
+  std::lock_guard<std::mutex> lk(g_timing_mu);
+  if (ms4)
+    for (int i = 0; i < 4; ++i) ms4[i] = g_ref_ms[i];
+  if (solves) *solves = g_ref_timed;
   return SP2B_OK;
 }
 

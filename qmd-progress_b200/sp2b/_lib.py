@@ -84,6 +84,7 @@ _SIGS = {
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
+    "sp2b_refinement_timing": (_i, [_dp, C.POINTER(C.c_longlong)]),
     "sp2b_selftest_wait_timeout": (_i, [_i]),
     "sp2b_set_step_timing": (_i, [_i]),
     "sp2b_step_timing": (_i, [_dp, _llp]),
