@@ -287,6 +287,9 @@ constexpr int NTHR = NWARP * 32;
 constexpr int EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
 constexpr int CHUNK = 16;  // columns per tcgen05.ld
+constexpr int SCR_WARP = 2048;                        // store staging per epilogue warp
+constexpr int SCR_OFF = tc::ST * tc::STAGE_BYTES;     // after the operand stages
+constexpr int SMEM_BYTES = SCR_OFF + EPI_WARPS * SCR_WARP + 1024;
 }  // namespace tcp
 
 struct TileInfo {
@@ -320,11 +323,12 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
 
 // Epilogue of one 128 x 128 accumulator tile for the warp that owns TMEM lane quarter q
 // and 64-column half `half`; tacc is the TMEM address of its lanes' hi*hi accumulator
-// (the cross accumulator follows at + BN columns).
+// (the cross accumulator follows at + BN columns); scr is the warp's 2 KB of shared
+// scratch for staging stores.
 template <typename T, int EPI>
 __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
                                          int q, int half, int lane, double alpha, double beta,
-                                         double (&sums)[4]) {
+                                         double (&sums)[4], uint8_t* scr) {
   using TR = SplitTraits<T>;
   const int ld = p.ld;
   if (EPI == 0 && ti.ok) {
@@ -358,49 +362,119 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       // (or 2 x 8) bits; only the sums that drive the branch rule are FP64.
       const float kInvF = (float)TR::kInv, kScaleF = (float)TR::kScale;
       const float af = (float)alpha, bf = (float)beta;  // 1/0 or -1/2: exact
+      // Off-diagonal tiles whose core weight is the same across the 16 columns take the
+      // short path: the norm and residual sums of the block in FP32 (two independent
+      // chains each, fixed order), added to the FP64 totals once per block.  The
+      // residual x - P = (x - hh) - 2^-s xx keeps the accumulators' precision: x - hh is
+      // exact when hh is within a factor 2 of x, and the FMA rounds once.
+      const bool uniform = !ti.diag && (ti.core <= 0 || c0 + 15 < ti.core || c0 >= ti.core);
+      if (uniform) {
+        float s0a = 0.f, s0b = 0.f, s2a = 0.f, s2b = 0.f;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int c = c0 + j;
-        const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
-        const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
-        const float val = fmaf(af, P, bf * x);
-        const T h = TR::from_f(val);
-        const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
-        const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
-        nhi[j] = h;
-        nlo[j] = l;
-        const int w = sym_weight(ti.diag, r, c);
-        // the residual X - X^2 (vv) needs the product at accumulator precision
-        const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
-                              (double)__uint_as_float(hh[j]));
-        const double dres = (double)x - Pd;
-        sums[0] = fma((double)w * vs, vs, sums[0]);
-        sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
-        if (r == c) {
-          sums[1] += vs;
-          sums[3] += Pd;
+        for (int j = 0; j < 16; ++j) {
+          const float hhf = __uint_as_float(hh[j]), xxf = __uint_as_float(xx[j]);
+          const float P = fmaf(kInvF, xxf, hhf);
+          const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
+          const float val = fmaf(af, P, bf * x);
+          const T h = TR::from_f(val);
+          const float hf = TR::to_f(h);
+          const T l = TR::from_f((val - hf) * kScaleF);
+          const float vs = fmaf(kInvF, TR::to_f(l), hf);
+          const float dres = fmaf(-kInvF, xxf, x - hhf);
+          nhi[j] = h;
+          nlo[j] = l;
+          if (j & 1) {
+            s0b = fmaf(vs, vs, s0b);
+            s2b = fmaf(dres, dres, s2b);
+          } else {
+            s0a = fmaf(vs, vs, s0a);
+            s2a = fmaf(dres, dres, s2a);
+          }
         }
-        if (Ohi && w && r != c) {
-          Ohi[(size_t)c * ld + r] = h;
-          Olo[(size_t)c * ld + r] = l;
+        const int wc = ti.core <= 0 ? 2 : (r < ti.core ? 1 : 0) + (c0 < ti.core ? 1 : 0);
+        sums[0] = fma(2.0, (double)s0a + (double)s0b, sums[0]);
+        sums[2] = fma((double)wc, (double)s2a + (double)s2b, sums[2]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = c0 + j;
+          const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
+          const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
+          const float val = fmaf(af, P, bf * x);
+          const T h = TR::from_f(val);
+          const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
+          const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
+          nhi[j] = h;
+          nlo[j] = l;
+          const int w = sym_weight(ti.diag, r, c);
+          // the residual X - X^2 (vv) needs the product at accumulator precision
+          const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
+                                (double)__uint_as_float(hh[j]));
+          const double dres = (double)x - Pd;
+          sums[0] = fma((double)w * vs, vs, sums[0]);
+          sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
+          if (r == c) {
+            sums[1] += vs;
+            sums[3] += Pd;
+          }
         }
       }
-      if (Ohi) {
-        if (!ti.diag) {
-          uint4* dh = reinterpret_cast<uint4*>(Ohi + (size_t)r * ld + c0);
-          uint4* dl = reinterpret_cast<uint4*>(Olo + (size_t)r * ld + c0);
-          const uint4* sh = reinterpret_cast<const uint4*>(nhi);
-          const uint4* sl = reinterpret_cast<const uint4*>(nlo);
-          dh[0] = sh[0];
-          dh[1] = sh[1];
-          dl[0] = sl[0];
-          dl[1] = sl[1];
-        } else {
-          for (int j = 0; j < 16; ++j)
-            if (r <= c0 + j) {
-              Ohi[(size_t)r * ld + c0 + j] = nhi[j];
-              Olo[(size_t)r * ld + c0 + j] = nlo[j];
-            }
+      if (!Ohi) continue;
+      // Stores of this 32 x 16 block (rows r0.., columns c0..) and of its mirror.  Whole
+      // blocks go through the warp's scratch so that every store instruction writes
+      // 16-byte pieces of a few rows: the mirror as 8 rows x 64 B per instruction, the
+      // block itself as 16 rows x 32 B; on a diagonal tile only blocks that straddle the
+      // diagonal store element by element (r <= c authoritative), and blocks below it
+      // store nothing (their mirror images carry them).
+      const int r0 = ti.i0 + q * 32;
+      const bool above = !ti.diag || c0 > r0 + 31;
+      const bool below = ti.diag && c0 + 15 < r0;
+      if (above) {
+        T* th = reinterpret_cast<T*>(scr);          // [16][32]: mirror rows c0 + j
+        T* tl = reinterpret_cast<T*>(scr + 1024);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          th[j * 32 + lane] = nhi[j];
+          tl[j * 32 + lane] = nlo[j];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int j = (lane >> 2) + 8 * i, piece = lane & 3;
+          const uint4 vh = *reinterpret_cast<const uint4*>(th + j * 32 + piece * 8);
+          const uint4 vl = *reinterpret_cast<const uint4*>(tl + j * 32 + piece * 8);
+          *reinterpret_cast<uint4*>(Ohi + (size_t)(c0 + j) * ld + r0 + piece * 8) = vh;
+          *reinterpret_cast<uint4*>(Olo + (size_t)(c0 + j) * ld + r0 + piece * 8) = vl;
+        }
+        __syncwarp();
+        T* dh = reinterpret_cast<T*>(scr);          // [32][16]: rows r0 + rr
+        T* dl = reinterpret_cast<T*>(scr + 1024);
+        reinterpret_cast<uint4*>(dh + lane * 16)[0] = reinterpret_cast<const uint4*>(nhi)[0];
+        reinterpret_cast<uint4*>(dh + lane * 16)[1] = reinterpret_cast<const uint4*>(nhi)[1];
+        reinterpret_cast<uint4*>(dl + lane * 16)[0] = reinterpret_cast<const uint4*>(nlo)[0];
+        reinterpret_cast<uint4*>(dl + lane * 16)[1] = reinterpret_cast<const uint4*>(nlo)[1];
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int rr = (lane >> 1) + 16 * i, piece = lane & 1;
+          const uint4 vh = *reinterpret_cast<const uint4*>(dh + rr * 16 + piece * 8);
+          const uint4 vl = *reinterpret_cast<const uint4*>(dl + rr * 16 + piece * 8);
+          *reinterpret_cast<uint4*>(Ohi + (size_t)(r0 + rr) * ld + c0 + piece * 8) = vh;
+          *reinterpret_cast<uint4*>(Olo + (size_t)(r0 + rr) * ld + c0 + piece * 8) = vl;
+        }
+        __syncwarp();
+      } else if (!below) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = c0 + j;
+          if (r < c) {
+            Ohi[(size_t)c * ld + r] = nhi[j];
+            Olo[(size_t)c * ld + r] = nlo[j];
+          }
+          if (r <= c) {
+            Ohi[(size_t)r * ld + c] = nhi[j];
+            Olo[(size_t)r * ld + c] = nlo[j];
+          }
         }
       }
     }
@@ -590,7 +664,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       const int a = tl & 1;
       if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
-      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums);
+      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
+                       smem + tcp::SCR_OFF + (warp - 2) * tcp::SCR_WARP);
       tc_fence_before();  // our TMEM reads are ordered before the release below
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
@@ -623,7 +698,8 @@ constexpr int A_BYTES = tc::BM * tc::BK * 2;            // 16 KB
 constexpr int BH_BYTES = BH * tc::BK * 2;               // 8 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * BH_BYTES; // 48 KB
 constexpr int ST = 4;
-constexpr int SMEM_BYTES = ST * STAGE_BYTES + 1024;
+constexpr int SCR_OFF = ST * STAGE_BYTES;
+constexpr int SMEM_BYTES = SCR_OFF + tcp::EPI_WARPS * tcp::SCR_WARP + 1024;
 }  // namespace tcq
 
 template <typename T, int EPI>
@@ -773,7 +849,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
       ti.core = p.core;
       ti.ok = brow <= tile.y;        // CTA 1's block of a diagonal pair lies below it
       ti.diag = brow == tile.y;
-      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums);
+      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
+                       smem + tcq::SCR_OFF + (warp - 2) * tcp::SCR_WARP);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(tempty0[a]);
@@ -957,10 +1034,10 @@ static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles,
   }
   auto kern = k_tc_persist<T, EPI>;
   cudaError_t e =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tcp::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   const int grid = std::min(ntiles, num_sms());
-  kern<<<grid, tcp::NTHR, tc::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
+  kern<<<grid, tcp::NTHR, tcp::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
   note_launch();
   return cudaGetLastError();
 }
