@@ -338,25 +338,41 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
     const T* Elo = (const T*)p.E_lo + base;
     T* Ohi = p.out ? (T*)p.out + base : nullptr;
     T* Olo = p.out ? (T*)p.out_lo + base : nullptr;
+    const int r0 = ti.i0 + q * 32;   // first row of this warp
+    // On a diagonal tile the blocks wholly below the diagonal (a prefix of this warp's
+    // chunks) carry weight zero and are stored through their mirror images: skipped.
+    int first = 0;
+    while (first < 64 / tcp::CHUNK && ti.diag && ti.j0 + half * 64 + first * tcp::CHUNK + 15 < r0)
+      ++first;
+    // the rows of X_k for the next chunk are fetched while this one is processed
+    uint4 pf[4];
+    auto fetch_e = [&](int c0x) {
+      const uint4* sh = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0x);
+      const uint4* sl = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0x);
+      pf[0] = sh[0];
+      pf[1] = sh[1];
+      pf[2] = sl[0];
+      pf[3] = sl[1];
+    };
+    if (first < 64 / tcp::CHUNK) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
 #pragma unroll 1
-    for (int cc = 0; cc < 64 / tcp::CHUNK; ++cc) {
+    for (int cc = first; cc < 64 / tcp::CHUNK; ++cc) {
       const int cl = half * 64 + cc * tcp::CHUNK;
       uint32_t hh[16], xx[16];
       tmem_ld16(tacc + cl, hh);
       tmem_ld16(tacc + tc::BN + cl, xx);
-      tmem_wait_ld();
       const int c0 = ti.j0 + cl;
       alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
       {
-        const uint4* sh = reinterpret_cast<const uint4*>(Ehi + (size_t)r * ld + c0);
-        const uint4* sl = reinterpret_cast<const uint4*>(Elo + (size_t)r * ld + c0);
         uint4* dh = reinterpret_cast<uint4*>(ehi);
         uint4* dl = reinterpret_cast<uint4*>(elo);
-        dh[0] = sh[0];
-        dh[1] = sh[1];
-        dl[0] = sl[0];
-        dl[1] = sl[1];
+        dh[0] = pf[0];
+        dh[1] = pf[1];
+        dl[0] = pf[2];
+        dl[1] = pf[3];
       }
+      if (cc + 1 < 64 / tcp::CHUNK) fetch_e(c0 + tcp::CHUNK);
+      tmem_wait_ld();
       // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
       // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
       // (or 2 x 8) bits; only the sums that drive the branch rule are FP64.
@@ -367,7 +383,8 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       // chains each, fixed order), added to the FP64 totals once per block.  The
       // residual x - P = (x - hh) - 2^-s xx keeps the accumulators' precision: x - hh is
       // exact when hh is within a factor 2 of x, and the FMA rounds once.
-      const bool uniform = !ti.diag && (ti.core <= 0 || c0 + 15 < ti.core || c0 >= ti.core);
+      const bool above = !ti.diag || c0 > r0 + 31;   // every element has r < c
+      const bool uniform = above && (ti.core <= 0 || c0 + 15 < ti.core || c0 >= ti.core);
       if (uniform) {
         float s0a = 0.f, s0b = 0.f, s2a = 0.f, s2b = 0.f;
 #pragma unroll
@@ -426,9 +443,6 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       // block itself as 16 rows x 32 B; on a diagonal tile only blocks that straddle the
       // diagonal store element by element (r <= c authoritative), and blocks below it
       // store nothing (their mirror images carry them).
-      const int r0 = ti.i0 + q * 32;
-      const bool above = !ti.diag || c0 > r0 + 31;
-      const bool below = ti.diag && c0 + 15 < r0;
       if (above) {
         T* th = reinterpret_cast<T*>(scr);          // [16][32]: mirror rows c0 + j
         T* tl = reinterpret_cast<T*>(scr + 1024);
@@ -463,7 +477,7 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
           *reinterpret_cast<uint4*>(Olo + (size_t)(r0 + rr) * ld + c0 + piece * 8) = vl;
         }
         __syncwarp();
-      } else if (!below) {
+      } else {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int c = c0 + j;
