@@ -290,6 +290,8 @@ constexpr int CHUNK = 16;  // columns per tcgen05.ld
 constexpr int SCR_WARP = 2048;                        // store staging per epilogue warp
 constexpr int SCR_OFF = tc::ST * tc::STAGE_BYTES;     // after the operand stages
 constexpr int SMEM_BYTES = SCR_OFF + EPI_WARPS * SCR_WARP + 1024;
+constexpr int E_BYTES = 4 * tc::TILE_BYTES;           // X_k block of a tile, hi + lo
+constexpr int SMEM_BYTES_E = 2 * tc::STAGE_BYTES + E_BYTES + EPI_WARPS * SCR_WARP + 1024;
 }  // namespace tcp
 
 struct TileInfo {
@@ -324,11 +326,13 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
 // Epilogue of one 128 x 128 accumulator tile for the warp that owns TMEM lane quarter q
 // and 64-column half `half`; tacc is the TMEM address of its lanes' hi*hi accumulator
 // (the cross accumulator follows at + BN columns); scr is the warp's 2 KB of shared
-// scratch for staging stores.
-template <typename T, int EPI>
+// scratch for staging stores.  ESM: the tile's X_k block was loaded by TMA into estage
+// (hi and lo of each 64-column half as 128-byte-swizzled 128 x 64 boxes) and is read from
+// there; otherwise each lane reads its row of X_k from global memory.
+template <typename T, int EPI, bool ESM>
 __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
                                          int q, int half, int lane, double alpha, double beta,
-                                         double (&sums)[4], uint8_t* scr) {
+                                         double (&sums)[4], uint8_t* scr, const uint8_t* estage) {
   using TR = SplitTraits<T>;
   const int ld = p.ld;
   if (EPI == 0 && ti.ok) {
@@ -354,7 +358,8 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       pf[2] = sl[0];
       pf[3] = sl[1];
     };
-    if (first < 64 / tcp::CHUNK) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
+    if (!ESM && first < 64 / tcp::CHUNK) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
+    const int rl = q * 32 + lane;   // row inside the tile
 #pragma unroll 1
     for (int cc = first; cc < 64 / tcp::CHUNK; ++cc) {
       const int cl = half * 64 + cc * tcp::CHUNK;
@@ -366,12 +371,22 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       {
         uint4* dh = reinterpret_cast<uint4*>(ehi);
         uint4* dl = reinterpret_cast<uint4*>(elo);
-        dh[0] = pf[0];
-        dh[1] = pf[1];
-        dl[0] = pf[2];
-        dl[1] = pf[3];
+        if (ESM) {
+          // 16-byte chunk k of row rl sits at chunk k ^ (rl & 7) (128-byte swizzle)
+          const uint8_t* eb = estage + half * 2 * tc::TILE_BYTES + rl * 128;
+          const int k0 = ((2 * cc) ^ (rl & 7)) * 16, k1 = ((2 * cc + 1) ^ (rl & 7)) * 16;
+          dh[0] = *reinterpret_cast<const uint4*>(eb + k0);
+          dh[1] = *reinterpret_cast<const uint4*>(eb + k1);
+          dl[0] = *reinterpret_cast<const uint4*>(eb + tc::TILE_BYTES + k0);
+          dl[1] = *reinterpret_cast<const uint4*>(eb + tc::TILE_BYTES + k1);
+        } else {
+          dh[0] = pf[0];
+          dh[1] = pf[1];
+          dl[0] = pf[2];
+          dl[1] = pf[3];
+        }
       }
-      if (cc + 1 < 64 / tcp::CHUNK) fetch_e(c0 + tcp::CHUNK);
+      if (!ESM && cc + 1 < 64 / tcp::CHUNK) fetch_e(c0 + tcp::CHUNK);
       tmem_wait_ld();
       // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
       // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
@@ -537,18 +552,26 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
 // EPI 0: SP2 step epilogue (A = B = E = X_k).  EPI 1: McWeeny combine of the INT8
 // refinement, D = 2 X^2 - acc with acc = X (4R) (A = X, B = 4R = 4(X^2 - X), E = X^2 in
 // FP64), written to the n_out x n_out density (row pitch ld_out) and mirrored.
-template <typename T, int EPI>
+// ESM (batched sub-graph steps): two operand stages, and the epilogue's X_k block comes
+// by TMA into a 64 KB stage (loaded while the tile's MMAs run) instead of per-lane global
+// loads.
+template <typename T, int EPI, bool ESM>
 __global__ void __launch_bounds__(tcp::NTHR, 1)
     k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                  const __grid_constant__ CUtensorMap tm_bhi,
                  const __grid_constant__ CUtensorMap tm_blo, const StepArgs p, int ntiles) {
   using TR = SplitTraits<T>;
+  constexpr int ST = ESM ? 2 : tc::ST;
+  constexpr int EOFF = ST * tc::STAGE_BYTES;                      // X_k block stage (ESM)
+  constexpr int SOFF = ESM ? EOFF + tcp::E_BYTES : tcp::SCR_OFF;  // store scratch
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[tc::ST];
   __shared__ __align__(8) uint64_t bar_empty[tc::ST];
   __shared__ __align__(8) uint64_t bar_tfull[2];
   __shared__ __align__(8) uint64_t bar_tempty[2];
   __shared__ __align__(8) uint64_t bar_final;
+  __shared__ __align__(8) uint64_t bar_efull;   // ESM: X_k block landed
+  __shared__ __align__(8) uint64_t bar_efree;   // ESM: all epilogue warps done with it
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
@@ -576,6 +599,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       mbar_init(smem_u32(&bar_tempty[a]), tcp::EPI_WARPS);
     }
     mbar_init(smem_u32(&bar_final), 1);
+    mbar_init(smem_u32(&bar_efull), 1);
+    mbar_init(smem_u32(&bar_efree), tcp::EPI_WARPS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), tcp::TMEM_COLS);
@@ -588,16 +613,16 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   if (warp == 0) {
     if (lane == 0) {
       // ---------------- TMA producer ----------------
-      int issued_phase[tc::ST];
-      for (int s = 0; s < tc::ST; ++s) issued_phase[s] = -1;
+      int issued_phase[ST];
+      for (int s = 0; s < ST; ++s) issued_phase[s] = -1;
       bool ok = true;
       uint32_t g = 0;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const TileInfo ti = persist_tile(p, t);
         for (int kb = 0; kb < ti.kb; ++kb, ++g) {
-          const int s = g % tc::ST;
-          const uint32_t u = g / tc::ST;
-          if (g >= (uint32_t)tc::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+          const int s = g % ST;
+          const uint32_t u = g / ST;
+          if (g >= (uint32_t)ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
             ok = false;
             break;
           }
@@ -612,7 +637,7 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
         }
       }
       if (!ok) {  // abort: wait (bounded) for this CTA's copies still in flight
-        for (int s = 0; s < tc::ST; ++s)
+        for (int s = 0; s < ST; ++s)
           if (issued_phase[s] >= 0)
             for (uint32_t i = 0; i < kSpinLimit; ++i)
               if (mbar_try(smem_u32(&bar_full[s]), issued_phase[s])) break;
@@ -636,8 +661,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
         tc_fence_after();
         const uint32_t acc_hh = tmem + a * 256, acc_x = tmem + a * 256 + tc::BN;
         for (int kb = 0; kb < ti.kb; ++kb, ++g) {
-          const int s = g % tc::ST;
-          if (!mbar_wait(smem_u32(&bar_full[s]), (g / tc::ST) & 1, &s_abort)) {
+          const int s = g % ST;
+          if (!mbar_wait(smem_u32(&bar_full[s]), (g / ST) & 1, &s_abort)) {
             ok = false;
             break;
           }
@@ -673,17 +698,57 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     const int half = (warp - 2) >> 2;   // 64-column half of the tile
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t tl = 0;
+    uint32_t eph = 0;          // ESM: X_k blocks loaded (and consumed) so far
+    bool e_pending = false;    // ESM, issuing thread: a load not yet waited for
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
       const TileInfo ti = persist_tile(p, t);
       const int a = tl & 1;
+      if (ESM && ti.ok) {
+        // warp 2 lane 0 loads this tile's X_k block once every warp has released the
+        // previous one; the load runs while the tile's MMAs finish
+        bool ok2 = true;
+        if (warp == 2) {
+          if (lane == 0) {
+            if (eph > 0) ok2 = mbar_wait(smem_u32(&bar_efree), (eph - 1) & 1, &s_abort);
+            if (ok2) {
+              const uint32_t eb = smem_u32(&bar_efull);
+              const uint32_t es = sbase + EOFF;
+              const int y = ti.row0 + ti.i0;
+              mbar_expect_tx(eb, tcp::E_BYTES);
+              tma_load_2d(es + 0 * tc::TILE_BYTES, &tm_hi, eb, ti.j0, y);
+              tma_load_2d(es + 1 * tc::TILE_BYTES, &tm_lo, eb, ti.j0, y);
+              tma_load_2d(es + 2 * tc::TILE_BYTES, &tm_hi, eb, ti.j0 + 64, y);
+              tma_load_2d(es + 3 * tc::TILE_BYTES, &tm_lo, eb, ti.j0 + 64, y);
+              e_pending = true;
+            }
+          }
+          ok2 = __shfl_sync(0xffffffffu, ok2 ? 1 : 0, 0) != 0;
+        }
+        if (!ok2) break;
+      }
       if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
-      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
-                       smem + tcp::SCR_OFF + (warp - 2) * tcp::SCR_WARP);
+      bool eok = true;
+      if (ESM && ti.ok) {
+        eok = mbar_wait(smem_u32(&bar_efull), eph & 1, &s_abort);
+        if (eok) e_pending = false;
+      }
+      if (eok)
+        epi_tile<T, EPI, ESM>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
+                              smem + SOFF + (warp - 2) * tcp::SCR_WARP, smem + EOFF);
       tc_fence_before();  // our TMEM reads are ordered before the release below
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
+      if (ESM && ti.ok) {
+        if (lane == 0) mbar_arrive(smem_u32(&bar_efree));
+        ++eph;
+      }
+      if (!eok) break;
     }
+    // a load that was issued but never waited for (abort) must land before the exit
+    if (ESM && e_pending)
+      for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try(smem_u32(&bar_efull), eph & 1)) break;
   }
   tc_fence_before();
   __syncthreads();
@@ -863,8 +928,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
       ti.core = p.core;
       ti.ok = brow <= tile.y;        // CTA 1's block of a diagonal pair lies below it
       ti.diag = brow == tile.y;
-      epi_tile<T, EPI>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
-                       smem + tcq::SCR_OFF + (warp - 2) * tcp::SCR_WARP);
+      epi_tile<T, EPI, false>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
+                              smem + tcq::SCR_OFF + (warp - 2) * tcp::SCR_WARP, nullptr);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(tempty0[a]);
@@ -1033,7 +1098,7 @@ static int num_sms() {
   return sms;
 }
 
-template <typename T, int EPI>
+template <typename T, int EPI, bool ESM = false>
 static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles, cudaStream_t st) {
   const bool bf16 = std::is_same<T, __nv_bfloat16>::value;
   CUtensorMap m[4];
@@ -1046,12 +1111,12 @@ static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles,
              !make_tmap(&m[3], a.B_lo, rows, a.ld, a.ld, bf16)) {
     return cudaErrorInvalidValue;
   }
-  auto kern = k_tc_persist<T, EPI>;
-  cudaError_t e =
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tcp::SMEM_BYTES);
+  auto kern = k_tc_persist<T, EPI, ESM>;
+  const int smem = ESM ? tcp::SMEM_BYTES_E : tcp::SMEM_BYTES;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   const int grid = std::min(ntiles, num_sms());
-  kern<<<grid, tcp::NTHR, tcp::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
+  kern<<<grid, tcp::NTHR, smem, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
   note_launch();
   return cudaGetLastError();
 }
@@ -1207,8 +1272,8 @@ cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf
   if (!a.tiles || a.ntiles <= 0 || a.ld % tc::BM != 0 || rows % tc::BM != 0 || a.A != a.B ||
       a.A_lo != a.B_lo)
     return cudaErrorInvalidValue;
-  return bf16 ? launch_persist<__nv_bfloat16, 0>(a, rows, a.ntiles, st)
-              : launch_persist<__half, 0>(a, rows, a.ntiles, st);
+  return bf16 ? launch_persist<__nv_bfloat16, 0, true>(a, rows, a.ntiles, st)
+              : launch_persist<__half, 0, true>(a, rows, a.ntiles, st);
 }
 
 // McWeeny combine of the INT8 refinement: D = 2 X^2 - X (4R), upper tiles, mirrored.
