@@ -327,12 +327,14 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
 // and 64-column half `half`; tacc is the TMEM address of its lanes' hi*hi accumulator
 // (the cross accumulator follows at + BN columns); scr is the warp's 2 KB of shared
 // scratch for staging stores.  ESM: the tile's X_k block was loaded by TMA into estage
-// (hi and lo of each 64-column half as 128-byte-swizzled 128 x 64 boxes) and is read from
-// there; otherwise each lane reads its row of X_k from global memory.
+// (hi and lo of each 64-column half as 128-byte-swizzled 128 x 64 boxes), is read from
+// there, and X_{k+1} is written back in place for a TMA store of the whole tile; only the
+// mirror of an off-diagonal tile is stored from the registers.  Otherwise each lane reads
+// its row of X_k from global memory and stores the block and its mirror itself.
 template <typename T, int EPI, bool ESM>
 __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
                                          int q, int half, int lane, double alpha, double beta,
-                                         double (&sums)[4], uint8_t* scr, const uint8_t* estage) {
+                                         double (&sums)[4], uint8_t* scr, uint8_t* estage) {
   using TR = SplitTraits<T>;
   const int ld = p.ld;
   if (EPI == 0 && ti.ok) {
@@ -368,13 +370,13 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       tmem_ld16(tacc + tc::BN + cl, xx);
       const int c0 = ti.j0 + cl;
       alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
+      // 16-byte chunk k of row rl of a staged box sits at chunk k ^ (rl & 7) (128-byte swizzle)
+      uint8_t* eb = ESM ? estage + half * 2 * tc::TILE_BYTES + rl * 128 : nullptr;
+      const int k0 = ((2 * cc) ^ (rl & 7)) * 16, k1 = ((2 * cc + 1) ^ (rl & 7)) * 16;
       {
         uint4* dh = reinterpret_cast<uint4*>(ehi);
         uint4* dl = reinterpret_cast<uint4*>(elo);
         if (ESM) {
-          // 16-byte chunk k of row rl sits at chunk k ^ (rl & 7) (128-byte swizzle)
-          const uint8_t* eb = estage + half * 2 * tc::TILE_BYTES + rl * 128;
-          const int k0 = ((2 * cc) ^ (rl & 7)) * 16, k1 = ((2 * cc + 1) ^ (rl & 7)) * 16;
           dh[0] = *reinterpret_cast<const uint4*>(eb + k0);
           dh[1] = *reinterpret_cast<const uint4*>(eb + k1);
           dl[0] = *reinterpret_cast<const uint4*>(eb + tc::TILE_BYTES + k0);
@@ -450,6 +452,32 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
             sums[3] += Pd;
           }
         }
+      }
+      if (ESM) {
+        // X_{k+1} in place of X_k; the whole tile leaves by TMA once every warp is done
+        *reinterpret_cast<uint4*>(eb + k0) = reinterpret_cast<const uint4*>(nhi)[0];
+        *reinterpret_cast<uint4*>(eb + k1) = reinterpret_cast<const uint4*>(nhi)[1];
+        *reinterpret_cast<uint4*>(eb + tc::TILE_BYTES + k0) = reinterpret_cast<const uint4*>(nlo)[0];
+        *reinterpret_cast<uint4*>(eb + tc::TILE_BYTES + k1) = reinterpret_cast<const uint4*>(nlo)[1];
+        if (ti.diag || !Ohi) continue;   // a diagonal tile is its own mirror
+        T* th = reinterpret_cast<T*>(scr);          // [16][32]: mirror rows c0 + j
+        T* tl = reinterpret_cast<T*>(scr + 1024);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          th[j * 32 + lane] = nhi[j];
+          tl[j * 32 + lane] = nlo[j];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int j = (lane >> 2) + 8 * i, piece = lane & 3;
+          const uint4 vh = *reinterpret_cast<const uint4*>(th + j * 32 + piece * 8);
+          const uint4 vl = *reinterpret_cast<const uint4*>(tl + j * 32 + piece * 8);
+          *reinterpret_cast<uint4*>(Ohi + (size_t)(c0 + j) * ld + r0 + piece * 8) = vh;
+          *reinterpret_cast<uint4*>(Olo + (size_t)(c0 + j) * ld + r0 + piece * 8) = vl;
+        }
+        __syncwarp();
+        continue;
       }
       if (!Ohi) continue;
       // Stores of this 32 x 16 block (rows r0.., columns c0..) and of its mirror.  Whole
@@ -549,17 +577,56 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
   }
 }
 
+// Lower triangle of a staged diagonal tile := transpose of its upper triangle, so that the
+// stored X_{k+1} is exactly symmetric (the MMA's values below the diagonal are not the
+// mirror of those above it bit for bit).  Layout as the X_k stage: box (half h, array a)
+// at (2h + a) * TILE_BYTES, row r at r * 128, 16-byte chunk k at (k ^ (r & 7)) * 16.
+// Thread t of the 256 epilogue threads handles row t / 2, every other 8-column chunk.
+__device__ __forceinline__ uint32_t stage_off(int a, int row, int col) {
+  const int h = col >> 6, cl = col & 63;
+  return (uint32_t)((h * 2 + a) * tc::TILE_BYTES + row * 128 + ((((cl >> 3) ^ (row & 7))) << 4) +
+                    ((cl & 7) << 1));
+}
+__device__ __forceinline__ void stage_symmetrize(uint8_t* stage, int t) {
+  const int r = t >> 1;
+  const int nk = (r + 7) >> 3;   // chunks holding some column c < r
+  for (int k = t & 1; k < nk; k += 2) {
+    const int cmax = min(8, r - 8 * k);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      uint16_t v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        v[e] = e < cmax ? *reinterpret_cast<const uint16_t*>(stage + stage_off(a, 8 * k + e, r)) : 0;
+      if (cmax == 8) {
+        uint4 w;
+        w.x = (uint32_t)v[0] | ((uint32_t)v[1] << 16);
+        w.y = (uint32_t)v[2] | ((uint32_t)v[3] << 16);
+        w.z = (uint32_t)v[4] | ((uint32_t)v[5] << 16);
+        w.w = (uint32_t)v[6] | ((uint32_t)v[7] << 16);
+        *reinterpret_cast<uint4*>(stage + stage_off(a, r, 8 * k)) = w;
+      } else {
+        for (int e = 0; e < cmax; ++e)
+          *reinterpret_cast<uint16_t*>(stage + stage_off(a, r, 8 * k + e)) = v[e];
+      }
+    }
+  }
+}
+
 // EPI 0: SP2 step epilogue (A = B = E = X_k).  EPI 1: McWeeny combine of the INT8
 // refinement, D = 2 X^2 - acc with acc = X (4R) (A = X, B = 4R = 4(X^2 - X), E = X^2 in
 // FP64), written to the n_out x n_out density (row pitch ld_out) and mirrored.
-// ESM (batched sub-graph steps): two operand stages, and the epilogue's X_k block comes
-// by TMA into a 64 KB stage (loaded while the tile's MMAs run) instead of per-lane global
-// loads.
+// ESM (batched sub-graph steps): two operand stages; the tile's X_k block comes by TMA
+// into a 64 KB stage (loaded while the tile's MMAs run), X_{k+1} is written over it and
+// leaves by TMA stores (tm_ohi / tm_olo: the output arrays), a diagonal tile symmetrised
+// in shared memory first; only off-diagonal mirrors use ordinary stores.
 template <typename T, int EPI, bool ESM>
 __global__ void __launch_bounds__(tcp::NTHR, 1)
     k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                  const __grid_constant__ CUtensorMap tm_bhi,
-                 const __grid_constant__ CUtensorMap tm_blo, const StepArgs p, int ntiles) {
+                 const __grid_constant__ CUtensorMap tm_blo,
+                 const __grid_constant__ CUtensorMap tm_ohi,
+                 const __grid_constant__ CUtensorMap tm_olo, const StepArgs p, int ntiles) {
   using TR = SplitTraits<T>;
   constexpr int ST = ESM ? 2 : tc::ST;
   constexpr int EOFF = ST * tc::STAGE_BYTES;                      // X_k block stage (ESM)
@@ -571,7 +638,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   __shared__ __align__(8) uint64_t bar_tempty[2];
   __shared__ __align__(8) uint64_t bar_final;
   __shared__ __align__(8) uint64_t bar_efull;   // ESM: X_k block landed
-  __shared__ __align__(8) uint64_t bar_efree;   // ESM: all epilogue warps done with it
+  __shared__ __align__(8) uint64_t bar_odone;   // ESM: every warp wrote its part of X_{k+1}
+  __shared__ __align__(8) uint64_t bar_osym;    // ESM: diagonal tile symmetrised
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
@@ -600,7 +668,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     }
     mbar_init(smem_u32(&bar_final), 1);
     mbar_init(smem_u32(&bar_efull), 1);
-    mbar_init(smem_u32(&bar_efree), tcp::EPI_WARPS);
+    mbar_init(smem_u32(&bar_odone), tcp::EPI_WARPS);
+    mbar_init(smem_u32(&bar_osym), tcp::EPI_WARPS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), tcp::TMEM_COLS);
@@ -699,17 +768,18 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t tl = 0;
     uint32_t eph = 0;          // ESM: X_k blocks loaded (and consumed) so far
+    uint32_t sph = 0;          // ESM: diagonal tiles symmetrised so far
     bool e_pending = false;    // ESM, issuing thread: a load not yet waited for
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
       const TileInfo ti = persist_tile(p, t);
       const int a = tl & 1;
       if (ESM && ti.ok) {
-        // warp 2 lane 0 loads this tile's X_k block once every warp has released the
-        // previous one; the load runs while the tile's MMAs finish
+        // warp 2 lane 0 loads this tile's X_k block once the previous tile's stores have
+        // read the stage; the load runs while the tile's MMAs finish
         bool ok2 = true;
         if (warp == 2) {
           if (lane == 0) {
-            if (eph > 0) ok2 = mbar_wait(smem_u32(&bar_efree), (eph - 1) & 1, &s_abort);
+            bulk_wait_read0();
             if (ok2) {
               const uint32_t eb = smem_u32(&bar_efull);
               const uint32_t es = sbase + EOFF;
@@ -739,16 +809,47 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       tc_fence_before();  // our TMEM reads are ordered before the release below
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
-      if (ESM && ti.ok) {
-        if (lane == 0) mbar_arrive(smem_u32(&bar_efree));
+      if (ESM && ti.ok && eok) {
+        fence_proxy_async_smem();   // this thread's stage writes, visible to the TMA store
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&bar_odone));
+        bool ok3 = true;
+        if (ti.diag) {
+          ok3 = mbar_wait(smem_u32(&bar_odone), eph & 1, &s_abort);
+          if (ok3) {
+            stage_symmetrize(smem + EOFF, (warp - 2) * 32 + lane);
+            fence_proxy_async_smem();
+          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&bar_osym));
+        }
+        if (warp == 2 && lane == 0 && ok3) {
+          const bool ok4 = ti.diag ? mbar_wait(smem_u32(&bar_osym), sph & 1, &s_abort)
+                                   : mbar_wait(smem_u32(&bar_odone), eph & 1, &s_abort);
+          if (ok4) {
+            const uint32_t es = sbase + EOFF;
+            const int y = ti.row0 + ti.i0;
+            tma_store_2d(&tm_ohi, es + 0 * tc::TILE_BYTES, ti.j0, y);
+            tma_store_2d(&tm_olo, es + 1 * tc::TILE_BYTES, ti.j0, y);
+            tma_store_2d(&tm_ohi, es + 2 * tc::TILE_BYTES, ti.j0 + 64, y);
+            tma_store_2d(&tm_olo, es + 3 * tc::TILE_BYTES, ti.j0 + 64, y);
+            bulk_commit();
+          }
+        }
+        ++eph;
+        if (ti.diag) ++sph;
+        if (!ok3) break;
+      } else if (ESM && ti.ok) {
         ++eph;
       }
       if (!eok) break;
     }
-    // a load that was issued but never waited for (abort) must land before the exit
+    // a load that was issued but never waited for (abort) must land before the exit,
+    // and every store of the stage must have completed
     if (ESM && e_pending)
       for (uint32_t i = 0; i < kSpinLimit; ++i)
         if (mbar_try(smem_u32(&bar_efull), eph & 1)) break;
+    if (ESM && warp == 2 && lane == 0) bulk_wait0();
   }
   tc_fence_before();
   __syncthreads();
@@ -1111,12 +1212,16 @@ static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles,
              !make_tmap(&m[3], a.B_lo, rows, a.ld, a.ld, bf16)) {
     return cudaErrorInvalidValue;
   }
+  CUtensorMap mo[2] = {m[0], m[1]};
+  if (ESM && (!make_tmap(&mo[0], a.out, rows, a.ld, a.ld, bf16) ||
+              !make_tmap(&mo[1], a.out_lo, rows, a.ld, a.ld, bf16)))
+    return cudaErrorInvalidValue;
   auto kern = k_tc_persist<T, EPI, ESM>;
   const int smem = ESM ? tcp::SMEM_BYTES_E : tcp::SMEM_BYTES;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   const int grid = std::min(ntiles, num_sms());
-  kern<<<grid, tcp::NTHR, smem, st>>>(m[0], m[1], m[2], m[3], a, ntiles);
+  kern<<<grid, tcp::NTHR, smem, st>>>(m[0], m[1], m[2], m[3], mo[0], mo[1], a, ntiles);
   note_launch();
   return cudaGetLastError();
 }
