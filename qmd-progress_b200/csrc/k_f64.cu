@@ -21,35 +21,73 @@ __global__ void k_gersh_partial(const double* __restrict__ h, int n, int ld, int
   rowsum[(size_t)blockIdx.y * n + i] = s;
 }
 
-__global__ void k_gersh_final(const double* __restrict__ h, int n, int ld, int nsplit,
-                              const double* __restrict__ rowsum, double* __restrict__ bounds) {
-  // single block: deterministic min/max over rows
-  __shared__ double smin[1024], smax[1024];
+// Row totals, per-block min/max of (h_ii - r_i, h_ii + r_i), and in the last block to
+// arrive the min/max over the blocks in block order; a NaN or overflow anywhere makes
+// both bounds NaN.
+__device__ __forceinline__ double nan_min(double a, double b) {
+  return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : fmin(a, b);
+}
+__device__ __forceinline__ double nan_max(double a, double b) {
+  return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(a, b);
+}
+__global__ void __launch_bounds__(256)
+    k_gersh_final(const double* __restrict__ h, int n, int ld, int nsplit,
+                  const double* __restrict__ rowsum, double* partials, unsigned* counter,
+                  double* __restrict__ bounds) {
+  __shared__ double smin[256], smax[256];
+  __shared__ int s_last;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double mn = 1e308, mx = -1e308;
-  bool bad = false;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  if (i < n) {
     double r = 0.0;
     for (int s = 0; s < nsplit; ++s) r += rowsum[(size_t)s * n + i];
     const double d = h[i + (size_t)i * ld];
-    if (!(r == r) || !(d == d) || fabs(r) > 1e300 || fabs(d) > 1e300) bad = true;
-    mn = fmin(mn, d - r);
-    mx = fmax(mx, d + r);
+    if (!(r == r) || !(d == d) || fabs(r) > 1e300 || fabs(d) > 1e300) {
+      mn = mx = __longlong_as_double(0x7ff8000000000000ll);
+    } else {
+      mn = d - r;
+      mx = d + r;
+    }
   }
-  if (bad) mn = mx = nan("");
   smin[threadIdx.x] = mn;
   smax[threadIdx.x] = mx;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if ((int)threadIdx.x < o) {
-      const double a = smin[threadIdx.x + o], b = smax[threadIdx.x + o];
-      smin[threadIdx.x] = (a != a || smin[threadIdx.x] != smin[threadIdx.x]) ? nan("") : fmin(smin[threadIdx.x], a);
-      smax[threadIdx.x] = (b != b || smax[threadIdx.x] != smax[threadIdx.x]) ? nan("") : fmax(smax[threadIdx.x], b);
+      smin[threadIdx.x] = nan_min(smin[threadIdx.x], smin[threadIdx.x + o]);
+      smax[threadIdx.x] = nan_max(smax[threadIdx.x], smax[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = smin[0];
+    partials[2 * blockIdx.x + 1] = smax[0];
+    __threadfence();
+    s_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  mn = 1e308;
+  mx = -1e308;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    mn = nan_min(mn, __ldcg(partials + 2 * b));
+    mx = nan_max(mx, __ldcg(partials + 2 * b + 1));
+  }
+  smin[threadIdx.x] = mn;
+  smax[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      smin[threadIdx.x] = nan_min(smin[threadIdx.x], smin[threadIdx.x + o]);
+      smax[threadIdx.x] = nan_max(smax[threadIdx.x], smax[threadIdx.x + o]);
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     bounds[0] = smin[0];
     bounds[1] = smax[0];
+    *counter = 0u;
   }
 }
 
@@ -62,12 +100,13 @@ int gersh_nsplit(int n) {
 }
 
 cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsplit,
-                         double* bounds, cudaStream_t st) {
+                         double* bounds, double* partials, unsigned* counter, cudaStream_t st) {
   const int ncol = (n + nsplit - 1) / nsplit;
   dim3 grid((n + 255) / 256, nsplit);
   k_gersh_partial<<<grid, 256, 0, st>>>(h, n, ld, ncol, rowsum);
   note_launch();
-  k_gersh_final<<<1, 1024, 0, st>>>(h, n, ld, nsplit, rowsum, bounds);
+  k_gersh_final<<<(n + 255) / 256, 256, 0, st>>>(h, n, ld, nsplit, rowsum, partials, counter,
+                                                  bounds);
   note_launch();
   return cudaGetLastError();
 }
@@ -87,18 +126,21 @@ __global__ void k_normalize_f64(const double* __restrict__ h, int n, int ld, int
   const double mm = emax - emin;
   const double alpha = -1.0 / mm, beta = emax / mm;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  const size_t total = (size_t)np * np;
-  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(idx / np), c = (int)(idx % np);
-    double v = 0.0;
-    if (r < n && c < n) {
-      v = alpha * h[(size_t)r * ld + c];
-      if (r == c) v += beta;
+  // groups of 8 consecutive elements of one row (np is a multiple of 128)
+  const uint32_t gpr = (uint32_t)np / 8, ngroups = gpr * (uint32_t)np;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    const int r = (int)(g / gpr), c0 = (int)(g - (uint32_t)r * gpr) * 8;
+    double v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int c = c0 + e;
+      v[e] = (r < n && c < n) ? alpha * h[(size_t)r * ld + c] + (r == c ? beta : 0.0) : 0.0;
+      s[0] += v[e] * v[e];
+      if (r == c) s[1] += v[e];
     }
-    x[idx] = v;
-    s[0] += v * v;
-    if (r == c) s[1] += v;
+    double2* dst = reinterpret_cast<double2*>(x + (size_t)r * np + c0);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dst[e] = make_double2(v[2 * e], v[2 * e + 1]);
   }
   block_sum<4>(s, red);
   if (threadIdx.x == 0) {

@@ -145,29 +145,34 @@ __global__ void k_oz_scale(OzScale* sc, int np) {
 // 2. Residue planes: R_t = rint(2^S X) mod m_t in the symmetric range (signed 8-bit).
 //    Plane t is np x np at res + t * np * np.
 // ---------------------------------------------------------------------------------
+// A residue of M = mh 2^21 + ml modulo m, any representative with |r| <= 127 (the
+// products only need r = M mod m and |r| <= 128).  v = mh (2^21 mod m) + ml is an integer
+// below 2^24 in magnitude, exact in FP32; q = rint(v / m) is off the nearest integer by at
+// most one ulp of v/m, so r = v - q m is exact and |r| <= m/2 + 0.005 m.
 template <int t>
-__device__ __forceinline__ int8_t oz_residue(int mh, int ml) {
+__device__ __forceinline__ int8_t oz_residue(float mhf, float mlf, int ml) {
   constexpr int m = oz::mod(t);
   if constexpr (m == 256) {
     return (int8_t)(uint8_t)(ml & 255);
   } else {
-    constexpr int c = oz::pow2_mod(21, m);   // 2^21 mod m
-    int r = (mh * c + ml) % m;                // |mh c + ml| < 2^31: exact, r in (-m, m)
-    if (r > (m - 1) / 2) r -= m;
-    else if (r < -((m - 1) / 2)) r += m;
-    return (int8_t)r;
+    constexpr float c = (float)oz::pow2_mod(21, m);
+    constexpr float inv = 1.0f / (float)m;
+    const float v = fmaf(mhf, c, mlf);
+    const float q = rintf(v * inv);
+    return (int8_t)__float2int_rn(fmaf(-q, (float)m, v));
   }
 }
 
 template <int t>
 __device__ __forceinline__ void oz_store_planes(int8_t* res, size_t plane, size_t off,
-                                                const int (&mh)[16], const int (&ml)[16]) {
+                                                const float (&mh)[16], const float (&mlf)[16],
+                                                const int (&ml)[16]) {
   if constexpr (t < oz::T) {
     alignas(16) int8_t v[16];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = oz_residue<t>(mh[q], ml[q]);
+    for (int q = 0; q < 16; ++q) v[q] = oz_residue<t>(mh[q], mlf[q], ml[q]);
     *reinterpret_cast<uint4*>(res + (size_t)t * plane + off) = *reinterpret_cast<const uint4*>(v);
-    oz_store_planes<t + 1>(res, plane, off, mh, ml);
+    oz_store_planes<t + 1>(res, plane, off, mh, mlf, ml);
   }
 }
 
@@ -187,18 +192,21 @@ __global__ void k_oz_residues(const T* __restrict__ hi, const T* __restrict__ lo
     reinterpret_cast<uint4*>(hv)[1] = reinterpret_cast<const uint4*>(hi + off)[1];
     reinterpret_cast<uint4*>(lv)[0] = reinterpret_cast<const uint4*>(lo + off)[0];
     reinterpret_cast<uint4*>(lv)[1] = reinterpret_cast<const uint4*>(lo + off)[1];
-    int mh[16], ml[16];
+    float mh[16], mlf[16];
+    int ml[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       // |x| <= sqrt(r2max), so |M| < sqrt(prod/2) < 2^36: exact in FP64, and the split
-      // M = mh 2^21 + ml (0 <= ml < 2^21, |mh| < 2^15) is exact in int32.
+      // M = mh 2^21 + ml (0 <= ml < 2^21, |mh| < 2^15) is exact in FP32 and int32.
       const double x = fma(SP::kInv, SP::d(lv[q]), SP::d(hv[q]));
       const double M = S < 0 ? 0.0 : rint(x * scale);
       const double h = floor(M * 0x1p-21);
-      mh[q] = (int)h;
-      ml[q] = (int)(M - h * 0x1p21);
+      const double l = M - h * 0x1p21;
+      mh[q] = (float)h;
+      mlf[q] = (float)l;
+      ml[q] = (int)l;
     }
-    oz_store_planes<0>(res, plane, off, mh, ml);
+    oz_store_planes<0>(res, plane, off, mh, mlf, ml);
   }
 }
 
@@ -338,7 +346,7 @@ __global__ void __launch_bounds__(oz::NTHR, 1)
       const int t = w / p.ntiles;
       const int2 tile = p.tiles[w - t * p.ntiles];
       const int a = tl & 1;
-      if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
+      if (!mbar_wait_idle(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
       // P mod m: u = P + off (off a multiple of m, u < 2^32), floor(u / m) by a 64-bit
       // reciprocal (exact for u < 2^32 since 2^-32 < 1/m).
@@ -382,33 +390,67 @@ __global__ void __launch_bounds__(oz::NTHR, 1)
 //    of the upper tiles.  One CTA per upper 32 x 32 block pair; the mirror goes through
 //    shared memory so both halves are stored row-contiguous.
 // ---------------------------------------------------------------------------------
-template <int t, int s>
-__device__ __forceinline__ void garner_inner(int& u, const int (&v)[oz::T]) {
-  if constexpr (s < t) {
-    constexpr int m = oz::mod(t);
-    constexpr int c = oz::inv_mod(oz::mod(s) % m, m);
-    u = (int)(((unsigned)(u + 2 * m - v[s]) * (unsigned)c) % (unsigned)m);
-    garner_inner<t, s + 1>(u, v);
+// Pairwise (tree) Chinese remaindering: residues modulo m_a, m_b combine into the residue
+// modulo m_a m_b as x = x_a + m_a ((x_b - x_a) m_a^-1 mod m_b).  Eight odd moduli pair up
+// to four 16-bit moduli, then two 32-bit ones, then one 64-bit modulus M07; the last
+// modulus 256 gives the top digit, whose top bit is the sign (Y >= prod/2).
+__host__ __device__ constexpr uint64_t inv_mod64(uint64_t a, uint64_t m) {
+  int64_t t = 0, nt = 1;
+  int64_t r = (int64_t)m, nr = (int64_t)(a % m);
+  while (nr != 0) {
+    const int64_t q = r / nr;
+    int64_t tmp = t - q * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - q * nr;
+    r = nr;
+    nr = tmp;
   }
+  return (uint64_t)(t < 0 ? t + (int64_t)m : t);
 }
-template <int t>
-__device__ __forceinline__ void garner(int (&v)[oz::T]) {
-  if constexpr (t < oz::T) {
-    int u = v[t];
-    garner_inner<t, 0>(u, v);
-    v[t] = u;
-    garner<t + 1>(v);
-  }
+namespace ozc {
+constexpr uint32_t M01 = 255u * 253u, M23 = 251u * 247u, M45 = 241u * 239u, M67 = 233u * 229u;
+constexpr uint64_t M0123 = (uint64_t)M01 * M23, M4567 = (uint64_t)M45 * M67;
+constexpr uint64_t M07 = M0123 * M4567;   // < 2^64
+constexpr uint32_t I01 = (uint32_t)inv_mod64(255, 253), I23 = (uint32_t)inv_mod64(251, 247);
+constexpr uint32_t I45 = (uint32_t)inv_mod64(241, 239), I67 = (uint32_t)inv_mod64(233, 229);
+constexpr uint32_t I0123 = (uint32_t)inv_mod64(M01 % M23, M23);
+constexpr uint32_t I4567 = (uint32_t)inv_mod64(M45 % M67, M67);
+constexpr uint64_t I07 = inv_mod64(M0123 % M4567, M4567);
+constexpr uint32_t I8 = (uint32_t)inv_mod64(M07 % 256u, 256u);
+}  // namespace ozc
+
+// x_a in [0, ma), x_b in [0, mb) (ma < 2 mb) -> x in [0, ma mb); 16-bit moduli
+template <uint32_t ma, uint32_t mb, uint32_t ia>
+__device__ __forceinline__ uint32_t crt_pair16(uint32_t xa, uint32_t xb) {
+  const uint32_t t = (xb + 2u * mb - (xa % mb)) % mb;
+  return xa + ma * ((t * ia) % mb);
+}
+// 32-bit level: moduli below 2^16, products below 2^32
+template <uint32_t ma, uint32_t mb, uint32_t ia>
+__device__ __forceinline__ uint32_t crt_pair32(uint32_t xa, uint32_t xb) {
+  const uint32_t xam = xa >= mb ? xa - mb : xa;   // xa < ma < 2 mb
+  const uint32_t t = xb >= xam ? xb - xam : xb + mb - xam;
+  return xa + ma * ((t * ia) % mb);
 }
 // Residues (in [0, m_t)) -> the symmetric integer Y, |Y| < prod/2, as a double
-// (Horner from the top digit: every partial value is floor(Y / prefix) and exact until
-// the last steps, which round once each).
-__device__ __forceinline__ double crt_value(int (&v)[oz::T]) {
-  garner<1>(v);
-  double acc = (double)(v[oz::T - 1] >= 128 ? v[oz::T - 1] - 256 : v[oz::T - 1]);
-#pragma unroll
-  for (int t = oz::T - 2; t >= 0; --t) acc = fma(acc, (double)oz::mod(t), (double)v[t]);
-  return acc;
+// (exact below 2^53 in magnitude, one rounding above).
+__device__ __forceinline__ double crt_value(const int (&q)[oz::T]) {
+  using namespace ozc;
+  const uint32_t x01 = crt_pair16<255u, 253u, I01>((uint32_t)q[0], (uint32_t)q[1]);
+  const uint32_t x23 = crt_pair16<251u, 247u, I23>((uint32_t)q[2], (uint32_t)q[3]);
+  const uint32_t x45 = crt_pair16<241u, 239u, I45>((uint32_t)q[4], (uint32_t)q[5]);
+  const uint32_t x67 = crt_pair16<233u, 229u, I67>((uint32_t)q[6], (uint32_t)q[7]);
+  const uint32_t x0123 = crt_pair32<M01, M23, I0123>(x01, x23);
+  const uint32_t x4567 = crt_pair32<M45, M67, I4567>(x45, x67);
+  const uint64_t xam = x0123 >= M4567 ? (uint64_t)x0123 - M4567 : (uint64_t)x0123;
+  const uint64_t t = x4567 >= xam ? x4567 - xam : (uint64_t)x4567 + M4567 - xam;
+  const uint64_t x07 = (uint64_t)x0123 + M0123 * ((t * I07) % M4567);
+  const uint32_t v8 = (((uint32_t)q[8] - (uint32_t)x07) * I8) & 255u;
+  if (v8 == 0) return (double)x07;
+  if (v8 == 255) return -(double)(M07 - x07);
+  const double m07 = (double)M07;
+  return (double)x07 + m07 * (double)(v8 >= 128 ? (int)v8 - 256 : (int)v8);
 }
 
 template <typename T>

@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
         }
         if (!ok2) break;
       }
-      if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
+      if (!mbar_wait_idle(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
       bool eok = true;
       if (ESM && ti.ok) {
@@ -1018,7 +1018,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
     for (int w = pair; w < ntiles; w += npairs, ++tl) {
       const int2 tile = ptiles[w];
       const int a = tl & 1;
-      if (!mbar_wait(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
+      if (!mbar_wait_idle(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
       TileInfo ti;
       const int brow = tile.x * 2 + (int)rank;
@@ -1083,22 +1083,25 @@ __global__ void k_normalize_split(const double* __restrict__ h, int n, int ld, i
   const double mm = emax - emin;
   const double alpha = -1.0 / mm, beta = emax / mm;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  const size_t total = (size_t)np * np;
-  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    const int r = (int)(idx / np), c = (int)(idx % np);
-    double v = 0.0;
-    if (r < n && c < n) {
-      v = alpha * h[(size_t)r * ld + c];
-      if (r == c) v += beta;
+  // groups of 8 consecutive elements of one row (np is a multiple of 128)
+  const uint32_t gpr = (uint32_t)np / 8, ngroups = gpr * (uint32_t)np;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    const int r = (int)(g / gpr), c0 = (int)(g - (uint32_t)r * gpr) * 8;
+    alignas(16) T a8[8], b8[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int c = c0 + e;
+      const double v = (r < n && c < n) ? alpha * h[(size_t)r * ld + c] + (r == c ? beta : 0.0) : 0.0;
+      const T a = TR::from_d(v);
+      const T b = TR::from_d((v - TR::to_d(a)) * TR::kScale);
+      a8[e] = a;
+      b8[e] = b;
+      const double vs = TR::to_d(a) + TR::kInv * TR::to_d(b);
+      s[0] += vs * vs;
+      if (r == c) s[1] += vs;
     }
-    const T a = TR::from_d(v);
-    const T b = TR::from_d((v - TR::to_d(a)) * TR::kScale);
-    hi[idx] = a;
-    lo[idx] = b;
-    const double vs = TR::to_d(a) + TR::kInv * TR::to_d(b);
-    s[0] += vs * vs;
-    if (r == c) s[1] += vs;
+    *reinterpret_cast<uint4*>(hi + (size_t)r * np + c0) = *reinterpret_cast<const uint4*>(a8);
+    *reinterpret_cast<uint4*>(lo + (size_t)r * np + c0) = *reinterpret_cast<const uint4*>(b8);
   }
   block_sum<4>(s, red);
   if (threadIdx.x == 0) {

@@ -62,7 +62,7 @@ struct StepArgs {
 int f64_tile(int np);  // tile edge chosen for this size (64 or 128)
 int f64_ntiles(int np);
 cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsplit,
-                         double* bounds, cudaStream_t st);
+                         double* bounds, double* partials, unsigned* counter, cudaStream_t st);
 int gersh_nsplit(int n);
 cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const double* bounds,
                                  double* x, double* partials, unsigned* counter, SP2Rec* rec0,

@@ -218,7 +218,9 @@ int dense_solve(const DenseJob& j) {
     c->h_small[1] = j.maxeval;
     SP2B_CUDA_TRY(cudaMemcpyAsync(bounds, c->h_small, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
   } else {
-    SP2B_CUDA_TRY(launch_gersh(hdev, n, n, c->rowsum, gersh_nsplit(n), bounds, st));
+    SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
+    SP2B_CUDA_TRY(launch_gersh(hdev, n, n, c->rowsum, gersh_nsplit(n), bounds, c->partials,
+                               c->counter, st));
   }
   SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
   SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
@@ -686,7 +688,9 @@ int sp2b_gershgorin(const double* h, int n, double* mineval, double* maxeval,
     SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, h, nn * sizeof(double), cudaMemcpyHostToDevice, st));
     hd = c->hin;
   }
-  SP2B_CUDA_TRY(launch_gersh(hd, n, n, c->rowsum, gersh_nsplit(n), c->small, st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), st));
+  SP2B_CUDA_TRY(launch_gersh(hd, n, n, c->rowsum, gersh_nsplit(n), c->small, c->partials,
+                               c->counter, st));
   SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small, c->small, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));
   *mineval = c->h_small[0];

@@ -48,6 +48,18 @@ __device__ __forceinline__ bool mbar_wait_limit(uint32_t a, uint32_t parity,
 __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag) {
   return mbar_wait_limit(a, parity, abort_flag, kSpinLimit);
 }
+// Bounded wait for warps that usually wait long (epilogue warps for a tile's MMAs): after
+// a short spin they sleep between polls, leaving issue slots to the MMA and TMA threads.
+__device__ __forceinline__ bool mbar_wait_idle(uint32_t a, uint32_t parity,
+                                               volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try(a, parity)) return true;
+    if ((i & 63u) == 63u && *abort_flag) return false;
+    if (i >= 32) __nanosleep(i < 1024 ? 64 : 256);
+  }
+  *abort_flag = 1;
+  return false;
+}
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
                                             int x, int y) {
   asm volatile(
