@@ -324,7 +324,8 @@ def main():
     exec_flops = 3 * 2.0 * 128 * 128 * npad * (nb * (nb + 1) // 2) if prec != _lib.PREC_FP64 else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "peak_source": f"{src} {peak_key}", "kernel": "k_tc_persist (SP2 step)",
+                "peak_source": f"{src} {peak_key}",
+                "kernel": "k_tc_pair (SP2 step, CTA pairs)" if npad % 256 == 0 else "k_tc_persist (SP2 step)",
                 "avg_launch_ms": step_avg_ms, "launches_timed": step_n.value,
                 "flops_per_launch": flops_launch,
                 "executed_tflops": (exec_flops / (step_avg_ms / 1e3) / 1e12) if exec_flops else None,
