@@ -234,6 +234,21 @@ int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, doubl
  * sp2b_set_step_timing(1) is on (ms, number of timed launches). */
 long long sp2b_launch_count(void);
 
+/* First-order density response by SP2 (forward mode): prg_compute_response_SP2
+ * (src/prg_response_mod.F90:653-782), in the reference's argument order (ham, prt, rsp,
+ * rho, lambda, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol, threshold, verbose).
+ * X follows the alg2 branch rule (no iteration decrement on the break branch, as there),
+ * Delta_0 = alpha H1, Delta <- {X, Delta} or 2 Delta - {X, Delta} with X's branch;
+ * rho = 2 X, rsp = 2 Delta.  FP64 on the DMMA path whatever opts->precision says: each
+ * anticommutator is two upper-tile products (3 N^3 flops per iteration with X^2, the
+ * reference spends three full products).  lambda and threshold are unused (as in the
+ * reference's dense path); pp (length >= maxsp2iter) receives the applied branches and
+ * icount their number (either may be NULL). */
+int sp2b_compute_response_sp2(const double* h0, const double* h1, double* rsp, double* rho, int n,
+                              double lambda, double bndfil, int minsp2iter, int maxsp2iter,
+                              const char* sp2conv, double idemtol, double threshold,
+                              int verbose, int* pp, int* icount, const sp2b_opts* opts);
+
 /* Scale exponent S and largest squared row norm of X of the last INT8 McWeeny
  * refinement on the current device (the residue products are exact for
  * (2^S sqrt(r2max) + sqrt(np)/2)^2 < prod(moduli)/2). */

@@ -1,5 +1,7 @@
 // FP64 kernels: Gershgorin bounds, normalisation, and the symmetric-tile DMMA product
 // with the fused SP2 epilogue.  This is the parity form of the SP2 step (1e-10).
+#include <algorithm>
+
 #include "reduce.cuh"
 
 namespace sp2b {
@@ -89,6 +91,35 @@ __global__ void __launch_bounds__(256)
     bounds[1] = smax[0];
     *counter = 0u;
   }
+}
+
+// Delta_0 = alpha H1 (alpha = -1/(e_max - e_min)) into the zero-padded np x np buffer
+// (src/prg_response_mod.F90:700: bml_scale(alpha, rsp_bml)).
+__global__ void k_resp_init(const double* __restrict__ h1, int n, int ld, int np,
+                            const double* __restrict__ bounds, double* __restrict__ d) {
+  const double alpha = -1.0 / (bounds[1] - bounds[0]);
+  const uint32_t gpr = (uint32_t)np / 8, ngroups = gpr * (uint32_t)np;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngroups; g += gridDim.x * blockDim.x) {
+    const int r = (int)(g / gpr), c0 = (int)(g - (uint32_t)r * gpr) * 8;
+    double v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int c = c0 + e;
+      v[e] = (r < n && c < n) ? alpha * h1[(size_t)r * ld + c] : 0.0;
+    }
+    double2* dst = reinterpret_cast<double2*>(d + (size_t)r * np + c0);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dst[e] = make_double2(v[2 * e], v[2 * e + 1]);
+  }
+}
+
+cudaError_t launch_resp_init(const double* h1, int n, int ld, int np, const double* bounds,
+                             double* d, cudaStream_t st) {
+  const size_t groups = (size_t)np * np / 8;
+  const int g = (int)std::min<size_t>((groups + 255) / 256, 148 * 8);
+  k_resp_init<<<g, 256, 0, st>>>(h1, n, ld, np, bounds, d);
+  note_launch();
+  return cudaGetLastError();
 }
 
 int gersh_nsplit(int n) {
@@ -276,6 +307,9 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
     if (br < 0) return;
     if (br == BR_X2) { alpha = 1.0; beta = 0.0; }
     else { alpha = -1.0; beta = 2.0; }
+    // response products after step k: P1 = a X Delta + b Delta (control 2, the step's
+    // own a, b), then Delta' = a Delta X + P1 (control 3)
+    if (p.control == 3) beta = 1.0;
   }
   int bi, bj, nloc = p.np, core = p.core;
   size_t row0 = 0;

@@ -53,8 +53,9 @@ __device__ inline void publish_and_finalize(const StepArgs& p, double (&s)[4], d
   block_sum<4>(t, red);
   if (threadIdx.x != 0) return;
   *p.counter = 0u;
-  if (!p.control) {
-    for (int q = 0; q < 4; ++q) p.sums_out[q] = t[q];
+  if (p.control != 1) {
+    if (p.sums_out)
+      for (int q = 0; q < 4; ++q) p.sums_out[q] = t[q];
     return;
   }
   const SP2Rec r = p.rec[p.k];
@@ -85,7 +86,19 @@ __device__ inline void publish_and_finalize(const StepArgs& p, double (&s)[4], d
 
 // Handles the start of a control-mode launch.  Returns the branch to apply, or -1 if
 // this launch has nothing to do (loop already finished or stopping before update).
+// Follower launches (control 2, 3: the products of the forward-mode response that run
+// after step k) apply the branch that step k applied, and nothing when step k applied
+// none: step k's last CTA recorded the update count (k + 1) and the branch in rec[k+1].
+// (Reading the done word instead would drop the last update, whose record also ends the
+// loop.)  They write no record.
+__device__ inline int follow_branch(const StepArgs& p) {
+  if (*(volatile const int*)&p.sout->nupd != p.k + 1) return -1;
+  const int b = p.rec[p.k + 1].last_branch;
+  return (b == BR_X2 || b == BR_2X_MINUS_X2) ? b : -1;
+}
+
 __device__ inline int control_prologue(const StepArgs& p) {
+  if (p.control >= 2) return follow_branch(p);
   // The solve-wide done word is set by the launch that finished the loop; every
   // later launch of the same solve (the host launches in chunks) returns at once.
   if (*(volatile const int*)&p.sout->done) return -1;

@@ -32,6 +32,8 @@ enum Algo : int {
   ALGO_BASIC = 4,        // prg_sp2_basic          :49-135
   ALGO_SEQ = 5,          // *_seq / *_seq_inplace / submatrix: replay pp
   ALGO_MIXED = 6,        // mixed-precision alg2 with a precision-aware stop rule
+  ALGO_RESP = 7,         // prg_compute_response_SP2 src/prg_response_mod.F90:653-782 (alg2
+                         // rules, no iteration decrement on the break branch, :751)
 };
 
 enum Conv : int { CONV_NONE = 0, CONV_REL = 1, CONV_ABS = 2 };
@@ -78,9 +80,10 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
   switch (c.algo) {
     case ALGO_ALG2:
     case ALGO_ALG2_GENSEQ:
-    case ALGO_MIXED: {
+    case ALGO_MIXED:
+    case ALGO_RESP: {
       int it = r.iter + 1;
-      double trx = (c.algo == ALGO_ALG2) ? r.trx : r.trx_data;  // genseq: trx = trace(1) (:452)
+      double trx = (c.algo == ALGO_ALG2 || c.algo == ALGO_RESP) ? r.trx : r.trx_data;  // genseq: trx = trace(1) (:452)
       const double trx2 = r.fro2;
       const double tr2xx2 = 2.0 * trx - trx2;                   // :325
       const double trxold = trx;
@@ -94,7 +97,7 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
         trx = trx2;
       } else {                                                  // :343
         d.branch = BR_STOP;
-        it -= 1;
+        if (c.algo != ALGO_RESP) it -= 1;
         trx = trxold;
         stop = 1;
       }

@@ -13,9 +13,11 @@ struct Ctx {
   int dev = -1;
   cudaStream_t stream = nullptr;
   std::mutex mu;
-  // FP64 square buffers (np x np): ping-pong iterates, plus one for McWeeny
-  double* x64[3] = {nullptr, nullptr, nullptr};
-  size_t x64_cap[3] = {0, 0, 0};
+  // FP64 square buffers (np x np): ping-pong iterates [0, 1]; the FP64-DMMA McWeeny
+  // product [2]; the forward-mode response's Delta ping-pong [2, 3] and its first
+  // product / host staging [4]
+  double* x64[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  size_t x64_cap[5] = {0, 0, 0, 0, 0};
   // split-precision iterates (hi/lo ping-pong)
   __half* hi[2] = {nullptr, nullptr};
   __half* lo[2] = {nullptr, nullptr};
@@ -82,6 +84,8 @@ struct DenseJob {
   double* bounds_out;
   int mcweeny;
   int mcweeny_products;  // SP2B_MCW_INT8 or SP2B_MCW_FP64
+  const double* h1;      // forward-mode response: perturbation H1 (nullptr: plain solve)
+  double* rsp;           // ... and its output, the response rho1 = 2 Delta
 };
 
 int dense_solve(const DenseJob& j);

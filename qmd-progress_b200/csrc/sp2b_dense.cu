@@ -182,6 +182,11 @@ int dense_solve(const DenseJob& j) {
     set_last_error("bad argument: pp is NULL");
     return SP2B_BAD_ARG;
   }
+  const bool resp = j.h1 != nullptr;   // forward-mode response (FP64 only)
+  if (resp && (!j.rsp || j.prec != SP2B_PREC_FP64)) {
+    set_last_error("bad argument: response needs rsp and FP64 precision");
+    return SP2B_BAD_ARG;
+  }
   int status = SP2B_OK;
   Ctx* c = get_ctx(&status);
   if (!c) return status;
@@ -200,7 +205,7 @@ int dense_solve(const DenseJob& j) {
   const bool oz = split && j.mcweeny == 1 && j.mcweeny_products == SP2B_MCW_INT8 && np <= 65536;
   const size_t nn = (size_t)n * n;
   SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
-  SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : 2));
+  SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : (resp ? 5 : 2)));
   if (split) SP2B_CUDA_TRY(c->ensure_split(np));
   if (oz) SP2B_CUDA_TRY(c->ensure_oz(np, st));
 
@@ -231,6 +236,15 @@ int dense_solve(const DenseJob& j) {
   else
     SP2B_CUDA_TRY(launch_normalize_f64(hdev, n, n, np, bounds, c->x64[0], c->partials, c->counter,
                                        c->rec, norm_out, st));
+  if (resp) {
+    // Delta_0 = alpha H1 (src/prg_response_mod.F90:700); a host H1 is staged in x64[4]
+    const double* h1dev = j.h1;
+    if (!j.dev_ptrs) {
+      SP2B_CUDA_TRY(cudaMemcpyAsync(c->x64[4], j.h1, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+      h1dev = c->x64[4];
+    }
+    SP2B_CUDA_TRY(launch_resp_init(h1dev, n, n, np, bounds, c->x64[2], st));
+  }
 
   // ---- control inputs ----
   // pp / vv / icount are host arrays in every mode (only matrices follow device_ptrs)
@@ -291,6 +305,26 @@ int dense_solve(const DenseJob& j) {
         SP2B_CUDA_TRY(launch_sym_gemm_f64(a, st));
       }
       if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev[2 * (k - k0) + 1], st));
+      if (resp) {
+        // {X_k, Delta_k} on the upper tiles from two products that follow step k's branch
+        // (a, b) = (1, 0) or (-1, 2): P1 = a X Delta + b Delta, Delta' = a Delta X + P1
+        // (src/prg_response_mod.F90:725-746); both exactly symmetric by construction
+        StepArgs q = a;
+        q.pp_out = nullptr;
+        q.vv_out = nullptr;
+        q.sums_out = c->small + 24;
+        q.control = 2;
+        q.A = c->x64[bin];
+        q.B = q.E = c->x64[2 + bin];
+        q.out = c->x64[4];
+        SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+        q.control = 3;
+        q.A = c->x64[2 + bin];
+        q.B = c->x64[bin];
+        q.E = c->x64[4];
+        q.out = c->x64[2 + bout];
+        SP2B_CUDA_TRY(launch_sym_gemm_f64(q, st));
+      }
     }
     SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_sout, c->sout, sizeof(SolveOut), cudaMemcpyDeviceToHost, st));
     SP2B_CUDA_TRY(cudaStreamSynchronize(st));
@@ -392,6 +426,13 @@ int dense_solve(const DenseJob& j) {
   }
   if (!j.dev_ptrs)
     SP2B_CUDA_TRY(cudaMemcpyAsync(j.rho, rho_dev, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (resp) {
+    // rho1 = 2 Delta (src/prg_response_mod.F90:771); host output staged in x64[4]
+    double* rsp_dev = j.dev_ptrs ? j.rsp : c->x64[4];
+    SP2B_CUDA_TRY(launch_finish_f64(c->x64[2 + fb], np, n, 2.0, rsp_dev, n, st));
+    if (!j.dev_ptrs)
+      SP2B_CUDA_TRY(cudaMemcpyAsync(j.rsp, rsp_dev, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
   if (oz) {
     int S = 0;
     double r2max = 0.0;
@@ -421,7 +462,9 @@ int dense_solve(const DenseJob& j) {
   }
 
   // ---- sequence outputs ----
-  const int iters = so.iter;
+  // (the response loop counts its break iteration, src/prg_response_mod.F90:751; its
+  // icount is the number of applied updates, the length of pp)
+  const int iters = (j.ctl.algo == ALGO_RESP) ? so.nupd : so.iter;
   if (j.pp_out && iters > 0)
     SP2B_CUDA_TRY(cudaMemcpyAsync(j.pp_out, c->pp_dev, iters * sizeof(int), cudaMemcpyDeviceToHost, st));
   if (j.vv_out) {
@@ -538,6 +581,27 @@ static void set_trace_ctl(DenseJob& j, int algo, double bndfil, int minit, int m
   j.ctl.conv = parse_conv(conv);
   j.ctl.idemtol = idemtol;
   j.ctl.occ = bndfil * (double)j.n;
+}
+
+int sp2b_compute_response_sp2(const double* h0, const double* h1, double* rsp, double* rho, int n,
+                              double lambda, double bndfil, int minsp2iter, int maxsp2iter,
+                              const char* sp2conv, double idemtol, double threshold,
+                              int verbose, int* pp, int* icount, const sp2b_opts* opts) {
+  (void)lambda;      // unused by the reference as well (src/prg_response_mod.F90:653)
+  (void)threshold;   // dense products are not thresholded
+  (void)verbose;
+  if (!h0 || !h1 || !rsp || !rho) {
+    set_last_error("bad argument: NULL matrix");
+    return SP2B_BAD_ARG;
+  }
+  DenseJob j = base_job(h0, rho, n, opts);
+  j.prec = SP2B_PREC_FP64;
+  j.h1 = h1;
+  j.rsp = rsp;
+  set_trace_ctl(j, ALGO_RESP, bndfil, minsp2iter, maxsp2iter, sp2conv, idemtol);
+  j.pp_out = pp;
+  j.icount_out = icount;
+  return dense_solve(j);
 }
 
 int sp2b_sp2_alg2(const double* h, double* rho, int n, double threshold, double bndfil,

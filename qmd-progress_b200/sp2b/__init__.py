@@ -23,7 +23,7 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "sp2_alg1_seq_inplace", "sp2_basic", "sp2_submatrix_inplace", "sp2_submatrix",
            "gershgorin", "normalize", "check_idempotency", "sp2sequence", "homolumogap",
            "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "MCW_INT8",
-           "MCW_FP64", "last_refinement_info"]
+           "MCW_FP64", "last_refinement_info", "compute_response_sp2"]
 
 
 @dataclass
@@ -49,6 +49,28 @@ def _ptr(a):
 def _opts(precision, mcweeny, mixed_tol, mcweeny_products=_lib.MCW_INT8):
     return make_opts(precision=precision, mcweeny=mcweeny, mixed_tol=mixed_tol,
                      mcweeny_products=mcweeny_products)
+
+
+def compute_response_sp2(h0, h1, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="Rel",
+                         idemtol=1e-10, lam=0.0, threshold=0.0):
+    """prg_compute_response_SP2 (src/prg_response_mod.F90:653-782): returns
+    (rho, rho1, pp, icount) for H0 and the perturbation H1 (FP64 on the GPU)."""
+    h0 = _f64(h0)
+    h1 = _f64(h1)
+    if h1.shape != h0.shape:
+        raise ValueError("H0 and H1 must have the same shape")
+    n = h0.shape[0]
+    rho = np.empty_like(h0)
+    rsp = np.empty_like(h0)
+    pp = np.zeros(max(maxsp2iter, 1) + 2, dtype=np.int32)
+    ic = C.c_int(0)
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_compute_response_sp2(_ptr(h0), _ptr(h1), _ptr(rsp), _ptr(rho), n, lam, bndfil,
+                                          minsp2iter, maxsp2iter, _conv(sp2conv), idemtol,
+                                          threshold, 0, _ptr(pp), C.byref(ic), C.byref(o)),
+          "compute_response_sp2")
+    k = ic.value
+    return rho, rsp, pp[:k].tolist(), k
 
 
 def last_refinement_info():

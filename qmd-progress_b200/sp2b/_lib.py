@@ -84,6 +84,8 @@ _SIGS = {
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
+    "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
+                                       C.c_char_p, C.c_double, C.c_double, _i, _vp, _ip, _vp]),
     "sp2b_refinement_timing": (_i, [_dp, C.POINTER(C.c_longlong)]),
     "sp2b_selftest_wait_timeout": (_i, [_i]),
     "sp2b_set_step_timing": (_i, [_i]),
