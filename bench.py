@@ -9,8 +9,8 @@ solve H -> D.  Inputs (8192^2 FP64 = 512 MiB) are larger than L2 (126 MB), so no
 flush is needed between steps.
 
   value   solves/s with H resident in HBM (device pointers through the C ABI)
-  e2e     solves/s through the C ABI with host buffers: H2D of H and D2H of D inside
-          every step
+  e2e     solves/s through the C ABI with host buffers: H2D of H (its upper triangle,
+          the library's contract for symmetric H) and D2H of D inside every step
   fp64    the same solve in FP64 (the parity form) for the mixed/FP64 ratio
 
 Multi-GPU (torchrun): independent replicas, one Hamiltonian per rank ("replicas only":
@@ -280,8 +280,11 @@ def main():
         e1.record(stream)
         barrier()
         te = max_over_ranks(e0.elapsed_time(e1))
+        # H crosses as its upper triangle (one 2D copy per 128-row panel, the library
+        # rebuilds the rest on the device); D comes back whole, with pp and vv
+        h2d = sum((n - r0) * min(128, n - r0) * 8 for r0 in range(0, n, 128))
         e2e = {"value": world * args.steps / (te / 1e3), "unit": "solves/s",
-               "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8 + 2 * 128 * 8}
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": n * n * 8 + 2 * 128 * 8}
 
     # ---- FP64 (parity form) beside it ----
     fp64 = None

@@ -5,7 +5,10 @@
  * instead of terminating the process the way the reference's Fortran `stop` does
  * (src/prg_sp2_mod.F90:118,362).  Matrices are dense FP64, n x n, column-major
  * (the Fortran / BML dense convention), and symmetric (a Hamiltonian): the library
- * relies on H = H^T and returns an exactly symmetric density matrix.  rho is the
+ * relies on H = H^T and returns an exactly symmetric density matrix.  Host-pointer
+ * calls copy only the elements at offsets i*n + j with j >= i (in Fortran's column-major
+ * terms the lower triangle, H(j+1, i+1) with j >= i) to the device and rebuild the rest
+ * from them; device-pointer calls read the whole matrix.  rho is the
  * spin-summed density, 2x the idempotent projector (src/prg_sp2_mod.F90:375).
  *
  * Matrix arguments (H, rho, the CSR arrays and halo lists of the sub-graph call) are

@@ -122,6 +122,34 @@ cudaError_t launch_resp_init(const double* h1, int n, int ld, int np, const doub
   return cudaGetLastError();
 }
 
+// Lower triangle of a symmetric n x n matrix (row pitch ld) from its upper triangle, by
+// 32 x 32 blocks through shared memory (the host-pointer entries copy only the upper
+// triangle across PCIe).  One CTA per block pair (ib <= jb).
+__global__ void __launch_bounds__(256) k_mirror_lower(double* __restrict__ a, int n, int ld) {
+  __shared__ double t[32][33];
+  int ib, jb;
+  upper_tile(blockIdx.x, ib, jb);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = ib * 32 + ty + 8 * k, c = jb * 32 + tx;
+    t[ty + 8 * k][tx] = (r < n && c < n) ? a[(size_t)r * ld + c] : 0.0;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = jb * 32 + ty + 8 * k, c = ib * 32 + tx;   // (r, c) = mirror of (c, r)
+    if (r < n && c < n && r > c) a[(size_t)r * ld + c] = t[tx][ty + 8 * k];
+  }
+}
+
+cudaError_t launch_mirror_lower(double* a, int n, int ld, cudaStream_t st) {
+  const long long nb = (n + 31) / 32;
+  k_mirror_lower<<<(unsigned)(nb * (nb + 1) / 2), 256, 0, st>>>(a, n, ld);
+  note_launch();
+  return cudaGetLastError();
+}
+
 int gersh_nsplit(int n) {
   const int rows_blocks = (n + 255) / 256;
   int ns = (4 * 148 + rows_blocks - 1) / rows_blocks;

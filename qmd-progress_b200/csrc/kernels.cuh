@@ -73,6 +73,7 @@ cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, doub
                               int ld, cudaStream_t st);
 cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,
                            cudaStream_t st);
+cudaError_t launch_mirror_lower(double* a, int n, int ld, cudaStream_t st);
 cudaError_t launch_resp_init(const double* h1, int n, int ld, int np, const double* bounds,
                              double* d, cudaStream_t st);
 

@@ -144,6 +144,21 @@ cudaError_t Ctx::ensure_oz(int np, cudaStream_t st) {
   return cudaSuccess;
 }
 
+// Host -> device copy of a symmetric n x n matrix: the upper triangle only, one 2D copy
+// per 128-row panel (rows [r0, r0 + 128), columns [r0, n)), ~(n + 128)/(2n) of the bytes;
+// the lower triangle is rebuilt on the device from it.
+static cudaError_t copy_symmetric_h2d(double* dst, const double* src, int n, cudaStream_t st) {
+  for (int r0 = 0; r0 < n; r0 += 128) {
+    const int rows = std::min(128, n - r0);
+    cudaError_t e = cudaMemcpy2DAsync(dst + (size_t)r0 * n + r0, (size_t)n * sizeof(double),
+                                      src + (size_t)r0 * n + r0, (size_t)n * sizeof(double),
+                                      (size_t)(n - r0) * sizeof(double), rows,
+                                      cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_mirror_lower(dst, n, n, st);
+}
+
 // ------------------------------------------------------------------------------------
 // Dense solve
 // ------------------------------------------------------------------------------------
@@ -213,7 +228,7 @@ int dense_solve(const DenseJob& j) {
   const double* hsrc = j.inplace ? j.rho : j.h;
   const double* hdev = hsrc;
   if (!j.dev_ptrs) {
-    SP2B_CUDA_TRY(cudaMemcpyAsync(c->hin, hsrc, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    SP2B_CUDA_TRY(copy_symmetric_h2d(c->hin, hsrc, n, st));
     hdev = c->hin;
   }
   double* bounds = c->small;       // [0..1]
@@ -240,7 +255,7 @@ int dense_solve(const DenseJob& j) {
     // Delta_0 = alpha H1 (src/prg_response_mod.F90:700); a host H1 is staged in x64[4]
     const double* h1dev = j.h1;
     if (!j.dev_ptrs) {
-      SP2B_CUDA_TRY(cudaMemcpyAsync(c->x64[4], j.h1, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+      SP2B_CUDA_TRY(copy_symmetric_h2d(c->x64[4], j.h1, n, st));
       h1dev = c->x64[4];
     }
     SP2B_CUDA_TRY(launch_resp_init(h1dev, n, n, np, bounds, c->x64[2], st));

@@ -255,3 +255,16 @@ def test_int8_mcweeny_against_eigh(cuda):
     assert np.linalg.norm(got.rho - d_ref) / n <= 1e-6
     assert abs(np.trace(got.rho) - n) <= 1e-6 * n
     assert O.check_idempotency(got.rho / 2.0) <= 1e-6
+
+
+def test_host_path_reads_one_triangle(cuda):
+    """Host-pointer calls copy the elements at offsets i*n + j, j >= i, and rebuild the
+    others on the device (H is symmetric by contract): garbage in the other triangle
+    changes nothing."""
+    n = 300
+    h = M.two_band_1d(n, seed=9)
+    ref = sp2b.sp2_alg2(h, 0.5, 0, 100, "None", 1e-10)
+    g = h.copy()
+    g[np.tril_indices(n, -1)] = 1e3
+    got = sp2b.sp2_alg2(g, 0.5, 0, 100, "None", 1e-10)
+    assert np.array_equal(got.rho, ref.rho)
