@@ -288,6 +288,7 @@ def main():
 
     # ---- FP64 (parity form) beside it ----
     fp64 = None
+    rho_mixed = rho_dev.clone() if prec != _lib.PREC_FP64 else None
     if prec != _lib.PREC_FP64 and args.fp64_steps > 0:
         solve_dev(_lib.PREC_FP64)
         barrier()
@@ -301,6 +302,10 @@ def main():
         fp64 = {"solves_per_s": world * args.fp64_steps / (tf / 1e3), "iters": it64,
                 "ms_per_solve": tf / args.fp64_steps,
                 "tflops": world * args.fp64_steps * 2.0 * n ** 3 * it64 / (tf / 1e3) / 1e12}
+        # accuracy of the mixed solve against the FP64 one (same H): ||dD||_F / N
+        dd = float((rho_mixed - rho_dev).norm().item())
+        fp64["mixed_err_fro_over_n"] = dd / n
+        fp64["mixed_err_rel_fro"] = dd / float(rho_dev.norm().item())
 
     clk.__exit__(None, None, None)
     clocks = clk.summary()
