@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=8192)
-    ap.add_argument("--precision", default="mixed_fp16", choices=["mixed_fp16", "mixed_bf16", "fp64"])
+    ap.add_argument("--precision", default="mixed_fp16",
+                    choices=["mixed_fp16", "mixed_bf16", "exact_int8", "fp64"])
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -206,7 +207,7 @@ def main():
     L = _lib.lib()
     n = args.n
     prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
-            "fp64": _lib.PREC_FP64}[args.precision]
+            "exact_int8": _lib.PREC_EXACT_INT8, "fp64": _lib.PREC_FP64}[args.precision]
     h_np = M.two_band_1d(n, seed=rank)
     stream = torch.cuda.current_stream()
     h_dev = torch.from_numpy(h_np).cuda()
@@ -358,8 +359,8 @@ def main():
         out = {"metric": "SP2 solves/s (dense two-band N=%d, mixed precision)" % n, "value": value,
                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f16" if prec == _lib.PREC_MIXED_FP16 else
-               ("bf16" if prec == _lib.PREC_MIXED_BF16 else "f64"),
+               "vs_baseline": None, "dtype": {_lib.PREC_MIXED_FP16: "f16", _lib.PREC_MIXED_BF16: "bf16",
+                                              _lib.PREC_EXACT_INT8: "i8"}.get(prec, "f64"),
                "data": "synthetic",
                "config": {"workload": f"two_band_1d_n{n}_{args.precision}_alg2_mcweeny1", "n": n,
                           "bndfil": 0.5, "idemtol": 1e-10, "sp2_iters": iters,
@@ -481,7 +482,7 @@ def run_subgraph(args, rank, world, local):
         return t, Lb.sp2b_launch_count() - l0
 
     prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
-            "fp64": _lib.PREC_FP64}[args.precision]
+            "exact_int8": _lib.PREC_EXACT_INT8, "fp64": _lib.PREC_FP64}[args.precision]
     with ClockSampler(local) as clk:
         t_ms, launches = timed(prec, args.steps)
     core_mixed = core_d.clone()
@@ -541,7 +542,7 @@ def run_cubic_dense(args, rank, local):
         return ic.value
 
     prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
-            "fp64": _lib.PREC_FP64}[args.precision]
+            "exact_int8": _lib.PREC_EXACT_INT8, "fp64": _lib.PREC_FP64}[args.precision]
     for _ in range(args.warmup):
         solve(prec)
     torch.cuda.synchronize()

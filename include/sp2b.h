@@ -41,6 +41,11 @@ extern "C" {
 #define SP2B_PREC_MIXED_FP16 1  /* FP16 hi+lo split products on tcgen05, FP32 accumulate,
                                    FP64 traces, final FP64 McWeeny step */
 #define SP2B_PREC_MIXED_BF16 2  /* same with BF16 hi+lo operands */
+#define SP2B_PREC_EXACT_INT8 3  /* every SP2 step's X^2 from exact INT8 residue products on
+                                   the tensor cores (X rounded to 2^-S, S ~ 35, then squared
+                                   exactly), X kept in FP64; stops on the alg2 rule or when
+                                   Tr(X - X^2) stagnates; no McWeeny step.  Dense entries
+                                   only; the sub-graph entry computes such calls in FP64. */
 
 /* Products of the McWeeny refinement that ends a mixed solve. */
 #define SP2B_MCW_INT8 0  /* X^2 exact from INT8 residue products (tcgen05 kind::i8) and CRT,

@@ -72,6 +72,17 @@ struct OzScale {
   int pad;
 };
 
+// SP2-step context of the launches that compute one step's X^2 (the exact INT8 mode):
+// they do nothing once the loop has finished or when this step's rule says stop, which
+// the step's last launch (k_oz_crt_step) would decide from the same record.
+__device__ __forceinline__ bool oz_skip(const OzStepCtl& c) {
+  if (!c.active) return false;
+  if (*(volatile const int*)&c.sout->done) return true;
+  const SP2Rec r = c.rec[c.k];
+  if (r.done) return true;
+  return sp2_decide(c.ctl, r, c.k, c.pp_in).branch == BR_STOP;
+}
+
 template <typename T>
 struct OzSplit;
 template <>
@@ -113,6 +124,31 @@ __global__ void k_oz_rownorm(const T* __restrict__ hi, const T* __restrict__ lo,
     }
     s = warp_sum(s);
     // NaN propagates as a maximum: its bit pattern is above every finite value
+    if (!(s <= best)) best = s;
+  }
+  if (lane == 0) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(best);
+    if (best != best) b = 0x7ff8000000000000ull;
+    atomicMax(&sc->r2max_bits, b);
+  }
+}
+
+// The same for an FP64 iterate (exact INT8 mode).
+__global__ void k_oz_rownorm_f64(const double* __restrict__ x, int np, OzScale* sc,
+                                 const OzStepCtl c) {
+  if (oz_skip(c)) return;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  double best = 0.0;
+  for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < np; row += gridDim.x * wpb) {
+    const double2* xr = reinterpret_cast<const double2*>(x + (size_t)row * np);
+    double s = 0.0;
+    for (int c = lane; c < np / 2; c += 32) {
+      const double2 v = xr[c];
+      s = fma(v.x, v.x, s);
+      s = fma(v.y, v.y, s);
+    }
+    s = warp_sum(s);
     if (!(s <= best)) best = s;
   }
   if (lane == 0) {
@@ -210,6 +246,37 @@ __global__ void k_oz_residues(const T* __restrict__ hi, const T* __restrict__ lo
   }
 }
 
+__global__ void k_oz_residues_f64(const double* __restrict__ x, int np,
+                                  const OzScale* __restrict__ sc, int8_t* __restrict__ res,
+                                  const OzStepCtl c) {
+  if (oz_skip(c)) return;
+  const int S = sc->S;
+  const double scale = ldexp(1.0, S < 0 ? 0 : S);
+  const size_t plane = (size_t)np * np;
+  const size_t groups = plane / 16;
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < groups;
+       g += (size_t)gridDim.x * blockDim.x) {
+    const size_t off = g * 16;
+    const double2* src = reinterpret_cast<const double2*>(x + off);
+    float mh[16], mlf[16];
+    int ml[16];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double2 v = src[q];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const double M = S < 0 ? 0.0 : rint((e ? v.y : v.x) * scale);
+        const double h = floor(M * 0x1p-21);
+        const double l = M - h * 0x1p21;
+        mh[2 * q + e] = (float)h;
+        mlf[2 * q + e] = (float)l;
+        ml[2 * q + e] = (int)l;
+      }
+    }
+    oz_store_planes<0>(res, plane, off, mh, mlf, ml);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // 3. Persistent INT8 product of every plane with itself, upper 128 x 256 tiles,
 //    epilogue P mod m_t -> uint8 plane Q_t.
@@ -221,10 +288,12 @@ struct OzGemmArgs {
   const int2* tiles;      // {bi (128-row block), bjp (256-column block)}
   uint8_t* q;             // T planes np x np
   int* err;
+  OzStepCtl ctl;
 };
 
 __global__ void __launch_bounds__(oz::NTHR, 1)
     k_oz_gemm(const __grid_constant__ CUtensorMap tm, const OzGemmArgs p) {
+  if (oz_skip(p.ctl)) return;   // the same answer in every CTA
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[oz::ST];
   __shared__ __align__(8) uint64_t bar_empty[oz::ST];
@@ -500,6 +569,70 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------------
+// 5. Exact INT8 mode: the step's last launch.  X_k^2 from the residues, the branch of
+//    step k from its record (control_prologue), X_{k+1} = a X_k^2 + b X_k in FP64 over
+//    both triangles, and the step's sums {||X_{k+1}||^2, Tr X_{k+1}, ||X_k - X_k^2||^2,
+//    Tr X_k^2} through the last-CTA finalisation, like the other step kernels.  A fixed
+//    grid walks the upper 32 x 32 block pairs (diagonal blocks hold both triangles, whose
+//    squares are equal bit for bit: the integer products are symmetric).
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_oz_crt_step(const uint8_t* __restrict__ q, const OzScale* __restrict__ sc, const StepArgs p) {
+  __shared__ double s_v[32][33];
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+  const int br = control_prologue(p);
+  if (br < 0) return;
+  const double a = br == BR_X2 ? 1.0 : -1.0, b = br == BR_X2 ? 0.0 : 2.0;
+  const int np = p.np;
+  const double* __restrict__ X = (const double*)p.E;
+  double* __restrict__ Xo = (double*)p.out;
+  const int S = sc->S;
+  const double down = S < 0 ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(1.0, -2 * S);
+  const size_t plane = (size_t)np * np;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const long long nb = np / 32, nblk = nb * (nb + 1) / 2;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (long long bid = blockIdx.x; bid < nblk; bid += gridDim.x) {
+    int ib, jb;
+    upper_tile((int)bid, ib, jb);
+    const double w = ib == jb ? 1.0 : 2.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int il = ty + 8 * k;
+      const int i = ib * 32 + il, j = jb * 32 + tx;
+      const size_t e = (size_t)i * np + j;
+      int v[oz::T];
+#pragma unroll
+      for (int t = 0; t < oz::T; ++t) v[t] = q[(size_t)t * plane + e];
+      const double x2 = crt_value(v) * down;
+      const double x = X[e];
+      const double nx = fma(a, x2, b * x);
+      const double d = x - x2;
+      s[0] = fma(w * nx, nx, s[0]);
+      s[2] = fma(w * d, d, s[2]);
+      if (i == j) {
+        s[1] += nx;
+        s[3] += x2;
+      }
+      Xo[e] = nx;
+      s_v[il][tx] = nx;
+    }
+    if (ib != jb) {
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int jl = ty + 8 * k;
+        Xo[(size_t)(jb * 32 + jl) * np + ib * 32 + tx] = s_v[tx][jl];
+      }
+    }
+    __syncthreads();
+  }
+  __threadfence();
+  publish_and_finalize(p, s, red, &s_flag);
+}
+
+// ---------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------
 int oz_nmod() { return oz::T; }
@@ -554,7 +687,7 @@ cudaError_t launch_oz_planes(const __half* xhi, const __half* xlo, int np, int b
 }
 
 cudaError_t launch_oz_gemm(const int8_t* res, int np, uint8_t* qout, const int2* tiles,
-                           int ntiles, int* err, cudaStream_t st) {
+                           int ntiles, int* err, cudaStream_t st, const OzStepCtl* ctl) {
   if (np % oz::BM != 0 || np > 65536 || ntiles <= 0) return cudaErrorInvalidValue;
   CUtensorMap tm;
   if (!make_tmap_box(&tm, res, (long long)oz::T * np, np, np, TMAP_U8, oz::BM))
@@ -568,6 +701,8 @@ cudaError_t launch_oz_gemm(const int8_t* res, int np, uint8_t* qout, const int2*
   a.tiles = tiles;
   a.q = qout;
   a.err = err;
+  if (ctl) a.ctl = *ctl;
+  else memset(&a.ctl, 0, sizeof(a.ctl));
   const int grid = std::min(oz::T * ntiles, oz_sms());
   k_oz_gemm<<<grid, oz::NTHR, oz::SMEM_BYTES, st>>>(tm, a);
   note_launch();
@@ -586,6 +721,30 @@ cudaError_t launch_oz_crt(const uint8_t* q, const __half* xhi, const __half* xlo
                                                   (__nv_bfloat16*)rhi, (__nv_bfloat16*)rlo);
   else
     k_oz_crt<__half><<<nblk, 256, 0, st>>>(q, xhi, xlo, np, sc, x2, rhi, rlo);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_oz_planes_f64(const double* x, int np, void* scale, int8_t* res,
+                                 const OzStepCtl* ctl, cudaStream_t st) {
+  if (np % oz::BM != 0 || np > 65536) return cudaErrorInvalidValue;
+  OzScale* sc = (OzScale*)scale;
+  cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(OzScale), st);
+  if (e != cudaSuccess) return e;
+  const int rgrid = std::min((np + 7) / 8, 148 * 8);
+  k_oz_rownorm_f64<<<rgrid, 256, 0, st>>>(x, np, sc, *ctl);
+  k_oz_scale<<<1, 1, 0, st>>>(sc, np);
+  const size_t groups = (size_t)np * np / 16;
+  const int g = (int)std::min<size_t>((groups + 255) / 256, 148 * 16);
+  k_oz_residues_f64<<<g, 256, 0, st>>>(x, np, sc, res, *ctl);
+  note_launch(3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_oz_crt_step(const uint8_t* q, const void* scale, const StepArgs& a,
+                               cudaStream_t st) {
+  if (a.np % 128 != 0) return cudaErrorInvalidValue;
+  k_oz_crt_step<<<148 * 8, 256, 0, st>>>(q, (const OzScale*)scale, a);
   note_launch();
   return cudaGetLastError();
 }

@@ -103,8 +103,21 @@ size_t oz_scale_bytes();
 void oz_tile_list(int np, std::vector<int2>& out);
 cudaError_t launch_oz_planes(const __half* xhi, const __half* xlo, int np, int bf16,
                              void* scale, int8_t* res, cudaStream_t st);
+// SP2-step context of the launches that compute one step's X^2 in the exact INT8 mode.
+struct OzStepCtl {
+  const SolveOut* sout;
+  const SP2Rec* rec;
+  const int* pp_in;
+  SP2Ctl ctl;
+  int k;
+  int active;   // 0: not part of an SP2 step (the McWeeny refinement)
+};
 cudaError_t launch_oz_gemm(const int8_t* res, int np, uint8_t* qout, const int2* tiles,
-                           int ntiles, int* err, cudaStream_t st);
+                           int ntiles, int* err, cudaStream_t st, const OzStepCtl* ctl = nullptr);
+cudaError_t launch_oz_planes_f64(const double* x, int np, void* scale, int8_t* res,
+                                 const OzStepCtl* ctl, cudaStream_t st);
+cudaError_t launch_oz_crt_step(const uint8_t* q, const void* scale, const StepArgs& a,
+                               cudaStream_t st);
 cudaError_t launch_oz_crt(const uint8_t* q, const __half* xhi, const __half* xlo, int np,
                           int bf16, const void* scale, double* x2, __half* rhi, __half* rlo,
                           cudaStream_t st);

@@ -208,8 +208,13 @@ int dense_solve(const DenseJob& j) {
   std::lock_guard<std::mutex> lk(c->mu);
   cudaStream_t st = j.stream ? j.stream : (j.dev_ptrs ? (cudaStream_t)0 : c->stream);
   const int n = j.n, np = padded(n);
-  const bool split = j.prec != SP2B_PREC_FP64;
+  const bool split = j.prec == SP2B_PREC_MIXED_FP16 || j.prec == SP2B_PREC_MIXED_BF16;
+  const bool exact = j.prec == SP2B_PREC_EXACT_INT8;   // FP64 iterate, INT8 products
   const int bf16 = j.prec == SP2B_PREC_MIXED_BF16;
+  if (!split && !exact && j.prec != SP2B_PREC_FP64) {
+    set_last_error("bad argument: precision %d", j.prec);
+    return SP2B_BAD_ARG;
+  }
   int maxlaunch;
   if (j.ctl.algo == ALGO_SEQ) maxlaunch = j.ctl.icount;
   else if (j.ctl.algo == ALGO_BASIC) maxlaunch = j.ctl.maxit + 1;
@@ -222,7 +227,13 @@ int dense_solve(const DenseJob& j) {
   SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
   SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : (resp ? 5 : 2)));
   if (split) SP2B_CUDA_TRY(c->ensure_split(np));
-  if (oz) SP2B_CUDA_TRY(c->ensure_oz(np, st));
+  if (oz || exact) {
+    if (np > 65536) {
+      set_last_error("bad argument: n=%d above the INT8 products' limit", n);
+      return SP2B_BAD_ARG;
+    }
+    SP2B_CUDA_TRY(c->ensure_oz(np, st));
+  }
 
   // ---- input ----
   const double* hsrc = j.inplace ? j.rho : j.h;
@@ -278,6 +289,15 @@ int dense_solve(const DenseJob& j) {
   a.np = np;
   a.control = 1;
   a.ctl = j.ctl;
+  // Stagnation of Tr(X - X^2) counts once it is within 32 x its rounding floor, ~N eps
+  // for products with relative error eps (2^-22 FP16 hi+lo, 2^-16 BF16 hi+lo, 2^-35
+  // exact INT8 after the 2^-S rounding of X).  The exact mode runs to the alg2 rule or
+  // to that stagnation (no mixed_tol, no McWeeny step).
+  {
+    const double eps = exact ? 0x1p-35 : (bf16 ? 0x1p-16 : 0x1p-22);
+    a.ctl.stag_tol = 32.0 * eps * (double)n;
+    if (exact) a.ctl.mixed_tol = 0.0;
+  }
   a.rec = c->rec;
   a.pp_in = c->pp_dev;
   a.pp_out = pp_out_dev;
@@ -306,7 +326,22 @@ int dense_solve(const DenseJob& j) {
       a.k = k;
       if (timing) SP2B_CUDA_TRY(cudaEventRecord(c->ev[2 * (k - k0)], st));
       const int bin = k & 1, bout = (k + 1) & 1;
-      if (split) {
+      if (exact) {
+        // X_k^2 exactly: residue planes of rint(2^S X_k), nine INT8 products, then the
+        // CRT kernel applies step k's branch and publishes the step's record
+        OzStepCtl oc;
+        oc.sout = c->sout;
+        oc.rec = c->rec;
+        oc.pp_in = c->pp_dev;
+        oc.ctl = a.ctl;
+        oc.k = k;
+        oc.active = 1;
+        SP2B_CUDA_TRY(launch_oz_planes_f64(c->x64[bin], np, c->oz_scale, c->oz_res, &oc, st));
+        SP2B_CUDA_TRY(launch_oz_gemm(c->oz_res, np, c->oz_q, c->oz_tiles, c->oz_ntiles, c->err, st, &oc));
+        a.E = c->x64[bin];
+        a.out = c->x64[bout];
+        SP2B_CUDA_TRY(launch_oz_crt_step(c->oz_q, c->oz_scale, a, st));
+      } else if (split) {
         a.A = a.B = a.E = c->hi[bin];
         a.A_lo = a.B_lo = a.E_lo = c->lo[bin];
         a.out = c->hi[bout];

@@ -80,7 +80,8 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   sp2b_opts_default(&dflt);
   dflt.precision = SP2B_PREC_MIXED_FP16;
   if (!opts) opts = &dflt;
-  const int prec = opts->precision;
+  // the exact INT8 mode has no batched form: such calls run the FP64 batch
+  const int prec = opts->precision == SP2B_PREC_EXACT_INT8 ? SP2B_PREC_FP64 : opts->precision;
   const bool dev = opts->device_ptrs != 0;
   const bool split = prec != SP2B_PREC_FP64;
   int status = SP2B_OK;

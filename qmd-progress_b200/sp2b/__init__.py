@@ -15,14 +15,15 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (MCW_FP64, MCW_INT8, PREC_FP64, PREC_MIXED_BF16, PREC_MIXED_FP16, SP2Error,
-                   check, lib, make_opts)
+from ._lib import (MCW_FP64, MCW_INT8, PREC_EXACT_INT8, PREC_FP64, PREC_MIXED_BF16,
+                   PREC_MIXED_FP16, SP2Error, check, lib, make_opts)
 
 __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq",
            "sp2_alg2_seq_inplace", "sp2_alg1", "sp2_alg1_genseq", "sp2_alg1_seq",
            "sp2_alg1_seq_inplace", "sp2_basic", "sp2_submatrix_inplace", "sp2_submatrix",
            "gershgorin", "normalize", "check_idempotency", "sp2sequence", "homolumogap",
-           "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "MCW_INT8",
+           "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "PREC_EXACT_INT8",
+           "MCW_INT8",
            "MCW_FP64", "last_refinement_info", "compute_response_sp2"]
 
 

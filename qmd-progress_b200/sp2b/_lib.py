@@ -22,6 +22,7 @@ SP2B_NO_DEVICE = 6
 PREC_FP64 = 0
 PREC_MIXED_FP16 = 1
 PREC_MIXED_BF16 = 2
+PREC_EXACT_INT8 = 3
 MCW_INT8 = 0
 MCW_FP64 = 1
 

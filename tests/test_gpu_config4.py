@@ -83,3 +83,10 @@ def test_cubic32_dense_mixed_against_fp64(cuda):
     print(f"config4: {len(pp_m)} mixed / {len(pp_f)} FP64 steps, ||dD||_F/N = {err_over_n:.3e}, "
           f"relative {rel:.3e}")
     assert err_over_n <= 2e-4
+    # the exact INT8 mode on the same lattice: FP64-grade accuracy
+    rho_x, pp_x = _genseq(torch, h, _lib.PREC_EXACT_INT8)
+    kx = min(len(pp_x), len(pp_f))
+    assert pp_x[:kx - 2] == pp_f[:kx - 2]
+    ex = float(rho_x.sub_(rho_f).norm().item()) / n
+    print(f"config4: exact INT8 {len(pp_x)} steps, ||dD||_F/N = {ex:.3e}")
+    assert ex <= 1e-6
