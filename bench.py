@@ -409,7 +409,8 @@ def run_subgraph(args, rank, world, local):
     diag[rows[on]] = val[on]
     rad = np.bincount(rows, weights=np.abs(val), minlength=n) - np.abs(diag)
     emin, emax = float(np.min(diag - rad)), float(np.max(diag + rad))
-    # full-system genseq on the GPU (dense, mixed) for the gap estimate
+    # full-system genseq on the GPU for the gap estimate and the branch sequence, in the
+    # exact INT8 form (FP64-grade, like the reference's double-precision genseq)
     t0 = time.time()
     hd = torch.zeros(n, n, dtype=torch.float64, device="cuda")
     hd[torch.from_numpy(rows).cuda(), torch.from_numpy(col.astype(np.int64)).cuda()] = \
@@ -418,7 +419,7 @@ def run_subgraph(args, rank, world, local):
     pp = np.zeros(128, dtype=np.int32)
     vv = np.zeros(128)
     ic = C.c_int(0)
-    o = _lib.make_opts(precision=_lib.PREC_MIXED_FP16, device_ptrs=True,
+    o = _lib.make_opts(precision=_lib.PREC_EXACT_INT8, device_ptrs=True,
                        stream=torch.cuda.current_stream().cuda_stream)
     _lib.check(Lb.sp2b_sp2_alg2_genseq(hd.data_ptr(), rd.data_ptr(), n, 0.0, 0.5, 0, 100, b"None",
                                        1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
@@ -435,7 +436,7 @@ def run_subgraph(args, rank, world, local):
         # prg_homolumogap threshold on this near-gapless lattice): the parts replay the
         # branch sequence the full-system genseq took
         seq, maxiter = [int(x) for x in pp[:full_iters]], full_iters
-        seq_source = "full-system genseq pp"
+        seq_source = "full-system exact-INT8 genseq pp"
 
     g_csr = G.thresholded_square_graph((rp, col, val), n, 0.6)
     parts = G.rcb_partition(G.lattice_coords(L), args.parts, seed=0, lo=0.4, hi=0.6)
@@ -486,6 +487,8 @@ def run_subgraph(args, rank, world, local):
     with ClockSampler(local) as clk:
         t_ms, launches = timed(prec, args.steps)
     core_mixed = core_d.clone()
+    nref = C.c_int(0)
+    Lb.sp2b_last_subgraph_refined(C.byref(nref), None, 0, None, 0)
     t64, _ = timed(_lib.PREC_FP64, max(1, args.fp64_steps))
     err_vs_fp64 = float((core_mixed - core_d).norm().item()) / n
     rel_vs_fp64 = float((core_mixed - core_d).norm().item() / core_d.norm().item())
@@ -502,7 +505,8 @@ def run_subgraph(args, rank, world, local):
                           "maxiter": maxiter, "full_genseq_iters": full_iters,
                           "homo": eh, "lumo": el, "sequence": seq_source,
                           "graph": "|H^2| > 0.6", "halo": "one jump",
-                          "partition": "RCB U[0.4,0.6]", "setup_s": setup_s},
+                          "partition": "RCB U[0.4,0.6]", "setup_s": setup_s,
+                          "parts_resolved_fp64": nref.value},
                "tflops": value * flops / 1e12, "flops_per_solve": flops,
                "fp64": {"solves_per_s": world * max(1, args.fp64_steps) / (t64 / 1e3),
                         "ms_per_solve": t64 / max(1, args.fp64_steps)},

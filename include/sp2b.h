@@ -56,11 +56,15 @@ extern "C" {
 typedef struct sp2b_opts {
   int precision;     /* SP2B_PREC_* (default FP64) */
   int mcweeny;       /* mixed only: FP64 McWeeny steps after the loop (default 1) */
-  double mixed_tol;  /* mixed only: stop once Tr(X - X^2) < mixed_tol (default 1e-3) */
+  double mixed_tol;  /* mixed only: stop after the update whose product gave
+                        Tr X - Tr X^2 < mixed_tol (default 1e-3) */
   int device_ptrs;   /* 1: matrix arguments are device pointers */
   void* stream;      /* cudaStream_t to run on (NULL: the per-library stream) */
   int verbose;
   int mcweeny_products; /* mixed only: SP2B_MCW_* (default SP2B_MCW_INT8) */
+  double refine_tol; /* sub-graph mixed only: parts whose core rows end with
+                        sum (X - X^2)_ii > refine_tol are solved again in FP64
+                        (default 1e-3; <= 0 turns this off) */
 } sp2b_opts;
 
 /* Fill opts with defaults (FP64, host pointers). */
@@ -200,12 +204,26 @@ int sp2b_subgraph_halos(int n, const long long* g_row_ptr, const int* g_col,
  *   rho_dense optional dense n x n output (may be NULL), core rows filled, rest zero;
  *   vv        maxiter sums over all parts' core rows of (X - X^2)^2, already passed
  *             through sqrt as prg_fnormGraph does (src/prg_graph_mod.F90:933-971).
- * Host or device pointers per opts.device_ptrs. */
+ * Host or device pointers per opts.device_ptrs.
+ *
+ * Split precisions: a part whose final iterate still has a state half-way between
+ * occupied and empty (core-row sum of (X - X^2)_ii above opts.refine_tol) is one whose
+ * density depends on rounding far below the split products' (a level within ~1e-5 of
+ * the chemical potential on a nearly gapless lattice); those parts are solved again
+ * in FP64 and their rows replaced, so they equal the FP64 call's.  vv stays that of
+ * the split-precision solve. */
 int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
                            const double* h_val, int nparts, const long long* halo_ptr,
                            const int* halo_idx, const int* llsize, const int* pp, int maxiter,
                            double mineval, double maxeval, double* rho_core,
                            double* rho_dense, double* vv, const sp2b_opts* opts);
+
+/* Parts the last sp2b_subgraph_sp2_loop call of this thread solved again in FP64:
+ * their number in *count, the first max_parts indices in parts (may be NULL), and the
+ * core-row idempotency sums of every part of that call in idem (nparts entries; may be
+ * NULL; zeros for FP64 calls). */
+int sp2b_last_subgraph_refined(int* count, int* parts, int max_parts, double* idem,
+                               int nparts);
 
 /* ---- device-resident building blocks (used by the torch binding) ------------------ */
 
@@ -232,8 +250,9 @@ int sp2b_dev_adjoint_step_f32(const float* g, const float* x, float* g_out, floa
 
 /* State of the last dense solve on the current device: SP2 step launches issued by
  * the host, X updates applied, Fortran iteration count, status; and, if recs != NULL,
- * up to max_recs control records as 8 doubles each
- * {trx, trx_data, fro2, idemperr, iter, done, status, last_branch}. */
+ * up to max_recs control records as 9 doubles each
+ * {trx, trx_data, fro2, idemperr, iter, done, status, last_branch, trp}; record k + 1
+ * holds the sums of X_{k+1} and trp = Tr X_k^2 as step k computed it. */
 int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, double* recs,
                          int max_recs);
 

@@ -461,9 +461,16 @@ static cudaError_t launch_f64_bt(const StepArgs& a, int bt, int ntiles, cudaStre
     auto kern = k_sym_gemm_f64<128, 2, 4>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
-  } else {
+  } else if (bt == 64) {
     using C = F64Cfg<64, 2, 2>;
     auto kern = k_sym_gemm_f64<64, 2, 2>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
+  } else {
+    // 32-edge tiles for small batches: 8 warps of 16 x 8 so that a tile's k loop is
+    // spread over all four schedulers (each element still sums k in the same order)
+    using C = F64Cfg<32, 2, 4>;
+    auto kern = k_sym_gemm_f64<32, 2, 4>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<ntiles, C::NT, C::SMEM, st>>>(a);
   }
@@ -481,7 +488,7 @@ cudaError_t launch_sym_gemm_f64(const StepArgs& a0, cudaStream_t st) {
 }
 
 cudaError_t launch_sym_gemm_f64_batched(const StepArgs& a, int bt, cudaStream_t st) {
-  if (!a.tiles || a.ntiles <= 0 || (bt != 64 && bt != 128)) return cudaErrorInvalidValue;
+  if (!a.tiles || a.ntiles <= 0 || (bt != 32 && bt != 64 && bt != 128)) return cudaErrorInvalidValue;
   return launch_f64_bt(a, bt, a.ntiles, st);
 }
 

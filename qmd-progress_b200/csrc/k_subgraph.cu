@@ -115,6 +115,46 @@ __global__ void k_scatter_parts(const double* __restrict__ x64, const T* __restr
   }
 }
 
+// Idempotency error of each part's core rows, sum over core rows i of (X - X^2)_ii =
+// X_ii - sum_j X_ij^2 (X symmetric), from the final split iterate.  One CTA per part,
+// fixed summation order.
+template <typename T>
+__global__ void k_part_idem(const T* __restrict__ hi, const T* __restrict__ lo,
+                            const PartDesc* __restrict__ parts, int ld, double* __restrict__ out) {
+  __shared__ double red[32];
+  const PartDesc P = parts[blockIdx.x];
+  double s = 0.0;
+  for (int r = threadIdx.x >> 5; r < P.ncore; r += blockDim.x >> 5) {
+    const size_t row = ((size_t)P.row0 + r) * ld;
+    for (int c = threadIdx.x & 31; c < P.n; c += 32) {
+      const double x =
+          SplitOps<T>::to_d(hi[row + c]) + SplitOps<T>::kInv * SplitOps<T>::to_d(lo[row + c]);
+      s -= x * x;
+      if (c == r) s += x;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    out[blockIdx.x] = t;
+  }
+}
+
+cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const PartDesc* parts,
+                             int nparts, int ld, double* out, cudaStream_t st) {
+  if (prec == SP2B_PREC_MIXED_BF16)
+    k_part_idem<__nv_bfloat16><<<nparts, 256, 0, st>>>((const __nv_bfloat16*)hi,
+                                                        (const __nv_bfloat16*)lo, parts, ld, out);
+  else
+    k_part_idem<__half><<<nparts, 256, 0, st>>>((const __half*)hi, (const __half*)lo, parts, ld,
+                                                out);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_extract_csr(const long long* rp, const int* col, const double* val,
                                const PartDesc* parts, int nparts, const int* halo,
                                const int* skey, const int* sval, int ld, double* xs,

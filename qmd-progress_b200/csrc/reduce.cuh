@@ -61,8 +61,11 @@ __device__ inline void publish_and_finalize(const StepArgs& p, double (&s)[4], d
   const SP2Rec r = p.rec[p.k];
   SP2Decision d = sp2_decide(p.ctl, r, p.k, p.pp_in);
   SP2Rec nx = d.next;
+  if (p.ctl.algo == ALGO_MIXED) sp2_mixed_stop(p.ctl, r, t[3], nx);
   nx.fro2 = t[0];
   nx.trx_data = t[1];
+  nx.trp = t[3];
+  nx.pbias = r.fro2 - t[3];
   nx.last_branch = d.branch;
   if (p.pp_out) p.pp_out[p.k] = d.branch;
   if (p.vv_out) {

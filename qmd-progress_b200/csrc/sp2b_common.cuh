@@ -57,7 +57,10 @@ struct SP2Rec {
   double trx_data;     // Tr X_k summed from the stored data
   double fro2;         // ||X_k||_F^2 from stored data (= Tr X_k^2 for symmetric X_k)
   double idemperr, idemperr1, idemperr2;
-  double err_hist[2];  // ALGO_MIXED: Tr(X - X^2) two and one steps back
+  double err_hist[2];  // ALGO_MIXED: Tr X - Tr P of the products two and one steps back
+  double trp;          // Tr P_{k-1}: trace of the product computed by the step that wrote
+                       // this record (as computed, before the branch was applied)
+  double pbias;        // ||X_{k-1}||_F^2 - Tr P_{k-1}: that product's systematic error
   int iter;            // completed Fortran iterations ("iter")
   int done;            // 1: the loop finished before launch k
   int status;          // SP2B_OK or an error code
@@ -85,8 +88,15 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
     case ALGO_RESP: {
       int it = r.iter + 1;
       double trx = (c.algo == ALGO_ALG2 || c.algo == ALGO_RESP) ? r.trx : r.trx_data;  // genseq: trx = trace(1) (:452)
-      const double trx2 = r.fro2;
-      const double tr2xx2 = 2.0 * trx - trx2;                   // :325
+      // ALGO_MIXED steers on the traces the exact recursion would have.  The products'
+      // systematic error (pbias, measured on the last product) lifts every converged
+      // occupied eigenvalue by its share: Tr X runs ahead of the exact trace by about
+      // pbias, and Tr X^2 by twice that.  Uncorrected, the rule steers that excess out
+      // of the frontier states and ends with the wrong ones occupied (on a 32^3 lattice
+      // with FP16 splits the excess reaches 1.7 electrons).
+      const double delta = (c.algo == ALGO_MIXED) ? r.pbias : 0.0;
+      const double trx2 = r.fro2 - 2.0 * delta;
+      const double tr2xx2 = 2.0 * (trx - delta) - trx2;         // :325
       const double trxold = trx;
       const double limdiff = dabs(trx2 - occ) - dabs(tr2xx2 - occ);
       int stop = 0;
@@ -101,25 +111,6 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
         if (c.algo != ALGO_RESP) it -= 1;
         trx = trxold;
         stop = 1;
-      }
-      if (c.algo == ALGO_MIXED && d.branch != BR_STOP) {
-        // Precision-aware stop: the trace noise of the reduced-precision products keeps
-        // limdiff from ever reaching idemtol, so stop (before updating) once the
-        // idempotency error e = Tr(X - X^2) is below mixed_tol, or has not improved over
-        // two steps (the two-step test of src/sp2_tensorcore/src/prg_sp2_tensorcore.cu:312)
-        // while within stag_tol of zero.  The bound matters on nearly gapless spectra,
-        // where e rises and falls for several steps before the quadratic phase (e.g. on
-        // a 16^3 lattice from 0.58 to 0.71 at step 46 of 62), and an unbounded two-step
-        // test stops there, far from convergence.
-        const double e = r.trx_data - r.fro2;
-        if (e <= c.mixed_tol || (r.iter >= 2 && e <= c.stag_tol && e >= r.err_hist[0])) {
-          d.branch = BR_STOP;
-          it -= 1;
-          trx = trxold;
-          stop = 1;
-        }
-        nx.err_hist[0] = r.err_hist[1];
-        nx.err_hist[1] = e;
       }
       nx.idemperr2 = r.idemperr1;                               // :351
       nx.idemperr1 = r.idemperr;
@@ -211,9 +202,30 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
   return d;
 }
 
+// ALGO_MIXED stop test, applied after update k (where the reference's genseq loop tests
+// convergence, src/prg_sp2_mod.F90:500-507) on that loop's own measure: the change of
+// trace e = Tr X_k - Tr P_k, with P_k the product as computed.  The reduced-precision
+// products are biased (the FP32 tensor-core accumulation loses a part in ~1e4 of a
+// 32768-term sum), and the biased map's fixed point has Tr X = Tr P, so e falls to the
+// products' rounding noise there.  Tr(X - X^2) summed from the stored data instead
+// settles at about -Tr(X^2 - P) (-1.66 on a 32^3 lattice with FP16 splits) and would
+// pass a small tolerance while the spectrum is still far from converged.  Stop once e is
+// below mixed_tol, or has not improved over two steps (the two-step test of
+// src/sp2_tensorcore/src/prg_sp2_tensorcore.cu:312) while within stag_tol of zero.  The
+// bound matters on nearly gapless spectra, where e rises and falls for several steps
+// before the quadratic phase (e.g. on a 16^3 lattice from 0.58 to 0.71 at step 46 of
+// 62), and an unbounded two-step test stops there, far from convergence.
+__host__ __device__ inline void sp2_mixed_stop(const SP2Ctl& c, const SP2Rec& r, double trp,
+                                               SP2Rec& nx) {
+  const double e = r.trx_data - trp;
+  if (e <= c.mixed_tol || (r.iter >= 2 && e <= c.stag_tol && e >= r.err_hist[0])) nx.done = 1;
+  nx.err_hist[0] = r.err_hist[1];
+  nx.err_hist[1] = e;
+}
+
 }  // namespace sp2b
 
-#define SP2B_CUDA_TRY(expr)                                                         \
+#define SP2B_CUDA_TRY(expr)                                                       \
   do {                                                                              \
     cudaError_t _e = (expr);                                                        \
     if (_e != cudaSuccess) {                                                        \

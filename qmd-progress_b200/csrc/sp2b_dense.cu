@@ -569,6 +569,7 @@ int sp2b_opts_default(sp2b_opts* o) {
   o->mcweeny = 1;
   o->mixed_tol = 1e-3;
   o->mcweeny_products = SP2B_MCW_INT8;
+  o->refine_tol = 1e-3;
   return SP2B_OK;
 }
 
@@ -957,9 +958,10 @@ int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, doubl
     std::vector<SP2Rec> r(m);
     SP2B_CUDA_TRY(cudaMemcpy(r.data(), c->rec, m * sizeof(SP2Rec), cudaMemcpyDeviceToHost));
     for (int i = 0; i < m; ++i) {
-      double* o = recs + 8 * i;
+      double* o = recs + 9 * i;
       o[0] = r[i].trx; o[1] = r[i].trx_data; o[2] = r[i].fro2; o[3] = r[i].idemperr;
       o[4] = r[i].iter; o[5] = r[i].done; o[6] = r[i].status; o[7] = r[i].last_branch;
+      o[8] = r[i].trp;
     }
   }
   return SP2B_OK;

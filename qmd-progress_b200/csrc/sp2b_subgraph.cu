@@ -48,6 +48,7 @@ struct SubBufs {
   SP2Rec* rec = nullptr;         size_t rec_cap = 0;
   int* pp = nullptr;             size_t pp_cap = 0;
   double* vv = nullptr;          size_t vv_cap = 0;
+  double* idem = nullptr;        size_t idem_cap = 0;   // per-part core idempotency sums
   // layout of the last call (reused when the part lists are unchanged)
   std::vector<long long> last_hp;
   std::vector<int> last_lls, last_hidx;
@@ -60,57 +61,59 @@ struct SubBufs {
   std::vector<unsigned char> exec_key;
 };
 static SubBufs g_sub[64];
+static SubBufs g_sub_ref[64];  // the FP64 re-solve of the parts a split call flags
 
-}  // namespace sp2b
+// Parts of the last sub-graph call of this thread solved again in FP64, and every
+// part's core-row idempotency sum.
+static thread_local std::vector<int> t_refined;
+static thread_local std::vector<double> t_idem;
 
-using namespace sp2b;
+// One batched solve: the part lists are host vectors, H (CSR) and the outputs device
+// arrays.  Stream-ordered on `st`; returns after the solve is complete.
+struct SubJob {
+  int n;
+  const long long* rp;
+  const int* col;
+  const double* val;
+  const std::vector<long long>* hp;
+  const std::vector<int>* lls;
+  const std::vector<int>* hidx;
+  const int* pp;         // host, maxiter entries
+  int maxiter;
+  double mineval, maxeval;
+  int prec;              // SP2B_PREC_FP64 / _MIXED_FP16 / _MIXED_BF16
+  double* core;          // device, packed core rows, or null
+  double* dense;         // device, n x n, or null
+  bool clear_dense;      // zero `dense` before the scatter
+  bool part_idem;        // split only: per-part idempotency sums into b.idem
+};
 
-extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
-                                      const double* h_val, int nparts, const long long* halo_ptr,
-                                      const int* halo_idx, const int* llsize, const int* pp,
-                                      int maxiter, double mineval, double maxeval,
-                                      double* rho_core, double* rho_dense, double* vv,
-                                      const sp2b_opts* opts) {
-  if (n <= 0 || nparts <= 0 || !h_row_ptr || !h_col || !h_val || !halo_ptr || !halo_idx ||
-      !llsize || maxiter < 0 || (maxiter > 0 && !pp) || !(maxeval - mineval > 0.0)) {
-    set_last_error("sp2b_subgraph_sp2_loop: bad argument");
-    return SP2B_BAD_ARG;
-  }
-  sp2b_opts dflt;
-  sp2b_opts_default(&dflt);
-  dflt.precision = SP2B_PREC_MIXED_FP16;
-  if (!opts) opts = &dflt;
-  // the exact INT8 mode has no batched form: such calls run the FP64 batch
-  const int prec = opts->precision == SP2B_PREC_EXACT_INT8 ? SP2B_PREC_FP64 : opts->precision;
-  const bool dev = opts->device_ptrs != 0;
+// Builds (or reuses) the layout, buffers and CUDA graph of `j` in `b`, launches the
+// graph on `st` and waits for it.  vvh receives the per-iteration sums of squares.
+static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
+                         std::vector<double>& vvh) {
+  const std::vector<long long>& hp = *j.hp;
+  const std::vector<int>& lls = *j.lls;
+  const std::vector<int>& hidx = *j.hidx;
+  const int nparts = (int)lls.size();
+  const int maxiter = j.maxiter, n = j.n, prec = j.prec;
   const bool split = prec != SP2B_PREC_FP64;
-  int status = SP2B_OK;
-  Ctx* c = get_ctx(&status);
-  if (!c) return status;
-  std::lock_guard<std::mutex> lk(c->mu);
-  SubBufs& b = g_sub[c->dev];
-  // work is ordered on the caller's stream (device pointers: NULL = the default
-  // stream); the CUDA graph is captured on the library stream and launched on `st`
-  cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : (dev ? (cudaStream_t)0 : c->stream);
+  const long long nhalo = hp[nparts];
   cudaStream_t cap = c->stream;
 
-  // ---- host-side layout (index lists are small; device inputs are fetched) ----
-  std::vector<long long> hp(nparts + 1);
-  std::vector<int> lls(nparts);
-  if (dev) {
-    SP2B_CUDA_TRY(cudaMemcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
-    SP2B_CUDA_TRY(cudaMemcpy(lls.data(), llsize, nparts * sizeof(int), cudaMemcpyDeviceToHost));
-  } else {
-    std::memcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long));
-    std::memcpy(lls.data(), llsize, nparts * sizeof(int));
+  // tile edge of the step kernel: 128 split; FP64 64, or 32 when the 64-tiles of all
+  // parts would not fill the SMs once (a handful of parts, e.g. the re-solve of flagged
+  // ones).  The FP64 sums run in the same k order for every edge, so the results agree
+  // bit for bit.
+  int bt = 128;
+  if (!split) {
+    long long t64 = 0;
+    for (int p = 0; p < nparts; ++p) {
+      const long long t = padded((int)(hp[p + 1] - hp[p])) / 64;
+      t64 += t * (t + 1) / 2;
+    }
+    bt = t64 < 148 ? 32 : 64;
   }
-  const long long nhalo = hp[nparts];
-  const int bt = split ? 128 : 64;  // tile edge of the step kernel
-  std::vector<int> hidx(nhalo);
-  if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
-  else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
-
-  // the tile list depends on the tile edge of the step kernel (128 split, 64 FP64)
   const bool same_layout = b.layout_valid && b.layout_bt == bt && b.last_hp == hp &&
                            b.last_lls == lls && b.last_hidx == hidx;
   if (!same_layout) {
@@ -202,13 +205,10 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     b.layout_valid = true;
   }
   const int ld = b.ld;
-  const long long rows = b.rows, coff = b.coff;
+  const long long rows = b.rows;
   const int ntiles = b.ntiles;
 
   // ---- device buffers ----
-  long long nnz;
-  if (dev) SP2B_CUDA_TRY(cudaMemcpy(&nnz, h_row_ptr + n, sizeof(long long), cudaMemcpyDeviceToHost));
-  else nnz = h_row_ptr[n];
   const size_t packed = (size_t)rows * ld;
   SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
   if (split) {
@@ -219,10 +219,213 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   } else {
     SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
   }
+  const bool idem = split && j.part_idem;
+  if (idem) SP2B_CUDA_TRY(grow_buf(b.idem, b.idem_cap, (size_t)nparts));
   SP2B_CUDA_TRY(grow_buf(b.partials, b.partials_cap, 4 * (size_t)ntiles));
   SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
   SP2B_CUDA_TRY(grow_buf(b.pp, b.pp_cap, (size_t)maxiter + 1));
   SP2B_CUDA_TRY(grow_buf(b.vv, b.vv_cap, (size_t)maxiter + 1));
+  if (maxiter > 0)  // pp is a host array in every mode
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, j.pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
+  double* core_d = j.core;
+  double* dense_d = j.dense;
+
+  // ---- the batched solve, captured once into a graph ----
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.ld = ld;
+  a.np = ld;
+  a.ntiles = ntiles;
+  a.tiles = b.tiles;
+  a.control = 1;
+  a.ctl.algo = ALGO_SEQ;
+  a.ctl.icount = maxiter;
+  a.ctl.n = n;
+  a.rec = b.rec;
+  a.pp_in = b.pp;
+  a.pp_out = nullptr;
+  a.vv_out = b.vv;
+  a.vv_accumulate = 1;
+  a.sout = c->sout;
+  a.partials = b.partials;
+  a.counter = c->counter;
+  a.err = c->err;
+
+  // The captured graph bakes in every pointer, size and scalar it launches with;
+  // reuse it when all of them are unchanged.
+  struct Key {
+    const void* p[22];
+    long long q[10];
+    double d[2];
+  } key;
+  memset(&key, 0, sizeof(key));
+  const void* ptrs[22] = {j.rp, j.col, j.val, core_d, dense_d, b.xs, b.x2, b.hi[0], b.hi[1],
+                          b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
+                          b.sval, b.partials, b.rec, b.pp, (const void*)cap,
+                          idem ? b.idem : nullptr};
+  memcpy(key.p, ptrs, sizeof(ptrs));
+  const long long qs[10] = {n, nparts, rows, ld, maxiter, prec, ntiles, (long long)(size_t)b.vv,
+                            j.clear_dense ? 1 : 0, bt};
+  memcpy(key.q, qs, sizeof(qs));
+  key.d[0] = j.mineval;
+  key.d[1] = j.maxeval;
+  std::vector<unsigned char> kbytes((unsigned char*)&key, (unsigned char*)&key + sizeof(key));
+  const bool reuse = b.exec && b.exec_key == kbytes;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = reuse ? b.exec : nullptr;
+  if (!reuse) {
+    if (b.exec) {
+      cudaGraphExecDestroy(b.exec);
+      b.exec = nullptr;
+    }
+    const long long launches_before = launch_count();  // captured launches do not run yet
+    SP2B_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    auto body = [&]() -> cudaError_t {
+      cudaError_t e;
+      if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), cap)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), cap)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), cap)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), cap)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(b.rec, 0, sizeof(SP2Rec), cap)) != cudaSuccess) return e;
+      if ((e = cudaMemsetAsync(b.vv, 0, ((size_t)maxiter + 1) * sizeof(double), cap)) != cudaSuccess)
+        return e;
+      if (dense_d && j.clear_dense &&
+          (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
+        return e;
+      if ((e = launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval, ld,
+                                  b.xs, cap)) != cudaSuccess)
+        return e;
+      if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval, prec,
+                                 split ? (void*)b.hi[0] : nullptr, split ? (void*)b.lo[0] : nullptr,
+                                 cap)) != cudaSuccess)
+        return e;
+      for (int k = 0; k < maxiter; ++k) {
+        a.k = k;
+        const int bin = k & 1, bout = (k + 1) & 1;
+        if (split) {
+          a.A = a.B = a.E = b.hi[bin];
+          a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
+          a.out = b.hi[bout];
+          a.out_lo = b.lo[bout];
+          e = launch_sym_gemm_tc_batched(a, rows, prec == SP2B_PREC_MIXED_BF16, cap);
+        } else {
+          double* xin = bin ? b.x2 : b.xs;
+          double* xout = bout ? b.x2 : b.xs;
+          a.A = a.B = a.E = xin;
+          a.out = xout;
+          e = launch_sym_gemm_f64_batched(a, bt, cap);
+        }
+        if (e != cudaSuccess) return e;
+      }
+      const int fb = maxiter & 1;
+      if ((e = launch_scatter_parts(fb ? b.x2 : b.xs, split ? (void*)b.hi[fb] : nullptr,
+                                    split ? (void*)b.lo[fb] : nullptr, prec, b.parts, nparts,
+                                    b.halo, ld, core_d, dense_d, n, cap)) != cudaSuccess)
+        return e;
+      if (idem)
+        return launch_part_idem(b.hi[fb], b.lo[fb], prec, b.parts, nparts, ld, b.idem, cap);
+      return cudaSuccess;
+    };
+    const cudaError_t be = body();
+    const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+    set_launch_count(launches_before);
+    if (be != cudaSuccess || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      set_last_error("graph capture failed: %s / %s", cudaGetErrorString(be), cudaGetErrorString(ce));
+      return SP2B_CUDA_ERROR;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      set_last_error("graph instantiate failed: %s", cudaGetErrorString(ie));
+      return SP2B_CUDA_ERROR;
+    }
+    b.exec = exec;
+    b.exec_key = kbytes;
+  }
+  cudaError_t le = cudaGraphLaunch(exec, st);
+  if (le == cudaSuccess) le = cudaStreamSynchronize(st);
+  note_launch(maxiter + 3 + (idem ? 1 : 0));  // extract, normalise, maxiter steps, scatter
+  if (le != cudaSuccess) {
+    set_last_error("graph launch failed: %s", cudaGetErrorString(le));
+    return SP2B_CUDA_ERROR;
+  }
+  vvh.assign(maxiter + 1, 0.0);
+  if (maxiter > 0)
+    SP2B_CUDA_TRY(cudaMemcpy(vvh.data(), b.vv, maxiter * sizeof(double), cudaMemcpyDeviceToHost));
+  int herr = 0;
+  SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr) {
+    set_last_error("a device-side wait timed out");
+    return SP2B_TIMEOUT;
+  }
+  for (int k = 0; k < maxiter; ++k)
+    if (!(vvh[k] == vvh[k])) {
+      set_last_error("non-finite values during sub-graph SP2");
+      return SP2B_BAD_INPUT;
+    }
+  return SP2B_OK;
+}
+
+}  // namespace sp2b
+
+using namespace sp2b;
+
+extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
+                                      const double* h_val, int nparts, const long long* halo_ptr,
+                                      const int* halo_idx, const int* llsize, const int* pp,
+                                      int maxiter, double mineval, double maxeval,
+                                      double* rho_core, double* rho_dense, double* vv,
+                                      const sp2b_opts* opts) {
+  t_refined.clear();
+  t_idem.clear();
+  if (n <= 0 || nparts <= 0 || !h_row_ptr || !h_col || !h_val || !halo_ptr || !halo_idx ||
+      !llsize || maxiter < 0 || (maxiter > 0 && !pp) || !(maxeval - mineval > 0.0)) {
+    set_last_error("sp2b_subgraph_sp2_loop: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  sp2b_opts dflt;
+  sp2b_opts_default(&dflt);
+  dflt.precision = SP2B_PREC_MIXED_FP16;
+  if (!opts) opts = &dflt;
+  // the exact INT8 mode has no batched form: such calls run the FP64 batch
+  const int prec = opts->precision == SP2B_PREC_EXACT_INT8 ? SP2B_PREC_FP64 : opts->precision;
+  const bool dev = opts->device_ptrs != 0;
+  const bool split = prec != SP2B_PREC_FP64;
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  SubBufs& b = g_sub[c->dev];
+  // work is ordered on the caller's stream (device pointers: NULL = the default
+  // stream); the CUDA graph is captured on the library stream and launched on `st`
+  cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : (dev ? (cudaStream_t)0 : c->stream);
+
+  // ---- host-side layout (index lists are small; device inputs are fetched) ----
+  std::vector<long long> hp(nparts + 1);
+  std::vector<int> lls(nparts);
+  if (dev) {
+    SP2B_CUDA_TRY(cudaMemcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
+    SP2B_CUDA_TRY(cudaMemcpy(lls.data(), llsize, nparts * sizeof(int), cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long));
+    std::memcpy(lls.data(), llsize, nparts * sizeof(int));
+  }
+  const long long nhalo = hp[nparts];
+  if (nhalo < 0) {
+    set_last_error("sp2b_subgraph_sp2_loop: bad halo_ptr");
+    return SP2B_BAD_ARG;
+  }
+  std::vector<int> hidx(nhalo);
+  if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
+  else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
+  long long coff = 0;
+  for (int p = 0; p < nparts; ++p) coff += (long long)lls[p] * (hp[p + 1] - hp[p]);
+
+  // ---- H and the outputs on the device ----
+  long long nnz;
+  if (dev) SP2B_CUDA_TRY(cudaMemcpy(&nnz, h_row_ptr + n, sizeof(long long), cudaMemcpyDeviceToHost));
+  else nnz = h_row_ptr[n];
   const long long* rp_d = h_row_ptr;
   const int* col_d = h_col;
   const double* val_d = h_val;
@@ -249,128 +452,59 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
       dense_d = b.dense;
     }
   }
-  if (maxiter > 0)  // pp and vv are host arrays in every mode
-    SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
 
-  // ---- the batched solve, captured once into a graph ----
-  StepArgs a;
-  memset(&a, 0, sizeof(a));
-  a.ld = ld;
-  a.np = ld;
-  a.ntiles = ntiles;
-  a.tiles = b.tiles;
-  a.control = 1;
-  a.ctl.algo = ALGO_SEQ;
-  a.ctl.icount = maxiter;
-  a.ctl.n = n;
-  a.rec = b.rec;
-  a.pp_in = b.pp;
-  a.pp_out = nullptr;
-  a.vv_out = b.vv;
-  a.vv_accumulate = 1;
-  a.sout = c->sout;
-  a.partials = b.partials;
-  a.counter = c->counter;
-  a.err = c->err;
+  const bool refine = split && opts->refine_tol > 0.0 && maxiter > 0;
+  SubJob j{n, rp_d, col_d, val_d, &hp, &lls, &hidx, pp, maxiter, mineval, maxeval, prec,
+           core_d, dense_d, true, refine};
+  std::vector<double> vvh;
+  int rc = batched_solve(c, b, j, st, vvh);
+  if (rc != SP2B_OK) return rc;
 
-  // The captured graph bakes in every pointer, size and scalar it launches with;
-  // reuse it when all of them are unchanged.
-  struct Key {
-    const void* p[21];
-    long long q[8];
-    double d[2];
-  } key;
-  memset(&key, 0, sizeof(key));
-  const void* ptrs[21] = {rp_d, col_d, val_d, core_d, dense_d, b.xs, b.x2, b.hi[0], b.hi[1],
-                          b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
-                          b.sval, b.partials, b.rec, b.pp, (const void*)cap};
-  memcpy(key.p, ptrs, sizeof(ptrs));
-  const long long qs[8] = {n, nparts, rows, ld, maxiter, prec, ntiles, (long long)(size_t)b.vv};
-  memcpy(key.q, qs, sizeof(qs));
-  key.d[0] = mineval;
-  key.d[1] = maxeval;
-  std::vector<unsigned char> kbytes((unsigned char*)&key, (unsigned char*)&key + sizeof(key));
-  const bool reuse = b.exec && b.exec_key == kbytes;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = reuse ? b.exec : nullptr;
-  if (!reuse) {
-  if (b.exec) {
-    cudaGraphExecDestroy(b.exec);
-    b.exec = nullptr;
-  }
-  const long long launches_before = launch_count();  // captured launches do not run yet
-  SP2B_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-  auto body = [&]() -> cudaError_t {
-    cudaError_t e;
-    if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), cap)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), cap)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), cap)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), cap)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(b.rec, 0, sizeof(SP2Rec), cap)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(b.vv, 0, ((size_t)maxiter + 1) * sizeof(double), cap)) != cudaSuccess) return e;
-    if (rho_dense && (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
-      return e;
-    if ((e = launch_extract_csr(rp_d, col_d, val_d, b.parts, nparts, b.halo, b.skey, b.sval, ld,
-                                b.xs, cap)) != cudaSuccess)
-      return e;
-    if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, mineval, maxeval, prec,
-                               split ? (void*)b.hi[0] : nullptr, split ? (void*)b.lo[0] : nullptr,
-                               cap)) != cudaSuccess)
-      return e;
-    for (int k = 0; k < maxiter; ++k) {
-      a.k = k;
-      const int bin = k & 1, bout = (k + 1) & 1;
-      if (split) {
-        a.A = a.B = a.E = b.hi[bin];
-        a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
-        a.out = b.hi[bout];
-        a.out_lo = b.lo[bout];
-        e = launch_sym_gemm_tc_batched(a, rows, prec == SP2B_PREC_MIXED_BF16, cap);
-      } else {
-        double* xin = bin ? b.x2 : b.xs;
-        double* xout = bout ? b.x2 : b.xs;
-        a.A = a.B = a.E = xin;
-        a.out = xout;
-        e = launch_sym_gemm_f64_batched(a, bt, cap);
-      }
-      if (e != cudaSuccess) return e;
+  // ---- FP64 re-solve of the parts left with a half-occupied state ----
+  if (refine) {
+    t_idem.assign(nparts, 0.0);
+    SP2B_CUDA_TRY(cudaMemcpy(t_idem.data(), b.idem, nparts * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<long long> rhp(1, 0);
+    std::vector<int> rlls, ridx;
+    for (int p = 0; p < nparts; ++p) {
+      if (!(t_idem[p] > opts->refine_tol)) continue;
+      t_refined.push_back(p);
+      ridx.insert(ridx.end(), hidx.begin() + hp[p], hidx.begin() + hp[p + 1]);
+      rhp.push_back((long long)ridx.size());
+      rlls.push_back(lls[p]);
     }
-    const int fb = maxiter & 1;
-    return launch_scatter_parts(fb ? b.x2 : b.xs, split ? (void*)b.hi[fb] : nullptr,
-                                split ? (void*)b.lo[fb] : nullptr, prec, b.parts, nparts, b.halo,
-                                ld, core_d, rho_dense ? dense_d : nullptr, n, cap);
-  };
-  const cudaError_t be = body();
-  const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
-  set_launch_count(launches_before);
-  if (be != cudaSuccess || ce != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    set_last_error("graph capture failed: %s / %s", cudaGetErrorString(be), cudaGetErrorString(ce));
-    return SP2B_CUDA_ERROR;
-  }
-  cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ie != cudaSuccess) {
-    set_last_error("graph instantiate failed: %s", cudaGetErrorString(ie));
-    return SP2B_CUDA_ERROR;
-  }
-  b.exec = exec;
-  b.exec_key = kbytes;
-  }
-  cudaError_t le = cudaGraphLaunch(exec, st);
-  if (le == cudaSuccess) le = cudaStreamSynchronize(st);
-  note_launch(maxiter + 3);  // extract, normalise, maxiter steps, scatter
-  if (le != cudaSuccess) {
-    set_last_error("graph launch failed: %s", cudaGetErrorString(le));
-    return SP2B_CUDA_ERROR;
+    if (!t_refined.empty()) {
+      SubBufs& rb = g_sub_ref[c->dev];
+      long long rcoff = 0;
+      for (size_t q = 0; q < rlls.size(); ++q) rcoff += (long long)rlls[q] * (rhp[q + 1] - rhp[q]);
+      double* rcore = nullptr;
+      if (core_d) {
+        SP2B_CUDA_TRY(grow_buf(rb.core, rb.core_cap, (size_t)std::max(rcoff, 1LL)));
+        rcore = rb.core;
+      }
+      SubJob rj{n, rp_d, col_d, val_d, &rhp, &rlls, &ridx, pp, maxiter, mineval, maxeval,
+                SP2B_PREC_FP64, rcore, dense_d, false, false};
+      std::vector<double> rvv;
+      rc = batched_solve(c, rb, rj, st, rvv);
+      if (rc != SP2B_OK) return rc;
+      if (core_d) {
+        // part p's block sits at sum_{q<p} llsize[q]*lsize[q] in both packings
+        long long src = 0;
+        for (size_t q = 0; q < t_refined.size(); ++q) {
+          const int p = t_refined[q];
+          long long dst = 0;
+          for (int r = 0; r < p; ++r) dst += (long long)lls[r] * (hp[r + 1] - hp[r]);
+          const long long m = (long long)lls[p] * (hp[p + 1] - hp[p]);
+          SP2B_CUDA_TRY(cudaMemcpyAsync(core_d + dst, rcore + src, m * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st));
+          src += m;
+        }
+        SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+      }
+    }
   }
 
   // ---- outputs ----
-  std::vector<double> vvh(maxiter + 1, 0.0);
-  if (maxiter > 0)
-    SP2B_CUDA_TRY(cudaMemcpy(vvh.data(), b.vv, maxiter * sizeof(double), cudaMemcpyDeviceToHost));
-  int herr = 0;
-  SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (vv) {
     for (int k = 0; k < maxiter; ++k) vvh[k] = std::sqrt(vvh[k]);  // prg_fnormGraph
     std::memcpy(vv, vvh.data(), maxiter * sizeof(double));
@@ -381,14 +515,15 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     if (rho_dense)
       SP2B_CUDA_TRY(cudaMemcpy(rho_dense, b.dense, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost));
   }
-  if (herr) {
-    set_last_error("a device-side wait timed out");
-    return SP2B_TIMEOUT;
-  }
-  for (int k = 0; k < maxiter; ++k)
-    if (!(vvh[k] == vvh[k])) {
-      set_last_error("non-finite values during sub-graph SP2");
-      return SP2B_BAD_INPUT;
-    }
+  return SP2B_OK;
+}
+
+extern "C" int sp2b_last_subgraph_refined(int* count, int* parts, int max_parts, double* idem,
+                                          int nparts) {
+  if (count) *count = (int)t_refined.size();
+  if (parts)
+    for (int q = 0; q < std::min(max_parts, (int)t_refined.size()); ++q) parts[q] = t_refined[q];
+  if (idem)
+    for (int p = 0; p < nparts; ++p) idem[p] = p < (int)t_idem.size() ? t_idem[p] : 0.0;
   return SP2B_OK;
 }

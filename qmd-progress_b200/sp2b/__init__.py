@@ -24,7 +24,8 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "gershgorin", "normalize", "check_idempotency", "sp2sequence", "homolumogap",
            "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "PREC_EXACT_INT8",
            "MCW_INT8",
-           "MCW_FP64", "last_refinement_info", "compute_response_sp2"]
+           "MCW_FP64", "last_refinement_info", "compute_response_sp2", "subgraph_sp2_loop",
+           "last_subgraph_refined"]
 
 
 @dataclass
@@ -323,8 +324,12 @@ def subgraph_halos(n, g_csr, parts, h_csr=None, double_jump=True):
 
 
 def subgraph_sp2_loop(n, h_csr, halo_ptr, halo_idx, llsize, pp, maxiter, mineval, maxeval,
-                      precision=PREC_MIXED_FP16, dense=True, core=False):
+                      precision=PREC_MIXED_FP16, dense=True, core=False, refine_tol=None):
     """prg_subgraphSP2Loop: returns (rho_dense [n x n] or None, rho_core or None, vv).
+
+    Split precisions re-solve in FP64 the parts whose core rows end with
+    sum (X - X^2)_ii > refine_tol (library default 1e-3; 0 turns it off); see
+    last_subgraph_refined().
 
     rho_dense holds the core rows of every part (rest zero), indexed rho[i, j]; vv is
     the per-iteration Frobenius norm over all parts' core rows (after prg_fnormGraph)."""
@@ -340,10 +345,21 @@ def subgraph_sp2_loop(n, h_csr, halo_ptr, halo_idx, llsize, pp, maxiter, mineval
     rho_dense = np.zeros((n, n), order="F") if dense else None
     rho_core = np.zeros(int(np.sum(lls.astype(np.int64) * ls))) if core else None
     vv = np.zeros(max(maxiter, 1))
-    o = make_opts(precision=precision)
+    o = make_opts(precision=precision, refine_tol=refine_tol)
     check(lib().sp2b_subgraph_sp2_loop(n, _ptr(rp), _ptr(col), _ptr(val), nparts, _ptr(hptr), _ptr(hidx),
                                        _ptr(lls), _ptr(pp_a), maxiter, mineval, maxeval,
                                        _ptr(rho_core) if core else None,
                                        rho_dense.ctypes.data_as(C.c_void_p) if dense else None,
                                        _ptr(vv), C.byref(o)), "subgraph_sp2_loop")
     return rho_dense, rho_core, vv[:maxiter]
+
+
+def last_subgraph_refined(nparts=0):
+    """(parts re-solved in FP64, per-part core idempotency sums) of this thread's last
+    subgraph_sp2_loop call."""
+    cnt = C.c_int(0)
+    lib().sp2b_last_subgraph_refined(C.byref(cnt), None, 0, None, 0)
+    parts = np.zeros(max(cnt.value, 1), dtype=np.int32)
+    idem = np.zeros(max(nparts, 1))
+    lib().sp2b_last_subgraph_refined(C.byref(cnt), _ptr(parts), cnt.value, _ptr(idem), nparts)
+    return [int(p) for p in parts[:cnt.value]], idem[:nparts]

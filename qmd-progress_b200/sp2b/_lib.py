@@ -33,7 +33,7 @@ STATUS_NAMES = {0: "SP2B_OK", 1: "SP2B_NOT_CONVERGED", 2: "SP2B_BAD_ARG", 3: "SP
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("mcweeny", C.c_int), ("mixed_tol", C.c_double),
                 ("device_ptrs", C.c_int), ("stream", C.c_void_p), ("verbose", C.c_int),
-                ("mcweeny_products", C.c_int)]
+                ("mcweeny_products", C.c_int), ("refine_tol", C.c_double)]
 
 
 class SP2Error(RuntimeError):
@@ -83,6 +83,7 @@ _SIGS = {
     "sp2b_dev_sp2_step_f32": (_i, [_vp, _vp, _i, _i, _vp]),
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
+    "sp2b_last_subgraph_refined": (_i, [_ip, _vp, _i, _vp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
@@ -149,9 +150,11 @@ def check(status: int, where: str):
 
 
 def make_opts(precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3, device_ptrs=False, stream=None,
-              mcweeny_products=MCW_INT8):
+              mcweeny_products=MCW_INT8, refine_tol=None):
     o = Opts()
     lib().sp2b_opts_default(C.byref(o))
+    if refine_tol is not None:
+        o.refine_tol = refine_tol
     o.precision = precision
     o.mcweeny = mcweeny
     o.mcweeny_products = mcweeny_products

@@ -179,8 +179,8 @@ def test_mixed_fp16_against_fp64(cuda, n):
     got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10, precision=sp2b.PREC_MIXED_FP16)
     k = min(len(got.pp), len(ref.pp))
     assert got.pp[:k] == ref.pp[:k]
-    # the mixed loop stops once Tr(X - X^2) < mixed_tol and lets the FP64 McWeeny step
-    # finish, so it never runs longer than the FP64 loop
+    # the mixed loop stops after the update whose product gave Tr X - Tr X^2 < mixed_tol
+    # and lets the McWeeny step finish, so it runs at most one step past the FP64 loop
     assert len(got.pp) <= len(ref.pp) + 1
     err = np.linalg.norm(got.rho - ref.rho) / n
     assert err <= 1e-6, err

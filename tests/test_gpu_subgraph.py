@@ -139,3 +139,46 @@ def test_distributed_path_single_rank_gpu_solver(cuda, tmp_path):
         dist.destroy_process_group()
     assert np.array_equal(rho, rho_loc)
     assert np.allclose(vv, vv_loc, rtol=1e-12, atol=0)
+
+
+def test_subgraph_refinement_replaces_flagged_parts_with_fp64(cuda):
+    """Parts whose split-precision result keeps sum_core (X - X^2)_ii above refine_tol are
+    solved again in FP64: their rows then equal the FP64 call's bit for bit (the FP64
+    batch sums in the same order whatever the tile edge), the dense and packed outputs
+    agree, and refine_tol = 0 leaves every part split-precision.  The sequence is cut
+    short so that the parts are still unconverged and the sums spread out."""
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    mi = maxiter - 6
+    h_csr = sp2b.dense_to_csr(h)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, h_csr)
+    off = np.concatenate([[0], np.cumsum(lls.astype(np.int64) * ls)])
+
+    def run(prec, tol, dense=False):
+        rho, core, _ = sp2b.subgraph_sp2_loop(n, h_csr, hp, hi, lls, pp[:mi], mi, emin, emax,
+                                              precision=prec, dense=dense, core=True,
+                                              refine_tol=tol)
+        return rho, core, sp2b.last_subgraph_refined(len(lls))
+
+    _, c64, _ = run(sp2b.PREC_FP64, None)
+    _, c0, (flag0, idem) = run(sp2b.PREC_MIXED_FP16, 0.0)
+    assert flag0 == []
+    _, _, (_, idem1) = run(sp2b.PREC_MIXED_FP16, None)
+    assert np.array_equal(idem, np.zeros_like(idem))      # nothing computed when off
+    # the device sums equal the ones recomputed from the packed rows
+    for p in range(len(lls)):
+        x = c0[off[p]:off[p + 1]].reshape(lls[p], ls[p]) / 2
+        ref = np.trace(x[:, :lls[p]]) - np.sum(x * x)
+        assert abs(idem1[p] - ref) <= 1e-9 * max(1.0, abs(ref))
+    assert idem1.max() > 0
+    tol = float(np.median(idem1[idem1 > 0]))
+    rho, core, (flagged, _) = run(sp2b.PREC_MIXED_FP16, tol, dense=True)
+    assert flagged == [int(p) for p in np.nonzero(idem1 > tol)[0]] and flagged
+    for p in range(len(lls)):
+        blk = slice(off[p], off[p + 1])
+        if p in flagged:
+            assert np.array_equal(core[blk], c64[blk])
+        else:
+            assert np.array_equal(core[blk], c0[blk])
+        idx = hi[hp[p]:hp[p + 1]]
+        assert np.array_equal(rho[np.ix_(idx[:lls[p]], idx)], core[blk].reshape(lls[p], ls[p]))
