@@ -347,8 +347,12 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
     const int r0 = ti.i0 + q * 32;   // first row of this warp
     // On a diagonal tile the blocks wholly below the diagonal (a prefix of this warp's
     // chunks) carry weight zero and are stored through their mirror images: skipped.
+    // The batched form (ESM) computes a diagonal tile whole instead: every element stands
+    // for itself in the sums, every warp has the same four chunks, and the tile leaves by
+    // TMA as computed.
     int first = 0;
-    while (first < 64 / tcp::CHUNK && ti.diag && ti.j0 + half * 64 + first * tcp::CHUNK + 15 < r0)
+    while (!ESM && first < 64 / tcp::CHUNK && ti.diag &&
+           ti.j0 + half * 64 + first * tcp::CHUNK + 15 < r0)
       ++first;
     // the rows of X_k for the next chunk are fetched while this one is processed
     uint4 pf[4];
@@ -402,7 +406,46 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       // exact when hh is within a factor 2 of x, and the FMA rounds once.
       const bool above = !ti.diag || c0 > r0 + 31;   // every element has r < c
       const bool uniform = above && (ti.core <= 0 || c0 + 15 < ti.core || c0 >= ti.core);
-      if (uniform) {
+      if (ESM && ti.diag) {
+        // whole diagonal tile: weight 1 in the norm, the row's core flag in the residual;
+        // the diagonal element of this lane's row (if in this chunk) is picked by selects
+        float s0a = 0.f, s0b = 0.f, s2a = 0.f, s2b = 0.f;
+        float dvs = 0.f, dhh = 0.f, dxx = 0.f;
+        const int jd = r - c0;   // this row's diagonal element is column j = jd
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float hhf = __uint_as_float(hh[j]), xxf = __uint_as_float(xx[j]);
+          const float P = fmaf(kInvF, xxf, hhf);
+          const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
+          const float val = fmaf(af, P, bf * x);
+          const T h = TR::from_f(val);
+          const float hf = TR::to_f(h);
+          const T l = TR::from_f((val - hf) * kScaleF);
+          const float dres = fmaf(-kInvF, xxf, x - hhf);
+          nhi[j] = h;
+          nlo[j] = l;
+          if (j & 1) {
+            s0b = fmaf(val, val, s0b);
+            s2b = fmaf(dres, dres, s2b);
+          } else {
+            s0a = fmaf(val, val, s0a);
+            s2a = fmaf(dres, dres, s2a);
+          }
+          if (c0 + 15 >= r0 && c0 <= r0 + 31) {   // warp-uniform: the chunk meets the diagonal
+            const bool dg = j == jd;
+            dvs = dg ? fmaf(kInvF, TR::to_f(l), hf) : dvs;
+            dhh = dg ? hhf : dhh;
+            dxx = dg ? xxf : dxx;
+          }
+        }
+        const bool rin = ti.core <= 0 || r < ti.core;
+        sums[0] += (double)s0a + (double)s0b;
+        if (rin) sums[2] += (double)s2a + (double)s2b;
+        if (jd >= 0 && jd < 16) {
+          sums[1] += (double)dvs;
+          sums[3] += fma(TR::kInv, (double)dxx, (double)dhh);
+        }
+      } else if (uniform) {
         float s0a = 0.f, s0b = 0.f, s2a = 0.f, s2b = 0.f;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
@@ -429,28 +472,48 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
         sums[0] = fma(2.0, (double)s0a + (double)s0b, sums[0]);
         sums[2] = fma((double)wc, (double)s2a + (double)s2b, sums[2]);
       } else {
+        // Blocks on the diagonal or across the core boundary: the same FP32 chains with
+        // per-element weights (selects, no branches); the diagonal element's value and
+        // product (the traces of X_{k+1} and of the product) enter the FP64 sums once.
+        float s0a = 0.f, s0b = 0.f, s2a = 0.f, s2b = 0.f;
+        float dvs = 0.f, dhh = 0.f, dxx = 0.f;
+        const int core = ti.core;
+        const float rin = (core <= 0 || r < core) ? 1.f : 0.f;   // row r is a core row
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int c = c0 + j;
-          const float P = fmaf(kInvF, __uint_as_float(xx[j]), __uint_as_float(hh[j]));
+          const float hhf = __uint_as_float(hh[j]), xxf = __uint_as_float(xx[j]);
+          const float P = fmaf(kInvF, xxf, hhf);
           const float x = fmaf(kInvF, TR::to_f(elo[j]), TR::to_f(ehi[j]));
           const float val = fmaf(af, P, bf * x);
           const T h = TR::from_f(val);
-          const T l = TR::from_f((val - TR::to_f(h)) * kScaleF);
-          const double vs = (double)fmaf(kInvF, TR::to_f(l), TR::to_f(h));
+          const float hf = TR::to_f(h);
+          const T l = TR::from_f((val - hf) * kScaleF);
+          const float vs = fmaf(kInvF, TR::to_f(l), hf);
+          const float dres = fmaf(-kInvF, xxf, x - hhf);
           nhi[j] = h;
           nlo[j] = l;
-          const int w = sym_weight(ti.diag, r, c);
-          // the residual X - X^2 (vv) needs the product at accumulator precision
-          const double Pd = fma(TR::kInv, (double)__uint_as_float(xx[j]),
-                                (double)__uint_as_float(hh[j]));
-          const double dres = (double)x - Pd;
-          sums[0] = fma((double)w * vs, vs, sums[0]);
-          sums[2] = fma((double)core_weight(w, r, c, ti.core) * dres, dres, sums[2]);
-          if (r == c) {
-            sums[1] += vs;
-            sums[3] += Pd;
+          // sym_weight / core_weight as selects
+          const bool dg = r == c;
+          const float wf = (!ti.diag || r < c) ? 2.f : (dg ? 1.f : 0.f);
+          const float cin = (core <= 0 || c < core) ? 1.f : 0.f;
+          const float cwf = core <= 0 ? wf : (wf == 0.f ? 0.f : (dg ? rin : rin + cin));
+          dvs = dg ? vs : dvs;
+          dhh = dg ? hhf : dhh;
+          dxx = dg ? xxf : dxx;
+          if (j & 1) {
+            s0b = fmaf(wf * vs, vs, s0b);
+            s2b = fmaf(cwf * dres, dres, s2b);
+          } else {
+            s0a = fmaf(wf * vs, vs, s0a);
+            s2a = fmaf(cwf * dres, dres, s2a);
           }
+        }
+        sums[0] += (double)s0a + (double)s0b;
+        sums[2] += (double)s2a + (double)s2b;
+        if (r >= c0 && r < c0 + 16) {
+          sums[1] += (double)dvs;
+          sums[3] += fma(TR::kInv, (double)dxx, (double)dhh);
         }
       }
       if (ESM) {
@@ -459,7 +522,8 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
         *reinterpret_cast<uint4*>(eb + k1) = reinterpret_cast<const uint4*>(nhi)[1];
         *reinterpret_cast<uint4*>(eb + tc::TILE_BYTES + k0) = reinterpret_cast<const uint4*>(nlo)[0];
         *reinterpret_cast<uint4*>(eb + tc::TILE_BYTES + k1) = reinterpret_cast<const uint4*>(nlo)[1];
-        if (ti.diag || !Ohi) continue;   // a diagonal tile is its own mirror
+        if (ti.diag) continue;   // computed whole: stored as it is
+        if (!Ohi) continue;
         T* th = reinterpret_cast<T*>(scr);          // [16][32]: mirror rows c0 + j
         T* tl = reinterpret_cast<T*>(scr + 1024);
 #pragma unroll
@@ -577,49 +641,14 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
   }
 }
 
-// Lower triangle of a staged diagonal tile := transpose of its upper triangle, so that the
-// stored X_{k+1} is exactly symmetric (the MMA's values below the diagonal are not the
-// mirror of those above it bit for bit).  Layout as the X_k stage: box (half h, array a)
-// at (2h + a) * TILE_BYTES, row r at r * 128, 16-byte chunk k at (k ^ (r & 7)) * 16.
-// Thread t of the 256 epilogue threads handles row t / 2, every other 8-column chunk.
-__device__ __forceinline__ uint32_t stage_off(int a, int row, int col) {
-  const int h = col >> 6, cl = col & 63;
-  return (uint32_t)((h * 2 + a) * tc::TILE_BYTES + row * 128 + ((((cl >> 3) ^ (row & 7))) << 4) +
-                    ((cl & 7) << 1));
-}
-__device__ __forceinline__ void stage_symmetrize(uint8_t* stage, int t) {
-  const int r = t >> 1;
-  const int nk = (r + 7) >> 3;   // chunks holding some column c < r
-  for (int k = t & 1; k < nk; k += 2) {
-    const int cmax = min(8, r - 8 * k);
-#pragma unroll
-    for (int a = 0; a < 2; ++a) {
-      uint16_t v[8];
-#pragma unroll
-      for (int e = 0; e < 8; ++e)
-        v[e] = e < cmax ? *reinterpret_cast<const uint16_t*>(stage + stage_off(a, 8 * k + e, r)) : 0;
-      if (cmax == 8) {
-        uint4 w;
-        w.x = (uint32_t)v[0] | ((uint32_t)v[1] << 16);
-        w.y = (uint32_t)v[2] | ((uint32_t)v[3] << 16);
-        w.z = (uint32_t)v[4] | ((uint32_t)v[5] << 16);
-        w.w = (uint32_t)v[6] | ((uint32_t)v[7] << 16);
-        *reinterpret_cast<uint4*>(stage + stage_off(a, r, 8 * k)) = w;
-      } else {
-        for (int e = 0; e < cmax; ++e)
-          *reinterpret_cast<uint16_t*>(stage + stage_off(a, r, 8 * k + e)) = v[e];
-      }
-    }
-  }
-}
-
 // EPI 0: SP2 step epilogue (A = B = E = X_k).  EPI 1: McWeeny combine of the INT8
 // refinement, D = 2 X^2 - acc with acc = X (4R) (A = X, B = 4R = 4(X^2 - X), E = X^2 in
 // FP64), written to the n_out x n_out density (row pitch ld_out) and mirrored.
 // ESM (batched sub-graph steps): two operand stages; the tile's X_k block comes by TMA
 // into a 64 KB stage (loaded while the tile's MMAs run), X_{k+1} is written over it and
-// leaves by TMA stores (tm_ohi / tm_olo: the output arrays), a diagonal tile symmetrised
-// in shared memory first; only off-diagonal mirrors use ordinary stores.
+// leaves by TMA stores (tm_ohi / tm_olo: the output arrays); a diagonal tile is computed
+// whole (both triangles, as the MMA gives them); only off-diagonal mirrors use ordinary
+// stores.
 template <typename T, int EPI, bool ESM>
 __global__ void __launch_bounds__(tcp::NTHR, 1)
     k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
@@ -639,7 +668,6 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   __shared__ __align__(8) uint64_t bar_final;
   __shared__ __align__(8) uint64_t bar_efull;   // ESM: X_k block landed
   __shared__ __align__(8) uint64_t bar_odone;   // ESM: every warp wrote its part of X_{k+1}
-  __shared__ __align__(8) uint64_t bar_osym;    // ESM: diagonal tile symmetrised
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
@@ -669,7 +697,6 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     mbar_init(smem_u32(&bar_final), 1);
     mbar_init(smem_u32(&bar_efull), 1);
     mbar_init(smem_u32(&bar_odone), tcp::EPI_WARPS);
-    mbar_init(smem_u32(&bar_osym), tcp::EPI_WARPS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), tcp::TMEM_COLS);
@@ -768,7 +795,6 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t tl = 0;
     uint32_t eph = 0;          // ESM: X_k blocks loaded (and consumed) so far
-    uint32_t sph = 0;          // ESM: diagonal tiles symmetrised so far
     bool e_pending = false;    // ESM, issuing thread: a load not yet waited for
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
       const TileInfo ti = persist_tile(p, t);
@@ -814,19 +840,9 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&bar_odone));
         bool ok3 = true;
-        if (ti.diag) {
+        if (warp == 2 && lane == 0) {
           ok3 = mbar_wait(smem_u32(&bar_odone), eph & 1, &s_abort);
           if (ok3) {
-            stage_symmetrize(smem + EOFF, (warp - 2) * 32 + lane);
-            fence_proxy_async_smem();
-          }
-          __syncwarp();
-          if (lane == 0) mbar_arrive(smem_u32(&bar_osym));
-        }
-        if (warp == 2 && lane == 0 && ok3) {
-          const bool ok4 = ti.diag ? mbar_wait(smem_u32(&bar_osym), sph & 1, &s_abort)
-                                   : mbar_wait(smem_u32(&bar_odone), eph & 1, &s_abort);
-          if (ok4) {
             const uint32_t es = sbase + EOFF;
             const int y = ti.row0 + ti.i0;
             tma_store_2d(&tm_ohi, es + 0 * tc::TILE_BYTES, ti.j0, y);
@@ -837,7 +853,6 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
           }
         }
         ++eph;
-        if (ti.diag) ++sph;
         if (!ok3) break;
       } else if (ESM && ti.ok) {
         ++eph;
