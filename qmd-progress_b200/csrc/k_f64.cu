@@ -445,6 +445,144 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
   publish_and_finalize(p, s, red, &s_flag);
 }
 
+// All SP2 steps of a batch of parts in one cooperative launch (see MultiStepArgs).
+// Tile math and the order of every sum are those of k_sym_gemm_f64<32, 2, 4>, so each
+// part's result equals that of the per-step launches bit for bit; the per-step sums
+// (traces, vv) are not formed.  Between steps every CTA of a part adds one to the part's
+// counter and waits, with a bounded spin, until the part's tiles have all finished the
+// step; operands are read through L2 (cp.async.cg, ld.global.cg), never a stale L1 line.
+__global__ void __launch_bounds__(256, 1) k_f64_multistep(const MultiStepArgs a) {
+  using C = F64Cfg<32, 2, 4>;
+  extern __shared__ __align__(16) double sm[];
+  const int4 t = a.tiles[blockIdx.x];
+  const size_t row0 = (size_t)t.x;
+  const int bi = t.y >> 16, bj = t.y & 0xffff, nloc = t.z, part = t.w;
+  const unsigned per = (unsigned)a.part_tiles[part];
+  const int i0 = bi * 32, j0 = bj * 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wm = warp / 4, wn = warp % 4;   // WM = 2, WN = 4
+  const int ld = a.ld;
+  const bool tile_ok = i0 < nloc && j0 < nloc;
+  const int KB = tile_ok ? nloc / C::BK : 0;
+  const bool diag = bi == bj;
+  __shared__ int s_bad;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int k = 0; k < a.maxiter; ++k) {
+    const double* __restrict__ X = a.x[k & 1] + row0 * ld;
+    double* __restrict__ out = a.x[(k + 1) & 1] + row0 * ld;
+    const bool sq = a.pp[k] != 0;
+    const double alpha = sq ? 1.0 : -1.0, beta = sq ? 0.0 : 2.0;
+    double acc[C::MI][C::NI][2];
+#pragma unroll
+    for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < C::NI; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
+    auto load = [&](int stage, int kb) {
+      double* As = sm + stage * 2 * C::BK * C::LDS;
+      double* Bs = As + C::BK * C::LDS;
+      const int k0 = kb * C::BK;
+      for (int c = tid; c < C::BK * 32 / 2; c += C::NT) {
+        const int row = c / 16, col = (c % 16) * 2;
+        cp_async16(As + row * C::LDS + col, X + (size_t)(k0 + row) * ld + i0 + col);
+        cp_async16(Bs + row * C::LDS + col, X + (size_t)(k0 + row) * ld + j0 + col);
+      }
+    };
+#pragma unroll
+    for (int s = 0; s < C::ST - 1; ++s) {
+      if (s < KB) load(s, s);
+      cp_async_commit();
+    }
+    for (int kb = 0; kb < KB; ++kb) {
+      cp_async_wait<C::ST - 2>();
+      __syncthreads();
+      {
+        const int nk = kb + C::ST - 1;
+        if (nk < KB) load(nk % C::ST, nk);
+        cp_async_commit();
+      }
+      const double* As = sm + (kb % C::ST) * 2 * C::BK * C::LDS;
+      const double* Bs = As + C::BK * C::LDS;
+#pragma unroll
+      for (int kk = 0; kk < C::BK; kk += 4) {
+        double av[C::MI], bv[C::NI];
+#pragma unroll
+        for (int mi = 0; mi < C::MI; ++mi) av[mi] = As[(kk + t4) * C::LDS + wm * C::TM + mi * 8 + g];
+#pragma unroll
+        for (int ni = 0; ni < C::NI; ++ni) bv[ni] = Bs[(kk + t4) * C::LDS + wn * C::TN + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < C::MI; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < C::NI; ++ni) dmma884(acc[mi][ni], av[mi], bv[ni]);
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();   // every warp is done with the stages before the next step reuses them
+#pragma unroll
+    for (int mi = 0; mi < (tile_ok ? C::MI : 0); ++mi) {
+#pragma unroll
+      for (int ni = 0; ni < C::NI; ++ni) {
+        const int r = i0 + wm * C::TM + mi * 8 + g;
+        const int c = j0 + wn * C::TN + ni * 8 + 2 * t4;
+        const double ex = __ldcg(X + (size_t)r * ld + c), ey = __ldcg(X + (size_t)r * ld + c + 1);
+        const double v0 = alpha * acc[mi][ni][0] + beta * ex;
+        const double v1 = alpha * acc[mi][ni][1] + beta * ey;
+        if (!diag) {
+          *reinterpret_cast<double2*>(out + (size_t)r * ld + c) = make_double2(v0, v1);
+          out[(size_t)c * ld + r] = v0;
+          out[(size_t)(c + 1) * ld + r] = v1;
+        } else {
+          if (r <= c) { out[(size_t)r * ld + c] = v0; out[(size_t)c * ld + r] = v0; }
+          if (r <= c + 1) { out[(size_t)r * ld + c + 1] = v1; out[(size_t)(c + 1) * ld + r] = v1; }
+        }
+      }
+    }
+    // per-part barrier before X_{k+1} is read
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(a.bar + part, 1u);
+      const unsigned target = per * (unsigned)(k + 1);
+      bool ok = false;
+      for (uint32_t it = 0; it < kSpinLimit; ++it) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a.bar + part) : "memory");
+        if (v >= target) { ok = true; break; }
+        if (*(volatile int*)a.err) break;
+        __nanosleep(64);
+      }
+      if (!ok) {
+        atomicExch(a.err, 1);
+        s_bad = 1;
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_bad) return;
+  }
+}
+
+cudaError_t launch_f64_multistep(const MultiStepArgs& a, cudaStream_t st) {
+  using C = F64Cfg<32, 2, 4>;
+  static int max_blocks = -1;
+  if (max_blocks < 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_f64_multistep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_f64_multistep, C::NT, C::SMEM);
+    max_blocks = sms * per_sm;
+  }
+  if (a.ntiles <= 0) return cudaSuccess;
+  if (a.ntiles > max_blocks) return cudaErrorCooperativeLaunchTooLarge;
+  void* args[] = {(void*)&a};
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_f64_multistep, dim3(a.ntiles),
+                                                    dim3(C::NT), args, C::SMEM, st);
+  note_launch();
+  return e;
+}
+
 int f64_tile(int np) {
   const int t128 = np / 128;
   return (t128 * (t128 + 1) / 2 >= 2 * 148) ? 128 : 64;

@@ -69,6 +69,23 @@ cudaError_t launch_normalize_f64(const double* h, int n, int ld, int np, const d
                                  double* norm_out, cudaStream_t st);
 cudaError_t launch_sym_gemm_f64(const StepArgs& a, cudaStream_t st);
 cudaError_t launch_sym_gemm_f64_batched(const StepArgs& a, int bt, cudaStream_t st);
+
+// All maxiter SP2 steps of a small batch of parts (the FP64 re-solve of flagged parts)
+// in one cooperative launch: one CTA per 32 x 32 upper tile; the tiles of a part meet
+// at a per-part barrier (a counter in `bar`, bounded wait) between steps.
+struct MultiStepArgs {
+  double* x[2];          // ping-pong packed buffers; x[0] holds X_0
+  const int4* tiles;     // (row0, bi << 16 | bj, k extent, part)
+  int ntiles;
+  const int* part_tiles; // tiles per part
+  const int* pp;         // device, maxiter branches (0: 2X - X^2, 1: X^2)
+  int maxiter;
+  int ld;
+  unsigned* bar;         // one zeroed counter per part
+  int* err;              // set to 1 when a barrier wait runs out
+};
+// Returns cudaErrorCooperativeLaunchTooLarge when the tiles cannot all be resident.
+cudaError_t launch_f64_multistep(const MultiStepArgs& a, cudaStream_t st);
 cudaError_t launch_finish_f64(const double* x, int np, int n, double scale, double* rho,
                               int ld, cudaStream_t st);
 cudaError_t launch_copy_in(const double* src, int n, int ld, int np, double* x,

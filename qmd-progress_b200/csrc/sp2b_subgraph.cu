@@ -49,6 +49,11 @@ struct SubBufs {
   int* pp = nullptr;             size_t pp_cap = 0;
   double* vv = nullptr;          size_t vv_cap = 0;
   double* idem = nullptr;        size_t idem_cap = 0;   // per-part core idempotency sums
+  // 32-edge FP64 layouts: the tile list of the one-launch multi-step solve
+  int4* ms_tiles = nullptr;      size_t ms_tiles_cap = 0;
+  int* ms_part_tiles = nullptr;  size_t ms_part_tiles_cap = 0;
+  unsigned* ms_bar = nullptr;    size_t ms_bar_cap = 0;
+  int ms_ntiles = 0;
   // layout of the last call (reused when the part lists are unchanged)
   std::vector<long long> last_hp;
   std::vector<int> last_lls, last_hidx;
@@ -86,6 +91,7 @@ struct SubJob {
   double* dense;         // device, n x n, or null
   bool clear_dense;      // zero `dense` before the scatter
   bool part_idem;        // split only: per-part idempotency sums into b.idem
+  bool multistep;        // FP64 only: all steps in one cooperative launch when it fits
 };
 
 // Builds (or reuses) the layout, buffers and CUDA graph of `j` in `b`, launches the
@@ -112,7 +118,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       const long long t = padded((int)(hp[p + 1] - hp[p])) / 64;
       t64 += t * (t + 1) / 2;
     }
-    bt = t64 < 148 ? 32 : 64;
+    bt = (t64 < 148 || j.multistep) ? 32 : 64;
   }
   const bool same_layout = b.layout_valid && b.layout_bt == bt && b.last_hp == hp &&
                            b.last_lls == lls && b.last_hidx == hidx;
@@ -181,6 +187,22 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
                                     P[p].ncore > 0 ? P[p].ncore : -1));
     }
     const int ntiles = (int)tiles.size();
+    if (bt == 32) {
+      // the multi-step launch: one CTA per tile, the part index in place of the core count
+      std::vector<int4> ms;
+      std::vector<int> per(nparts, 0);
+      for (const int4& t : tiles) {
+        const int p = row_part[t.x];
+        ms.push_back(make_int4(t.x, t.y, t.z, p));
+        ++per[p];
+      }
+      SP2B_CUDA_TRY(grow_buf(b.ms_tiles, b.ms_tiles_cap, ms.size()));
+      SP2B_CUDA_TRY(grow_buf(b.ms_part_tiles, b.ms_part_tiles_cap, (size_t)nparts));
+      SP2B_CUDA_TRY(grow_buf(b.ms_bar, b.ms_bar_cap, (size_t)nparts));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(b.ms_tiles, ms.data(), ms.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(b.ms_part_tiles, per.data(), nparts * sizeof(int), cudaMemcpyHostToDevice, st));
+      b.ms_ntiles = (int)ms.size();
+    }
     SP2B_CUDA_TRY(grow_buf(b.parts, b.parts_cap, nparts));
     SP2B_CUDA_TRY(grow_buf(b.tiles, b.tiles_cap, ntiles));
     SP2B_CUDA_TRY(grow_buf(b.row_part, b.row_part_cap, rows));
@@ -229,6 +251,49 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, j.pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
   double* core_d = j.core;
   double* dense_d = j.dense;
+
+  // ---- a few FP64 parts: every step in one cooperative launch ----
+  if (j.multistep && !split && bt == 32 && maxiter > 0) {
+    SP2B_CUDA_TRY(cudaMemsetAsync(b.xs, 0, packed * sizeof(double), st));
+    SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
+    SP2B_CUDA_TRY(cudaMemsetAsync(b.ms_bar, 0, nparts * sizeof(unsigned), st));
+    if (dense_d && j.clear_dense)
+      SP2B_CUDA_TRY(cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), st));
+    SP2B_CUDA_TRY(launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
+                                     ld, b.xs, st));
+    SP2B_CUDA_TRY(launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval,
+                                    prec, nullptr, nullptr, st));
+    MultiStepArgs ma;
+    ma.x[0] = b.xs;
+    ma.x[1] = b.x2;
+    ma.tiles = b.ms_tiles;
+    ma.ntiles = b.ms_ntiles;
+    ma.part_tiles = b.ms_part_tiles;
+    ma.pp = b.pp;
+    ma.maxiter = maxiter;
+    ma.ld = ld;
+    ma.bar = b.ms_bar;
+    ma.err = c->err;
+    const cudaError_t me = launch_f64_multistep(ma, st);
+    if (me == cudaSuccess) {
+      SP2B_CUDA_TRY(launch_scatter_parts((maxiter & 1) ? b.x2 : b.xs, nullptr, nullptr, prec,
+                                         b.parts, nparts, b.halo, ld, core_d, dense_d, n, st));
+      SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+      int herr = 0;
+      SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (herr) {
+        set_last_error("a device-side wait timed out");
+        return SP2B_TIMEOUT;
+      }
+      vvh.assign(maxiter + 1, 0.0);   // the one-launch form forms no per-step sums
+      return SP2B_OK;
+    }
+    if (me != cudaErrorCooperativeLaunchTooLarge) {
+      set_last_error("multi-step launch failed: %s", cudaGetErrorString(me));
+      return SP2B_CUDA_ERROR;
+    }
+    (void)cudaGetLastError();   // too many tiles to be resident at once: per-step launches
+  }
 
   // ---- the batched solve, captured once into a graph ----
   StepArgs a;
@@ -455,7 +520,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
 
   const bool refine = split && opts->refine_tol > 0.0 && maxiter > 0;
   SubJob j{n, rp_d, col_d, val_d, &hp, &lls, &hidx, pp, maxiter, mineval, maxeval, prec,
-           core_d, dense_d, true, refine};
+           core_d, dense_d, true, refine, false};
   std::vector<double> vvh;
   int rc = batched_solve(c, b, j, st, vvh);
   if (rc != SP2B_OK) return rc;
@@ -483,7 +548,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         rcore = rb.core;
       }
       SubJob rj{n, rp_d, col_d, val_d, &rhp, &rlls, &ridx, pp, maxiter, mineval, maxeval,
-                SP2B_PREC_FP64, rcore, dense_d, false, false};
+                SP2B_PREC_FP64, rcore, dense_d, false, false, true};
       std::vector<double> rvv;
       rc = batched_solve(c, rb, rj, st, rvv);
       if (rc != SP2B_OK) return rc;
