@@ -445,6 +445,14 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
   publish_and_finalize(p, s, red, &s_flag);
 }
 
+// Tiles of the one-launch form: 32 x 32, 8 warps of 16 x 8, k blocks of 32 in a 4-deep
+// pipeline (the k order of every sum is that of F64Cfg<32, 2, 4>: 4 at a time, ascending).
+struct MsCfg {
+  static constexpr int BK = 32, NT = 256, LDS = 36, ST = 4;
+  static constexpr int TM = 16, TN = 8, MI = 2, NI = 1;
+  static constexpr size_t SMEM = (size_t)ST * 2 * BK * LDS * sizeof(double);
+};
+
 // All SP2 steps of a batch of parts in one cooperative launch (see MultiStepArgs).
 // Tile math and the order of every sum are those of k_sym_gemm_f64<32, 2, 4>, so each
 // part's result equals that of the per-step launches bit for bit; the per-step sums
@@ -452,7 +460,7 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
 // counter and waits, with a bounded spin, until the part's tiles have all finished the
 // step; operands are read through L2 (cp.async.cg, ld.global.cg), never a stale L1 line.
 __global__ void __launch_bounds__(256, 1) k_f64_multistep(const MultiStepArgs a) {
-  using C = F64Cfg<32, 2, 4>;
+  using C = MsCfg;
   extern __shared__ __align__(16) double sm[];
   const int4 t = a.tiles[blockIdx.x];
   const size_t row0 = (size_t)t.x;
@@ -484,7 +492,7 @@ __global__ void __launch_bounds__(256, 1) k_f64_multistep(const MultiStepArgs a)
       double* Bs = As + C::BK * C::LDS;
       const int k0 = kb * C::BK;
       for (int c = tid; c < C::BK * 32 / 2; c += C::NT) {
-        const int row = c / 16, col = (c % 16) * 2;
+        const int row = c / 16, col = (c % 16) * 2;   // BT / 2 = 16 pieces per row
         cp_async16(As + row * C::LDS + col, X + (size_t)(k0 + row) * ld + i0 + col);
         cp_async16(Bs + row * C::LDS + col, X + (size_t)(k0 + row) * ld + j0 + col);
       }
@@ -564,7 +572,7 @@ __global__ void __launch_bounds__(256, 1) k_f64_multistep(const MultiStepArgs a)
 }
 
 cudaError_t launch_f64_multistep(const MultiStepArgs& a, cudaStream_t st) {
-  using C = F64Cfg<32, 2, 4>;
+  using C = MsCfg;
   static int max_blocks = -1;
   if (max_blocks < 0) {
     int dev = 0, sms = 0, per_sm = 0;

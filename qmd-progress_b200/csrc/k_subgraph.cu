@@ -116,41 +116,50 @@ __global__ void k_scatter_parts(const double* __restrict__ x64, const T* __restr
 }
 
 // Idempotency error of each part's core rows, sum over core rows i of (X - X^2)_ii =
-// X_ii - sum_j X_ij^2 (X symmetric), from the final split iterate.  One CTA per part,
-// fixed summation order.
+// X_ii - sum_j X_ij^2 (X symmetric), from the final split iterate.  Grid (part, 16
+// row groups); each warp reads whole rows in 16-byte pieces (padding columns are zero);
+// out[part * 16 + group] holds the group's partial, summed in a fixed order by the host.
 template <typename T>
 __global__ void k_part_idem(const T* __restrict__ hi, const T* __restrict__ lo,
                             const PartDesc* __restrict__ parts, int ld, double* __restrict__ out) {
   __shared__ double red[32];
   const PartDesc P = parts[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double s = 0.0;
-  for (int r = threadIdx.x >> 5; r < P.ncore; r += blockDim.x >> 5) {
+  for (int r = blockIdx.y * nw + warp; r < P.ncore; r += gridDim.y * nw) {
     const size_t row = ((size_t)P.row0 + r) * ld;
-    for (int c = threadIdx.x & 31; c < P.n; c += 32) {
-      const double x =
-          SplitOps<T>::to_d(hi[row + c]) + SplitOps<T>::kInv * SplitOps<T>::to_d(lo[row + c]);
-      s -= x * x;
-      if (c == r) s += x;
+    for (int c0 = lane * 8; c0 < P.np; c0 += 256) {
+      const uint4 vh = *reinterpret_cast<const uint4*>(hi + row + c0);
+      const uint4 vl = *reinterpret_cast<const uint4*>(lo + row + c0);
+      const T* h8 = reinterpret_cast<const T*>(&vh);
+      const T* l8 = reinterpret_cast<const T*>(&vl);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const double x = SplitOps<T>::to_d(h8[e]) + SplitOps<T>::kInv * SplitOps<T>::to_d(l8[e]);
+        s -= x * x;
+        if (c0 + e == r) s += x;
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  if (lane == 0) red[warp] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-    out[blockIdx.x] = t;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    out[(size_t)blockIdx.x * gridDim.y + blockIdx.y] = t;
   }
 }
 
 cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const PartDesc* parts,
                              int nparts, int ld, double* out, cudaStream_t st) {
+  const dim3 grid(nparts, kPartIdemGroups);
   if (prec == SP2B_PREC_MIXED_BF16)
-    k_part_idem<__nv_bfloat16><<<nparts, 256, 0, st>>>((const __nv_bfloat16*)hi,
-                                                        (const __nv_bfloat16*)lo, parts, ld, out);
+    k_part_idem<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)hi,
+                                                      (const __nv_bfloat16*)lo, parts, ld, out);
   else
-    k_part_idem<__half><<<nparts, 256, 0, st>>>((const __half*)hi, (const __half*)lo, parts, ld,
-                                                out);
+    k_part_idem<__half><<<grid, 256, 0, st>>>((const __half*)hi, (const __half*)lo, parts, ld,
+                                              out);
   note_launch();
   return cudaGetLastError();
 }

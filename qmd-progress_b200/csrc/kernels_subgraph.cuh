@@ -26,7 +26,9 @@ cudaError_t launch_scatter_parts(const double* x64, const void* hi, const void* 
                                  const PartDesc* parts, int nparts, const int* halo, int ld,
                                  double* core_out, double* dense, long long n, cudaStream_t st);
 
-// Sum over each part's core rows of (X - X^2)_ii from the split iterate (hi, lo).
+// Sum over each part's core rows of (X - X^2)_ii from the split iterate (hi, lo), as
+// kPartIdemGroups partial sums per part (out[part * kPartIdemGroups + g]).
+constexpr int kPartIdemGroups = 16;
 cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const PartDesc* parts,
                              int nparts, int ld, double* out, cudaStream_t st);
 

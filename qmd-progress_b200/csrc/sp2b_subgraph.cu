@@ -242,7 +242,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
   }
   const bool idem = split && j.part_idem;
-  if (idem) SP2B_CUDA_TRY(grow_buf(b.idem, b.idem_cap, (size_t)nparts));
+  if (idem) SP2B_CUDA_TRY(grow_buf(b.idem, b.idem_cap, (size_t)nparts * kPartIdemGroups));
   SP2B_CUDA_TRY(grow_buf(b.partials, b.partials_cap, 4 * (size_t)ntiles));
   SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
   SP2B_CUDA_TRY(grow_buf(b.pp, b.pp_cap, (size_t)maxiter + 1));
@@ -527,8 +527,12 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
 
   // ---- FP64 re-solve of the parts left with a half-occupied state ----
   if (refine) {
+    std::vector<double> part((size_t)nparts * kPartIdemGroups);
+    SP2B_CUDA_TRY(cudaMemcpy(part.data(), b.idem, part.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost));
     t_idem.assign(nparts, 0.0);
-    SP2B_CUDA_TRY(cudaMemcpy(t_idem.data(), b.idem, nparts * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < nparts; ++p)
+      for (int g = 0; g < kPartIdemGroups; ++g) t_idem[p] += part[(size_t)p * kPartIdemGroups + g];
     std::vector<long long> rhp(1, 0);
     std::vector<int> rlls, ridx;
     for (int p = 0; p < nparts; ++p) {
