@@ -71,7 +71,8 @@ typedef struct sp2b_opts {
 int sp2b_opts_default(sp2b_opts* opts);
 
 /* Options used by the PROGRESS-named exports (prg_sp2b.h).  Initialised from the
- * environment variable SP2B_PRECISION ("fp64", "mixed", "mixed_bf16") on first use. */
+ * environment variable SP2B_PRECISION ("fp64", "mixed", "mixed_bf16", "exact") on
+ * first use. */
 int sp2b_set_default_opts(const sp2b_opts* opts);
 int sp2b_get_default_opts(sp2b_opts* opts);
 

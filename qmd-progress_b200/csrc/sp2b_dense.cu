@@ -586,6 +586,7 @@ int sp2b_get_default_opts(sp2b_opts* o) {
     if (e) {
       if (!strcmp(e, "mixed") || !strcmp(e, "mixed_fp16")) g_def.precision = SP2B_PREC_MIXED_FP16;
       else if (!strcmp(e, "mixed_bf16")) g_def.precision = SP2B_PREC_MIXED_BF16;
+      else if (!strcmp(e, "exact") || !strcmp(e, "exact_int8")) g_def.precision = SP2B_PREC_EXACT_INT8;
     }
     g_def_init = true;
   }
