@@ -291,6 +291,9 @@ constexpr int SCR_WARP = 2048;                        // store staging per epilo
 constexpr int SCR_OFF = tc::ST * tc::STAGE_BYTES;     // after the operand stages
 constexpr int SMEM_BYTES = SCR_OFF + EPI_WARPS * SCR_WARP + 1024;
 constexpr int E_BYTES = 4 * tc::TILE_BYTES;           // X_k block of a tile, hi + lo
+constexpr int EH_BYTES = 2 * tc::TILE_BYTES;          // batched: one 64-column half of it
+constexpr int NWARP_E = NWARP + 1;                    // batched: + the X_k block warp
+constexpr int NTHR_E = NWARP_E * 32;
 constexpr int SMEM_BYTES_E = 2 * tc::STAGE_BYTES + E_BYTES + EPI_WARPS * SCR_WARP + 1024;
 }  // namespace tcp
 
@@ -334,7 +337,8 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
 template <typename T, int EPI, bool ESM>
 __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
                                          int q, int half, int lane, double alpha, double beta,
-                                         double (&sums)[4], uint8_t* scr, uint8_t* estage) {
+                                         double (&sums)[4], uint8_t* scr, uint8_t* estage,
+                                         int cc_lo = 0, int cc_hi = 64 / tcp::CHUNK) {
   using TR = SplitTraits<T>;
   const int ld = p.ld;
   if (EPI == 0 && ti.ok) {
@@ -350,9 +354,8 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
     // The batched form (ESM) computes a diagonal tile whole instead: every element stands
     // for itself in the sums, every warp has the same four chunks, and the tile leaves by
     // TMA as computed.
-    int first = 0;
-    while (!ESM && first < 64 / tcp::CHUNK && ti.diag &&
-           ti.j0 + half * 64 + first * tcp::CHUNK + 15 < r0)
+    int first = cc_lo;
+    while (!ESM && first < cc_hi && ti.diag && ti.j0 + half * 64 + first * tcp::CHUNK + 15 < r0)
       ++first;
     // the rows of X_k for the next chunk are fetched while this one is processed
     uint4 pf[4];
@@ -364,18 +367,19 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       pf[2] = sl[0];
       pf[3] = sl[1];
     };
-    if (!ESM && first < 64 / tcp::CHUNK) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
+    if (!ESM && first < cc_hi) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
     const int rl = q * 32 + lane;   // row inside the tile
 #pragma unroll 1
-    for (int cc = first; cc < 64 / tcp::CHUNK; ++cc) {
+    for (int cc = first; cc < cc_hi; ++cc) {
       const int cl = half * 64 + cc * tcp::CHUNK;
       uint32_t hh[16], xx[16];
       tmem_ld16(tacc + cl, hh);
       tmem_ld16(tacc + tc::BN + cl, xx);
       const int c0 = ti.j0 + cl;
       alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
-      // 16-byte chunk k of row rl of a staged box sits at chunk k ^ (rl & 7) (128-byte swizzle)
-      uint8_t* eb = ESM ? estage + half * 2 * tc::TILE_BYTES + rl * 128 : nullptr;
+      // 16-byte chunk k of row rl of a staged box sits at chunk k ^ (rl & 7) (128-byte
+      // swizzle); estage is this half's stage: the hi box, then the lo box
+      uint8_t* eb = ESM ? estage + rl * 128 : nullptr;
       const int k0 = ((2 * cc) ^ (rl & 7)) * 16, k1 = ((2 * cc + 1) ^ (rl & 7)) * 16;
       {
         uint4* dh = reinterpret_cast<uint4*>(ehi);
@@ -392,7 +396,7 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
           dl[1] = pf[3];
         }
       }
-      if (!ESM && cc + 1 < 64 / tcp::CHUNK) fetch_e(c0 + tcp::CHUNK);
+      if (!ESM && cc + 1 < cc_hi) fetch_e(c0 + tcp::CHUNK);
       tmem_wait_ld();
       // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
       // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
@@ -650,7 +654,7 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
 // whole (both triangles, as the MMA gives them); only off-diagonal mirrors use ordinary
 // stores.
 template <typename T, int EPI, bool ESM>
-__global__ void __launch_bounds__(tcp::NTHR, 1)
+__global__ void __launch_bounds__(ESM ? tcp::NTHR_E : tcp::NTHR, 1)
     k_tc_persist(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                  const __grid_constant__ CUtensorMap tm_bhi,
                  const __grid_constant__ CUtensorMap tm_blo,
@@ -666,8 +670,8 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
   __shared__ __align__(8) uint64_t bar_tfull[2];
   __shared__ __align__(8) uint64_t bar_tempty[2];
   __shared__ __align__(8) uint64_t bar_final;
-  __shared__ __align__(8) uint64_t bar_efull;   // ESM: X_k block landed
-  __shared__ __align__(8) uint64_t bar_odone;   // ESM: every warp wrote its part of X_{k+1}
+  __shared__ __align__(8) uint64_t bar_efull[2];   // ESM: X_k half block landed (per stage)
+  __shared__ __align__(8) uint64_t bar_odone[2];   // ESM: every warp wrote its part of it
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
@@ -695,8 +699,10 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       mbar_init(smem_u32(&bar_tempty[a]), tcp::EPI_WARPS);
     }
     mbar_init(smem_u32(&bar_final), 1);
-    mbar_init(smem_u32(&bar_efull), 1);
-    mbar_init(smem_u32(&bar_odone), tcp::EPI_WARPS);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&bar_efull[b]), 1);
+      mbar_init(smem_u32(&bar_odone[b]), tcp::EPI_WARPS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), tcp::TMEM_COLS);
@@ -788,83 +794,96 @@ __global__ void __launch_bounds__(tcp::NTHR, 1)
       if (!ok) s_abort = 1;
     }
     __syncwarp();
+  } else if (ESM && warp == tcp::NWARP) {
+    // ---------------- X_k half blocks (batched form, one thread) ----------------
+    // Phase v = 2u + h is the 64-column half h of this CTA's u-th valid tile; it uses
+    // half stage h = v & 1, whose barriers then complete their (v >> 1)-th phase.  While
+    // the epilogue warps work on phase v, the load of phase v + 1 is in flight or done;
+    // a stage is refilled with phase v + 2 once the stores of phase v have read it.
+    if (lane == 0) {
+      int tt[2] = {-1, -1};       // tile whose half each stage holds
+      int pend[2] = {-1, -1};     // phase parity of a load not yet consumed
+      auto next_ok = [&](int t) {
+        while (t < ntiles && !persist_tile(p, t).ok) t += gridDim.x;
+        return t;
+      };
+      auto load = [&](int b, int t, uint32_t v) {   // half b of tile t, phase v
+        const TileInfo tj = persist_tile(p, t);
+        const uint32_t eb = smem_u32(&bar_efull[b]);
+        const uint32_t es = sbase + EOFF + b * tcp::EH_BYTES;
+        mbar_expect_tx(eb, tcp::EH_BYTES);
+        tma_load_2d(es, &tm_hi, eb, tj.j0 + 64 * b, tj.row0 + tj.i0);
+        tma_load_2d(es + tc::TILE_BYTES, &tm_lo, eb, tj.j0 + 64 * b, tj.row0 + tj.i0);
+        tt[b] = t;
+        pend[b] = (int)((v >> 1) & 1);
+      };
+      int t_load = next_ok(blockIdx.x);   // tile of the next loads
+      if (t_load < ntiles) {
+        load(0, t_load, 0);
+        load(1, t_load, 1);
+        t_load = next_ok(t_load + gridDim.x);
+      }
+      for (uint32_t v = 0;; ++v) {
+        const int b = v & 1;
+        if (tt[b] < 0) break;
+        if (!mbar_wait(smem_u32(&bar_odone[b]), (v >> 1) & 1, &s_abort)) break;
+        pend[b] = -1;   // consumed by the epilogue warps, so it had landed
+        const TileInfo tj = persist_tile(p, tt[b]);
+        const uint32_t es = sbase + EOFF + b * tcp::EH_BYTES;
+        tma_store_2d(&tm_ohi, es, tj.j0 + 64 * b, tj.row0 + tj.i0);
+        tma_store_2d(&tm_olo, es + tc::TILE_BYTES, tj.j0 + 64 * b, tj.row0 + tj.i0);
+        bulk_commit();
+        tt[b] = -1;
+        if (t_load < ntiles) {
+          bulk_wait_read0();
+          load(b, t_load, v + 2);
+          if (b == 1) t_load = next_ok(t_load + gridDim.x);
+        }
+      }
+      for (int b = 0; b < 2; ++b)   // loads issued but never consumed (abort)
+        if (pend[b] >= 0)
+          for (uint32_t i = 0; i < kSpinLimit; ++i)
+            if (mbar_try(smem_u32(&bar_efull[b]), pend[b])) break;
+      bulk_wait0();
+    }
+    __syncwarp();
   } else {
     // ---------------- epilogue (8 warps) ----------------
     const int q = warp & 3;             // TMEM lane quarter of this warp
-    const int half = (warp - 2) >> 2;   // 64-column half of the tile
+    const int half = (warp - 2) >> 2;   // 64-column half of the tile (batched: 32-column quarter of each half)
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
     uint32_t tl = 0;
-    uint32_t eph = 0;          // ESM: X_k blocks loaded (and consumed) so far
-    bool e_pending = false;    // ESM, issuing thread: a load not yet waited for
+    uint32_t eu = 0;   // ESM: valid tiles consumed so far
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tl) {
       const TileInfo ti = persist_tile(p, t);
       const int a = tl & 1;
-      if (ESM && ti.ok) {
-        // warp 2 lane 0 loads this tile's X_k block once the previous tile's stores have
-        // read the stage; the load runs while the tile's MMAs finish
-        bool ok2 = true;
-        if (warp == 2) {
-          if (lane == 0) {
-            bulk_wait_read0();
-            if (ok2) {
-              const uint32_t eb = smem_u32(&bar_efull);
-              const uint32_t es = sbase + EOFF;
-              const int y = ti.row0 + ti.i0;
-              mbar_expect_tx(eb, tcp::E_BYTES);
-              tma_load_2d(es + 0 * tc::TILE_BYTES, &tm_hi, eb, ti.j0, y);
-              tma_load_2d(es + 1 * tc::TILE_BYTES, &tm_lo, eb, ti.j0, y);
-              tma_load_2d(es + 2 * tc::TILE_BYTES, &tm_hi, eb, ti.j0 + 64, y);
-              tma_load_2d(es + 3 * tc::TILE_BYTES, &tm_lo, eb, ti.j0 + 64, y);
-              e_pending = true;
-            }
-          }
-          ok2 = __shfl_sync(0xffffffffu, ok2 ? 1 : 0, 0) != 0;
-        }
-        if (!ok2) break;
-      }
       if (!mbar_wait_idle(smem_u32(&bar_tfull[a]), (tl >> 1) & 1, &s_abort)) break;
       tc_fence_after();
       bool eok = true;
       if (ESM && ti.ok) {
-        eok = mbar_wait(smem_u32(&bar_efull), eph & 1, &s_abort);
-        if (eok) e_pending = false;
-      }
-      if (eok)
+        // two phases, one per 64-column half; this warp takes 32 columns of each
+        for (int h = 0; h < 2 && eok; ++h) {
+          const uint32_t v = 2 * eu + h;
+          const int b = v & 1;
+          eok = mbar_wait(smem_u32(&bar_efull[b]), (v >> 1) & 1, &s_abort);
+          if (!eok) break;
+          epi_tile<T, EPI, ESM>(p, ti, tmem + lane_base + a * 256, q, h, lane, alpha, beta, sums,
+                                smem + SOFF + (warp - 2) * tcp::SCR_WARP,
+                                smem + EOFF + b * tcp::EH_BYTES, 2 * half, 2 * half + 2);
+          fence_proxy_async_smem();   // this thread's stage writes, visible to the TMA store
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_u32(&bar_odone[b]));
+        }
+        ++eu;
+      } else {
         epi_tile<T, EPI, ESM>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
-                              smem + SOFF + (warp - 2) * tcp::SCR_WARP, smem + EOFF);
+                              smem + SOFF + (warp - 2) * tcp::SCR_WARP, nullptr);
+      }
       tc_fence_before();  // our TMEM reads are ordered before the release below
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&bar_tempty[a]));
-      if (ESM && ti.ok && eok) {
-        fence_proxy_async_smem();   // this thread's stage writes, visible to the TMA store
-        __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&bar_odone));
-        bool ok3 = true;
-        if (warp == 2 && lane == 0) {
-          ok3 = mbar_wait(smem_u32(&bar_odone), eph & 1, &s_abort);
-          if (ok3) {
-            const uint32_t es = sbase + EOFF;
-            const int y = ti.row0 + ti.i0;
-            tma_store_2d(&tm_ohi, es + 0 * tc::TILE_BYTES, ti.j0, y);
-            tma_store_2d(&tm_olo, es + 1 * tc::TILE_BYTES, ti.j0, y);
-            tma_store_2d(&tm_ohi, es + 2 * tc::TILE_BYTES, ti.j0 + 64, y);
-            tma_store_2d(&tm_olo, es + 3 * tc::TILE_BYTES, ti.j0 + 64, y);
-            bulk_commit();
-          }
-        }
-        ++eph;
-        if (!ok3) break;
-      } else if (ESM && ti.ok) {
-        ++eph;
-      }
       if (!eok) break;
     }
-    // a load that was issued but never waited for (abort) must land before the exit,
-    // and every store of the stage must have completed
-    if (ESM && e_pending)
-      for (uint32_t i = 0; i < kSpinLimit; ++i)
-        if (mbar_try(smem_u32(&bar_efull), eph & 1)) break;
-    if (ESM && warp == 2 && lane == 0) bulk_wait0();
   }
   tc_fence_before();
   __syncthreads();
@@ -1239,7 +1258,8 @@ static cudaError_t launch_persist(const StepArgs& a, long long rows, int ntiles,
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   const int grid = std::min(ntiles, num_sms());
-  kern<<<grid, tcp::NTHR, smem, st>>>(m[0], m[1], m[2], m[3], mo[0], mo[1], a, ntiles);
+  kern<<<grid, ESM ? tcp::NTHR_E : tcp::NTHR, smem, st>>>(m[0], m[1], m[2], m[3], mo[0], mo[1], a,
+                                                          ntiles);
   note_launch();
   return cudaGetLastError();
 }
