@@ -91,6 +91,80 @@ __global__ void k_norm_parts(double* __restrict__ xs, const int* __restrict__ ro
   }
 }
 
+// Split precisions: extraction, normalisation and the hi/lo split in one pass, without
+// the FP64 packed block.  Grid (part, row group); each warp builds one row of X0 at a
+// time in shared memory (zero, scatter the row's CSR entries found in the part's node
+// list, add emax/(emax - emin) on the diagonal) and writes its hi/lo halves over the
+// part's np columns (rows n..np-1 are zero padding).  The values are those of
+// k_extract_csr followed by k_norm_parts, bit for bit.
+template <typename T>
+__global__ void __launch_bounds__(256) k_extract_split(
+    const long long* __restrict__ rp, const int* __restrict__ col, const double* __restrict__ val,
+    const PartDesc* __restrict__ parts, const int* __restrict__ halo, const int* __restrict__ skey,
+    const int* __restrict__ sval, int ld, double emin, double emax, T* __restrict__ hi,
+    T* __restrict__ lo) {
+  __shared__ double rowbuf[8][512];
+  const PartDesc P = parts[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double mm = emax - emin;
+  const double alpha = -1.0 / mm, beta = emax / mm;
+  const int* hl = halo + P.hoff;
+  const int* sk = skey + P.hoff;
+  const int* sv = sval + P.hoff;
+  double* buf = rowbuf[warp];
+  for (int r = blockIdx.y * 8 + warp; r < P.np; r += gridDim.y * 8) {
+    for (int c = lane; c < P.np; c += 32) buf[c] = 0.0;
+    __syncwarp();
+    if (r < P.n) {
+      const int v = hl[r];
+      for (long long e = rp[v] + lane; e < rp[v + 1]; e += 32) {
+        const int u = col[e];
+        int a = 0, b = P.n - 1;
+        while (a <= b) {
+          const int mid = (a + b) >> 1;
+          const int key = sk[mid];
+          if (key == u) {
+            buf[sv[mid]] = val[e];
+            break;
+          }
+          if (key < u) a = mid + 1;
+          else b = mid - 1;
+        }
+      }
+    }
+    __syncwarp();
+    T* oh = hi + ((size_t)P.row0 + r) * ld;
+    T* ol = lo + ((size_t)P.row0 + r) * ld;
+    for (int c = lane; c < P.np; c += 32) {
+      double x = 0.0;
+      if (r < P.n && c < P.n) {
+        x = alpha * buf[c];
+        if (r == c) x += beta;
+      }
+      const T a = SplitOps<T>::from_d(x);
+      oh[c] = a;
+      ol[c] = SplitOps<T>::from_d((x - SplitOps<T>::to_d(a)) * SplitOps<T>::kScale);
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_extract_split(const long long* rp, const int* col, const double* val,
+                                 const PartDesc* parts, int nparts, const int* halo,
+                                 const int* skey, const int* sval, int ld, double emin,
+                                 double emax, int prec, void* hi, void* lo, cudaStream_t st) {
+  const dim3 grid(nparts, 16);
+  if (prec == SP2B_PREC_MIXED_BF16)
+    k_extract_split<__nv_bfloat16><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld,
+                                                          emin, emax, (__nv_bfloat16*)hi,
+                                                          (__nv_bfloat16*)lo);
+  else
+    k_extract_split<__half><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld, emin,
+                                                  emax, (__half*)hi, (__half*)lo);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // rho (core rows) = 2 X: packed per-part output and, optionally, a dense n x n
 // column-major matrix (bml_submatrix2matrix, src/prg_subgraphloop_mod.F90:111-113).
 template <typename T>

@@ -232,7 +232,9 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
 
   // ---- device buffers ----
   const size_t packed = (size_t)rows * ld;
-  SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
+  // split precisions with parts up to 512 go straight from CSR to hi/lo (no FP64 block)
+  const bool fused = split && ld <= 512;
+  if (!fused) SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
   if (split) {
     for (int i = 0; i < 2; ++i) {
       SP2B_CUDA_TRY(grow_buf(b.hi[i], b.hi_cap[i], packed));
@@ -347,7 +349,8 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     SP2B_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
     auto body = [&]() -> cudaError_t {
       cudaError_t e;
-      if ((e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), cap)) != cudaSuccess) return e;
+      if (!fused && (e = cudaMemsetAsync(b.xs, 0, packed * sizeof(double), cap)) != cudaSuccess)
+        return e;
       if ((e = cudaMemsetAsync(c->counter, 0, 4 * sizeof(unsigned), cap)) != cudaSuccess) return e;
       if ((e = cudaMemsetAsync(c->err, 0, sizeof(int), cap)) != cudaSuccess) return e;
       if ((e = cudaMemsetAsync(c->sout, 0, sizeof(SolveOut), cap)) != cudaSuccess) return e;
@@ -357,13 +360,20 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       if (dense_d && j.clear_dense &&
           (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
         return e;
-      if ((e = launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval, ld,
-                                  b.xs, cap)) != cudaSuccess)
-        return e;
-      if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval, prec,
-                                 split ? (void*)b.hi[0] : nullptr, split ? (void*)b.lo[0] : nullptr,
-                                 cap)) != cudaSuccess)
-        return e;
+      if (fused) {
+        if ((e = launch_extract_split(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
+                                      ld, j.mineval, j.maxeval, prec, b.hi[0], b.lo[0], cap)) !=
+            cudaSuccess)
+          return e;
+      } else {
+        if ((e = launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
+                                    ld, b.xs, cap)) != cudaSuccess)
+          return e;
+        if ((e = launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval, prec,
+                                   split ? (void*)b.hi[0] : nullptr,
+                                   split ? (void*)b.lo[0] : nullptr, cap)) != cudaSuccess)
+          return e;
+      }
       for (int k = 0; k < maxiter; ++k) {
         a.k = k;
         const int bin = k & 1, bout = (k + 1) & 1;
