@@ -91,18 +91,19 @@ __global__ void k_norm_parts(double* __restrict__ xs, const int* __restrict__ ro
   }
 }
 
-// Split precisions: extraction, normalisation and the hi/lo split in one pass, without
-// the FP64 packed block.  Grid (part, row group); each warp builds one row of X0 at a
+// Extraction and normalisation in one pass (parts up to 512): straight into the hi/lo
+// split (split precisions, no FP64 packed block) or into the FP64 packed block, without
+// clearing it first.  Grid (part, row group); each warp builds one row of X0 at a
 // time in shared memory (zero, scatter the row's CSR entries found in the part's node
 // list, add emax/(emax - emin) on the diagonal) and writes its hi/lo halves over the
-// part's np columns (rows n..np-1 are zero padding).  The values are those of
-// k_extract_csr followed by k_norm_parts, bit for bit.
-template <typename T>
+// part's np columns (rows n..np-1 are zero padding; columns past np are never read).
+// The values are those of k_extract_csr followed by k_norm_parts, bit for bit.
+template <typename T, bool F64>
 __global__ void __launch_bounds__(256) k_extract_split(
     const long long* __restrict__ rp, const int* __restrict__ col, const double* __restrict__ val,
     const PartDesc* __restrict__ parts, const int* __restrict__ halo, const int* __restrict__ skey,
     const int* __restrict__ sval, int ld, double emin, double emax, T* __restrict__ hi,
-    T* __restrict__ lo) {
+    T* __restrict__ lo, double* __restrict__ xs) {
   __shared__ double rowbuf[8][512];
   const PartDesc P = parts[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -133,17 +134,20 @@ __global__ void __launch_bounds__(256) k_extract_split(
       }
     }
     __syncwarp();
-    T* oh = hi + ((size_t)P.row0 + r) * ld;
-    T* ol = lo + ((size_t)P.row0 + r) * ld;
+    const size_t ro = ((size_t)P.row0 + r) * ld;
     for (int c = lane; c < P.np; c += 32) {
       double x = 0.0;
       if (r < P.n && c < P.n) {
         x = alpha * buf[c];
         if (r == c) x += beta;
       }
-      const T a = SplitOps<T>::from_d(x);
-      oh[c] = a;
-      ol[c] = SplitOps<T>::from_d((x - SplitOps<T>::to_d(a)) * SplitOps<T>::kScale);
+      if (F64) {
+        xs[ro + c] = x;
+      } else {
+        const T a = SplitOps<T>::from_d(x);
+        hi[ro + c] = a;
+        lo[ro + c] = SplitOps<T>::from_d((x - SplitOps<T>::to_d(a)) * SplitOps<T>::kScale);
+      }
     }
     __syncwarp();
   }
@@ -152,15 +156,20 @@ __global__ void __launch_bounds__(256) k_extract_split(
 cudaError_t launch_extract_split(const long long* rp, const int* col, const double* val,
                                  const PartDesc* parts, int nparts, const int* halo,
                                  const int* skey, const int* sval, int ld, double emin,
-                                 double emax, int prec, void* hi, void* lo, cudaStream_t st) {
+                                 double emax, int prec, void* hi, void* lo, double* xs,
+                                 cudaStream_t st) {
   const dim3 grid(nparts, 16);
-  if (prec == SP2B_PREC_MIXED_BF16)
-    k_extract_split<__nv_bfloat16><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld,
-                                                          emin, emax, (__nv_bfloat16*)hi,
-                                                          (__nv_bfloat16*)lo);
+  if (prec == SP2B_PREC_FP64)
+    k_extract_split<__half, true><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld,
+                                                        emin, emax, nullptr, nullptr, xs);
+  else if (prec == SP2B_PREC_MIXED_BF16)
+    k_extract_split<__nv_bfloat16, false><<<grid, 256, 0, st>>>(
+        rp, col, val, parts, halo, skey, sval, ld, emin, emax, (__nv_bfloat16*)hi,
+        (__nv_bfloat16*)lo, nullptr);
   else
-    k_extract_split<__half><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld, emin,
-                                                  emax, (__half*)hi, (__half*)lo);
+    k_extract_split<__half, false><<<grid, 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld,
+                                                         emin, emax, (__half*)hi, (__half*)lo,
+                                                         nullptr);
   note_launch();
   return cudaGetLastError();
 }

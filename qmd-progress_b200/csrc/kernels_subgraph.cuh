@@ -26,12 +26,13 @@ cudaError_t launch_scatter_parts(const double* x64, const void* hi, const void* 
                                  const PartDesc* parts, int nparts, const int* halo, int ld,
                                  double* core_out, double* dense, long long n, cudaStream_t st);
 
-// Split precisions: CSR extraction, normalisation with the global bounds and the hi/lo
-// split straight into the packed 16-bit buffers (np <= 512 per part).
+// CSR extraction and normalisation with the global bounds in one pass (np <= 512 per
+// part): split precisions into the packed hi/lo buffers, FP64 into xs.
 cudaError_t launch_extract_split(const long long* rp, const int* col, const double* val,
                                  const PartDesc* parts, int nparts, const int* halo,
                                  const int* skey, const int* sval, int ld, double emin,
-                                 double emax, int prec, void* hi, void* lo, cudaStream_t st);
+                                 double emax, int prec, void* hi, void* lo, double* xs,
+                                 cudaStream_t st);
 
 // Sum over each part's core rows of (X - X^2)_ii from the split iterate (hi, lo), as
 // kPartIdemGroups partial sums per part (out[part * kPartIdemGroups + g]).

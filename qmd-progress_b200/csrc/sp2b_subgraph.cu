@@ -232,9 +232,9 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
 
   // ---- device buffers ----
   const size_t packed = (size_t)rows * ld;
-  // split precisions with parts up to 512 go straight from CSR to hi/lo (no FP64 block)
-  const bool fused = split && ld <= 512;
-  if (!fused) SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
+  // parts up to 512: CSR straight to X0 (split: hi/lo, no FP64 block; FP64: no clearing)
+  const bool fused = ld <= 512;
+  if (!split || !fused) SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
   if (split) {
     for (int i = 0; i < 2; ++i) {
       SP2B_CUDA_TRY(grow_buf(b.hi[i], b.hi_cap[i], packed));
@@ -256,15 +256,21 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
 
   // ---- a few FP64 parts: every step in one cooperative launch ----
   if (j.multistep && !split && bt == 32 && maxiter > 0) {
-    SP2B_CUDA_TRY(cudaMemsetAsync(b.xs, 0, packed * sizeof(double), st));
     SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
     SP2B_CUDA_TRY(cudaMemsetAsync(b.ms_bar, 0, nparts * sizeof(unsigned), st));
     if (dense_d && j.clear_dense)
       SP2B_CUDA_TRY(cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), st));
-    SP2B_CUDA_TRY(launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
-                                     ld, b.xs, st));
-    SP2B_CUDA_TRY(launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval,
-                                    prec, nullptr, nullptr, st));
+    if (fused) {
+      SP2B_CUDA_TRY(launch_extract_split(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey,
+                                         b.sval, ld, j.mineval, j.maxeval, prec, nullptr, nullptr,
+                                         b.xs, st));
+    } else {
+      SP2B_CUDA_TRY(cudaMemsetAsync(b.xs, 0, packed * sizeof(double), st));
+      SP2B_CUDA_TRY(launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey,
+                                       b.sval, ld, b.xs, st));
+      SP2B_CUDA_TRY(launch_norm_parts(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval,
+                                      prec, nullptr, nullptr, st));
+    }
     MultiStepArgs ma;
     ma.x[0] = b.xs;
     ma.x[1] = b.x2;
@@ -362,7 +368,8 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
         return e;
       if (fused) {
         if ((e = launch_extract_split(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
-                                      ld, j.mineval, j.maxeval, prec, b.hi[0], b.lo[0], cap)) !=
+                                      ld, j.mineval, j.maxeval, prec, split ? b.hi[0] : nullptr,
+                                      split ? b.lo[0] : nullptr, split ? nullptr : b.xs, cap)) !=
             cudaSuccess)
           return e;
       } else {
