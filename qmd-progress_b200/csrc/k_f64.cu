@@ -445,10 +445,11 @@ __global__ void __launch_bounds__(WM* WN * 32, 1) k_sym_gemm_f64(const StepArgs 
   publish_and_finalize(p, s, red, &s_flag);
 }
 
-// Tiles of the one-launch form: 32 x 32, 8 warps of 16 x 8, k blocks of 32 in a 4-deep
-// pipeline (the k order of every sum is that of F64Cfg<32, 2, 4>: 4 at a time, ascending).
+// Tiles of the one-launch form: 32 x 32, 8 warps of 16 x 8, k blocks of 64 in a 3-deep
+// pipeline (the k order of every sum is that of F64Cfg<32, 2, 4>: 4 at a time, ascending);
+// 110 KB of stages, two CTAs per SM.
 struct MsCfg {
-  static constexpr int BK = 32, NT = 256, LDS = 36, ST = 4;
+  static constexpr int BK = 64, NT = 256, LDS = 36, ST = 3;
   static constexpr int TM = 16, TN = 8, MI = 2, NI = 1;
   static constexpr size_t SMEM = (size_t)ST * 2 * BK * LDS * sizeof(double);
 };
