@@ -190,6 +190,21 @@ int sp2b_subgraph_halos(int n, const long long* g_row_ptr, const int* g_col,
                         long long* halo_ptr, int* halo_idx, long long halo_cap,
                         long long* halo_needed, int* lsize, int* llsize);
 
+/* Graph of the sub-graph loop on the GPU: the pattern of |H^2| > gthreshold (the H^2
+ * graph the sub-graph benchmark partitions,
+ * benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65, formed there
+ * with a BML sparse product and a threshold).  H is CSR (row_ptr int64 [n+1], col int32,
+ * val FP64); each G_ij = sum_k H_ik H_kj is summed in the order of row i's entries with
+ * separately rounded products and sums.  Output: g_row_ptr (n+1) and g_col (capacity
+ * g_cap), columns ascending in each row, the diagonal kept when above the threshold.
+ * Returns SP2B_BAD_ARG with the needed capacity in *g_needed (g_row_ptr filled) when
+ * g_col is NULL or too small, SP2B_BAD_INPUT when a row of H^2 has more than 2048
+ * candidate columns.  Host or device pointers per opts.device_ptrs. */
+int sp2b_graph_square_threshold(int n, const long long* h_row_ptr, const int* h_col,
+                                const double* h_val, double gthreshold, long long* g_row_ptr,
+                                int* g_col, long long g_cap, long long* g_needed,
+                                const sp2b_opts* opts);
+
 /* ---- graph-partitioned SP2 (replaces prg_subgraphSP2Loop) ------------------------- */
 
 /* prg_subgraphSP2Loop, src/prg_subgraphloop_mod.F90:36-126, flattened (the reference

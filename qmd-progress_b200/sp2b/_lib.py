@@ -84,6 +84,8 @@ _SIGS = {
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_last_subgraph_refined": (_i, [_ip, _vp, _i, _vp, _i]),
+    "sp2b_graph_square_threshold": (_i, [_i, _vp, _vp, _vp, _d, _vp, _vp, C.c_longlong, _vp,
+                                         C.POINTER(Opts)]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,

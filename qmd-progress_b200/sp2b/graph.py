@@ -55,6 +55,31 @@ def thresholded_square_graph(h_csr, n: int, gthreshold: float):
     return G.indptr.astype(np.int64), G.indices.astype(np.int32)
 
 
+def square_graph_gpu(h_csr, n: int, gthreshold: float):
+    """thresholded_square_graph on the GPU (sp2b_graph_square_threshold): the same CSR
+    pattern of |H^2| > gthreshold, columns ascending."""
+    import ctypes as C
+    from . import _lib
+    rp = np.ascontiguousarray(h_csr[0], dtype=np.int64)
+    col = np.ascontiguousarray(h_csr[1], dtype=np.int32)
+    val = np.ascontiguousarray(h_csr[2], dtype=np.float64)
+    L = _lib.lib()
+    grp = np.zeros(n + 1, dtype=np.int64)
+    need = C.c_longlong(0)
+    o = _lib.make_opts()
+    st = L.sp2b_graph_square_threshold(n, rp.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                       float(gthreshold), grp.ctypes.data, None, 0, C.byref(need),
+                                       C.byref(o))
+    if st != _lib.SP2B_BAD_ARG or need.value != int(grp[n]):
+        _lib.check(st, "graph_square_threshold")
+    gcol = np.zeros(max(int(need.value), 1), dtype=np.int32)
+    _lib.check(L.sp2b_graph_square_threshold(n, rp.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                             float(gthreshold), grp.ctypes.data, gcol.ctypes.data,
+                                             len(gcol), C.byref(need), C.byref(o)),
+               "graph_square_threshold")
+    return grp, gcol[:need.value]
+
+
 def thresholded_graph(dense: np.ndarray, gthreshold: float):
     """Pattern of |A| > gthreshold of a dense matrix as CSR (bml_threshold, then the
     nonzero pattern, as tests/src/test_subgraphloop.F90:100 does with the density)."""
