@@ -190,6 +190,29 @@ int sp2b_subgraph_halos(int n, const long long* g_row_ptr, const int* g_col,
                         long long* halo_ptr, int* halo_idx, long long halo_cap,
                         long long* halo_needed, int* lsize, int* llsize);
 
+/* ---- SP2-Fermi (replaces src/prg_sp2_fermi_mod.F90), FP64 ------------------------ */
+
+/* prg_sp2_fermi_init, src/prg_sp2_fermi_mod.F90:43-177.  Gershgorin bounds give
+ * h1 = tscale*min, hN = tscale*max and the first mu; each pass normalises
+ * X0 = ((hN - mu) I - H)/(hN - h1) and runs nsteps SP2 steps, the first pass choosing
+ * sgnlist[i] (1: X <- 2X - X^2, -1: X <- X^2) from the traces, later passes replaying it,
+ * with X1 = dX/dmu carried along; Newton steps on mu until |nocc - Tr X| <= occ_err_limit;
+ * beta = -Tr X1 / Tr X(I - X) (-1000 when that trace is below trace_limit).  x receives X
+ * of the last pass (occupations in [0, 1], not 2X).  Host or device pointers for h and x
+ * per opts.device_ptrs; sgnlist (nsteps) and the scalars are host memory. */
+int sp2b_sp2_fermi_init(const double* h, int n, int nsteps, double nocc, double tscale,
+                        double threshold, double occ_err_limit, double trace_limit, double* x,
+                        double* mu, double* beta, double* h1, double* hN, int* sgnlist,
+                        const sp2b_opts* opts);
+
+/* prg_sp2_fermi, src/prg_sp2_fermi_mod.F90:388-470: passes of X0 = ((hN - mu) I - H)/
+ * (hN - h1) and the nsteps steps of sgnlist, each followed by a Newton step on mu with
+ * DX = -beta X (I - X); osteps passes, or (osteps = 0) until |nocc - Tr X| <= eps.
+ * x = X + lambda DX with the last pass's lambda; mu is updated in place. */
+int sp2b_sp2_fermi(const double* h, int n, int osteps, int nsteps, double nocc, double* mu,
+                   double beta, double h1, double hN, const int* sgnlist, double threshold,
+                   double eps, double trace_limit, double* x, const sp2b_opts* opts);
+
 /* Graph of the sub-graph loop on the GPU: the pattern of |H^2| > gthreshold (the H^2
  * graph the sub-graph benchmark partitions,
  * benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65, formed there

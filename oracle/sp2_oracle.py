@@ -581,3 +581,94 @@ def adjoint_sp2_seq(h, a, pp, mineval, maxeval):
         anti = g @ xk + xk @ g
         g = anti if pp[k] == 1 else 2.0 * g - anti
     return -g / (maxeval - mineval)
+
+
+# --------------------------------------------------------------------------------------
+# SP2-Fermi: the truncated SP2 expansion at finite temperature (src/prg_sp2_fermi_mod.F90)
+# --------------------------------------------------------------------------------------
+def normalize_fermi(h, h1, hN, mu):
+    """``prg_normalize_fermi`` (``src/prg_normalize_mod.F90:59-72``):
+    X0 = ((hN - mu) I - H)/(hN - h1)."""
+    h = np.asarray(h, dtype=np.float64)
+    return ((hN - mu) * np.eye(h.shape[0]) - h) * (1.0 / (hN - h1))
+
+
+def sp2_fermi_init(h, nsteps, nocc, tscale, occ_err_limit, trace_limit, max_outer=200):
+    """``prg_sp2_fermi_init`` (``src/prg_sp2_fermi_mod.F90:43-177``).
+
+    Returns (x, mu, beta, h1, hN, sgnlist).  sgnlist[i] = 1 means X <- 2X - X^2, -1 means
+    X <- X^2; it is chosen on the first pass from the traces (:104-110) and replayed after.
+    X1 = dX/dmu follows the same recursion through {X, X1} (:112-122); Newton steps on mu
+    (:140-151) until |nocc - Tr X| <= occ_err_limit; beta = -Tr X1 / Tr X(I - X) (:158-168).
+    """
+    h = np.asarray(h, dtype=np.float64)
+    n = h.shape[0]
+    gmin, gmax = gershgorin(h)                                     # :68
+    mu = 0.5 * (gmax + gmin)                                       # :69
+    h1, hN = tscale * gmin, tscale * gmax                          # :70-71
+    occ_err = 1.0
+    first = True
+    sgn = [0] * nsteps
+    outer = 0
+    x = x1 = None
+    while occ_err > occ_err_limit:                                 # :89
+        outer += 1
+        if outer > max_outer:
+            raise SP2NotConverging("sp2_fermi_init: occupation did not converge")
+        x = normalize_fermi(h, h1, hN, mu)                         # :91-92
+        x1 = -np.eye(n) / (hN - h1)                                # :94-96
+        for i in range(nsteps):                                    # :98
+            x2 = x @ x
+            tr0, tr2 = float(np.trace(x)), float(np.trace(x2))
+            if first:                                              # :105-111
+                sgn[i] = -1 if abs(tr2 - nocc) < abs(2.0 * tr0 - tr2 - nocc) else 1
+            tmp = x @ x1 + x1 @ x                                  # :113-114
+            x1 = 2.0 * x1 - tmp if sgn[i] == 1 else tmp            # :116-120
+            x = 2.0 * x - x2 if sgn[i] == 1 else x2                # :122-126
+        first = False
+        tr0, tr1 = float(np.trace(x)), float(np.trace(x1))         # :131-132
+        occ_err = abs(nocc - tr0)                                  # :133
+        lam = (nocc - tr0) / tr1 if abs(tr1) > trace_limit else 0.0   # :146-150
+        mu += lam                                                  # :151
+    trx = float(np.trace(x @ (np.eye(n) - x)))                     # :157-159
+    tr1 = float(np.trace(x1))
+    beta = -tr1 / trx if abs(trx) > trace_limit else -1000.0       # :161-166
+    return x, mu, beta, h1, hN, sgn
+
+
+def sp2_fermi(h, osteps, nsteps, nocc, mu, beta, h1, hN, sgnlist, eps, trace_limit,
+              max_outer=200):
+    """``prg_sp2_fermi`` (``src/prg_sp2_fermi_mod.F90:388-470``): replay sgnlist from
+    X0 = normalize_fermi(H, h1, hN, mu); Newton steps on mu with the derivative
+    DX = -beta X (I - X) (:438-455), osteps times or until |nocc - Tr X| <= eps; returns
+    (X + lambda DX, mu) with the last step's lambda (:460)."""
+    h = np.asarray(h, dtype=np.float64)
+    n = h.shape[0]
+    occ_err = 1.0 + eps                                            # :416
+    it = 0
+    lam = 0.0
+    x = dx = None
+    while (osteps == 0 and occ_err > eps) or (osteps > 0 and it < osteps):   # :418-419
+        it += 1
+        if it > max_outer:
+            raise SP2NotConverging("sp2_fermi: occupation did not converge")
+        x = normalize_fermi(h, h1, hN, mu)                         # :423-424
+        for i in range(nsteps):                                    # :426-437
+            x2 = x @ x
+            x = 2.0 * x - x2 if sgnlist[i] == 1 else x2
+        tr0 = float(np.trace(x))                                   # :439
+        occ_err = abs(nocc - tr0)                                  # :440
+        dx = -beta * (x @ (np.eye(n) - x))                         # :443-445
+        trdx = float(np.trace(dx))
+        lam = (nocc - tr0) / trdx if abs(trdx) > trace_limit else 0.0   # :448-453
+        mu += lam                                                  # :455
+    return x + lam * dx, mu
+
+
+def build_density_t_fermi(h, kbt, mu):
+    """2 C diag(f) C^T with the Fermi-Dirac occupations f = 1/(1 + exp((e - mu)/kbT)): the
+    reference's finite-temperature check of SP2-Fermi (``tests/src/main.F90:789-795``,
+    ``prg_build_density_T_fermi``)."""
+    evals, evecs = np.linalg.eigh(np.asarray(h, dtype=np.float64))
+    f = 1.0 / (1.0 + np.exp(np.clip((evals - mu) / kbt, -700, 700)))
+    return 2.0 * (evecs * f) @ evecs.T

@@ -105,7 +105,8 @@ __global__ void k_resp_init(const double* __restrict__ h1, int n, int ld, int np
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int c = c0 + e;
-      v[e] = (r < n && c < n) ? alpha * h1[(size_t)r * ld + c] : 0.0;
+      // h1 == nullptr: the identity (dX0/dmu of the SP2-Fermi normalisation)
+      v[e] = (r < n && c < n) ? alpha * (h1 ? h1[(size_t)r * ld + c] : (r == c ? 1.0 : 0.0)) : 0.0;
     }
     double2* dst = reinterpret_cast<double2*>(d + (size_t)r * np + c0);
 #pragma unroll

@@ -34,6 +34,8 @@ enum Algo : int {
   ALGO_MIXED = 6,        // mixed-precision alg2 with a precision-aware stop rule
   ALGO_RESP = 7,         // prg_compute_response_SP2 src/prg_response_mod.F90:653-782 (alg2
                          // rules, no iteration decrement on the break branch, :751)
+  ALGO_FERMI_GEN = 8,    // prg_sp2_fermi_init's first pass src/prg_sp2_fermi_mod.F90:98-127:
+                         // branch from the traces, exactly icount steps
 };
 
 enum Conv : int { CONV_NONE = 0, CONV_REL = 1, CONV_ABS = 2 };
@@ -188,6 +190,15 @@ __host__ __device__ inline SP2Decision sp2_decide(const SP2Ctl& c, const SP2Rec&
       nx.iter = it + 1;
       nx.trx = trx;
       nx.done = stop;
+      break;
+    }
+    case ALGO_FERMI_GEN: {
+      // X^2 when |Tr X^2 - nocc| < |2 Tr X - Tr X^2 - nocc| (:105-111), else 2X - X^2
+      const double trx = r.trx_data, trx2 = r.fro2;
+      d.branch = (dabs(trx2 - occ) < dabs(2.0 * trx - trx2 - occ)) ? BR_X2 : BR_2X_MINUS_X2;
+      nx.iter = k + 1;
+      nx.done = (k + 1 >= c.icount) ? 1 : 0;
+      nx.trx = (d.branch == BR_2X_MINUS_X2) ? 2.0 * trx - trx2 : trx2;
       break;
     }
     default: {  // ALGO_SEQ

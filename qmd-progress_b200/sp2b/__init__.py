@@ -25,7 +25,7 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "PREC_EXACT_INT8",
            "MCW_INT8",
            "MCW_FP64", "last_refinement_info", "compute_response_sp2", "subgraph_sp2_loop",
-           "last_subgraph_refined"]
+           "last_subgraph_refined", "sp2_fermi_init", "sp2_fermi"]
 
 
 @dataclass
@@ -73,6 +73,39 @@ def compute_response_sp2(h0, h1, bndfil, minsp2iter=0, maxsp2iter=100, sp2conv="
           "compute_response_sp2")
     k = ic.value
     return rho, rsp, pp[:k].tolist(), k
+
+
+def sp2_fermi_init(h, nsteps, nocc, tscale=1.0, occ_err_limit=1e-9, trace_limit=1e-12,
+                   threshold=0.0):
+    """prg_sp2_fermi_init (src/prg_sp2_fermi_mod.F90:43-177), FP64 on the GPU: returns
+    (x, mu, beta, h1, hN, sgnlist); x holds occupations in [0, 1] (X, not 2X)."""
+    h = _f64(h)
+    n = h.shape[0]
+    x = np.empty_like(h)
+    sgn = np.zeros(max(nsteps, 1), dtype=np.int32)
+    mu, beta, h1, hN = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_sp2_fermi_init(_ptr(h), n, nsteps, nocc, tscale, threshold, occ_err_limit,
+                                    trace_limit, _ptr(x), C.byref(mu), C.byref(beta),
+                                    C.byref(h1), C.byref(hN),
+                                    sgn.ctypes.data_as(C.POINTER(C.c_int)), C.byref(o)),
+          "sp2_fermi_init")
+    return x, mu.value, beta.value, h1.value, hN.value, sgn[:nsteps].tolist()
+
+
+def sp2_fermi(h, osteps, nsteps, nocc, mu, beta, h1, hN, sgnlist, eps=1e-4, trace_limit=1e-12,
+              threshold=0.0):
+    """prg_sp2_fermi (src/prg_sp2_fermi_mod.F90:388-470), FP64 on the GPU: returns (x, mu)."""
+    h = _f64(h)
+    n = h.shape[0]
+    x = np.empty_like(h)
+    sgn = np.ascontiguousarray(sgnlist, dtype=np.int32)
+    m = C.c_double(mu)
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_sp2_fermi(_ptr(h), n, osteps, nsteps, nocc, C.byref(m), beta, h1, hN,
+                               sgn.ctypes.data_as(C.POINTER(C.c_int)), threshold, eps,
+                               trace_limit, _ptr(x), C.byref(o)), "sp2_fermi")
+    return x, m.value
 
 
 def last_refinement_info():

@@ -25,6 +25,7 @@ SOURCES = [
     "k_graph.cu",
     "sp2b_dense.cu",
     "sp2b_subgraph.cu",
+    "sp2b_fermi.cu",
     "sp2b_noalloc.cu",
     "sp2b_adjoint.cu",
     "sp2b_host.cpp",

@@ -86,6 +86,10 @@ _SIGS = {
     "sp2b_last_subgraph_refined": (_i, [_ip, _vp, _i, _vp, _i]),
     "sp2b_graph_square_threshold": (_i, [_i, _vp, _vp, _vp, _d, _vp, _vp, C.c_longlong, _vp,
                                          C.POINTER(Opts)]),
+    "sp2b_sp2_fermi_init": (_i, [_vp, _i, _i, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp, _dp, _ip,
+                                 C.POINTER(Opts)]),
+    "sp2b_sp2_fermi": (_i, [_vp, _i, _i, _i, _d, _dp, _d, _d, _d, _ip, _d, _d, _d, _vp,
+                            C.POINTER(Opts)]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
