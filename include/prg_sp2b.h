@@ -77,6 +77,19 @@ void prg_sp2_submatrix(bml_matrix_t* ham_bml, bml_matrix_t* rho_bml, double thre
 void prg_sp2_submatrix_inplace(bml_matrix_t* rho_bml, double threshold, int* pp, int* icount,
                                double* vv, double mineval, double maxeval, int core_size);
 
+/* SP2-Fermi (src/prg_progress_mod.h:433-480; FP64 on the GPU, sp2b_sp2_fermi_init /
+ * sp2b_sp2_fermi).  The prototypes follow the reference header; its Fortran binding of
+ * prg_sp2_fermi_init (src/prg_c_interface.F90:904-927) takes a trailing `verbose` that
+ * the header does not declare and that this export does not read. */
+void prg_sp2_fermi_init(bml_matrix_t* h_bml, int nsteps, double nocc, double tscale,
+                        double threshold, double occErrLimit, double traceLimit,
+                        bml_matrix_t* x_bml, double* mu, double* beta, double* h1, double* hN,
+                        int* sgnlist);
+
+void prg_sp2_fermi(bml_matrix_t* h_bml, int osteps, int nsteps, double nocc, double* mu,
+                   double* beta, double* h1, double* hN, int* sgnlist, double threshold,
+                   double eps, double traceLimit, bml_matrix_t* x_bml);
+
 /* prg_normalize (src/prg_normalize_mod.F90:32-46) and prg_check_idempotency
  * (src/prg_densitymatrix_mod.F90:862-880), the two helpers the SP2 tests call. */
 void prg_normalize(bml_matrix_t* h_bml);

@@ -179,6 +179,28 @@ void prg_sp2_submatrix_inplace(bml_matrix_t* rho, double threshold, int* pp, int
          "prg_sp2_submatrix_inplace");
 }
 
+void prg_sp2_fermi_init(bml_matrix_t* h, int nsteps, double nocc, double tscale, double threshold,
+                        double occErrLimit, double traceLimit, bml_matrix_t* x, double* mu,
+                        double* beta, double* h1, double* hN, int* sgnlist) {
+  if (!same_n(h, x) || !mu || !beta || !h1 || !hN || !sgnlist)
+    return finish(SP2B_BAD_ARG, "prg_sp2_fermi_init");
+  sp2b_opts o = defaults();
+  finish(sp2b_sp2_fermi_init(h->data, h->n, nsteps, nocc, tscale, threshold, occErrLimit,
+                             traceLimit, x->data, mu, beta, h1, hN, sgnlist, &o),
+         "prg_sp2_fermi_init");
+}
+
+void prg_sp2_fermi(bml_matrix_t* h, int osteps, int nsteps, double nocc, double* mu, double* beta,
+                   double* h1, double* hN, int* sgnlist, double threshold, double eps,
+                   double traceLimit, bml_matrix_t* x) {
+  if (!same_n(h, x) || !mu || !beta || !h1 || !hN || !sgnlist)
+    return finish(SP2B_BAD_ARG, "prg_sp2_fermi");
+  sp2b_opts o = defaults();
+  finish(sp2b_sp2_fermi(h->data, h->n, osteps, nsteps, nocc, mu, *beta, *h1, *hN, sgnlist,
+                        threshold, eps, traceLimit, x->data, &o),
+         "prg_sp2_fermi");
+}
+
 void prg_normalize(bml_matrix_t* h) {
   if (!h || !h->data) return finish(SP2B_BAD_ARG, "prg_normalize");
   sp2b_opts o = defaults();

@@ -116,6 +116,8 @@ _SIGS = {
     "prg_prg_sp2_alg1_seq_inplace": (None, [_vp, _d, _i, _vp, _ip, _vp, _d, _d]),
     "prg_sp2_submatrix": (None, [_vp, _vp, _d, _vp, _ip, _vp, _d, _d, _i]),
     "prg_sp2_submatrix_inplace": (None, [_vp, _d, _vp, _ip, _vp, _d, _d, _i]),
+    "prg_sp2_fermi_init": (None, [_vp, _i, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp, _dp, _ip]),
+    "prg_sp2_fermi": (None, [_vp, _i, _i, _d, _dp, _dp, _dp, _dp, _ip, _d, _d, _d, _vp]),
     "prg_normalize": (None, [_vp]),
     "prg_check_idempotency": (None, [_vp, _d, _dp]),
 }
