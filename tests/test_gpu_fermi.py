@@ -70,3 +70,35 @@ def test_fermi_derivative_is_dtrx_dmu(cuda):
     # take X from the returned x and compare beta's numerator with the finite difference
     t = np.trace(x @ (np.eye(n) - x))
     assert abs(-beta * t - dtr) <= 1e-4 * abs(dtr)
+
+
+def test_progress_named_fermi_exports(cuda):
+    """prg_sp2_fermi_init / prg_sp2_fermi through bml handles (the reference's argument
+    order, prg_sp2_fermi_mod.F90) give the oracle's mu, beta, sequence and X."""
+    import ctypes as C
+    from sp2b import _lib
+    h = np.asfortranarray(_lattice(6))
+    n = h.shape[0]
+    nocc, nsteps = 0.5 * n, 14
+    xr, mur, betar, h1r, hNr, sgnr = O.sp2_fermi_init(h, nsteps, nocc, 1.0, 1e-9, 1e-12)
+    L = _lib.lib()
+    x = np.zeros((n, n), order="F")
+    hb = L.sp2b_bml_wrap_dense(h.ctypes.data_as(C.c_void_p), n)
+    xb = L.sp2b_bml_wrap_dense(x.ctypes.data_as(C.c_void_p), n)
+    mu, beta, h1, hN = C.c_double(0), C.c_double(0), C.c_double(0), C.c_double(0)
+    sgn = np.zeros(nsteps, dtype=np.int32)
+    L.prg_sp2_fermi_init(hb, nsteps, nocc, 1.0, 0.0, 1e-9, 1e-12, xb, C.byref(mu), C.byref(beta),
+                         C.byref(h1), C.byref(hN), sgn.ctypes.data_as(C.POINTER(C.c_int)))
+    assert L.sp2b_prg_last_status() == 0
+    assert list(sgn) == list(sgnr)
+    assert abs(mu.value - mur) <= 1e-9 * max(1.0, abs(mur))
+    assert abs(beta.value - betar) <= 1e-9 * abs(betar)
+    assert np.linalg.norm(x - xr) <= 1e-10 * np.linalg.norm(xr)
+    xf_r, mu2_r = O.sp2_fermi(h, 2, nsteps, nocc, mur, betar, h1r, hNr, sgnr, 1e-4, 1e-12)
+    L.prg_sp2_fermi(hb, 2, nsteps, nocc, C.byref(mu), C.byref(beta), C.byref(h1), C.byref(hN),
+                    sgn.ctypes.data_as(C.POINTER(C.c_int)), 0.0, 1e-4, 1e-12, xb)
+    assert L.sp2b_prg_last_status() == 0
+    assert abs(mu.value - mu2_r) <= 1e-9 * max(1.0, abs(mu2_r))
+    assert np.linalg.norm(x - xf_r) <= 1e-10 * np.linalg.norm(xf_r)
+    for b in (hb, xb):
+        L.sp2b_bml_free(b)
