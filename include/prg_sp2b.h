@@ -90,6 +90,20 @@ void prg_sp2_fermi(bml_matrix_t* h_bml, int osteps, int nsteps, double nocc, dou
                    double* beta, double* h1, double* hN, int* sgnlist, double threshold,
                    double eps, double traceLimit, bml_matrix_t* x_bml);
 
+/* prg_sp2_fermi_init_norecs (src/prg_c_interface.F90:929-952; sp2b_sp2_fermi_init_norecs):
+ * *beta in is the target, *nsteps in the most steps; verbose is not read. */
+void prg_sp2_fermi_init_norecs(bml_matrix_t* h_bml, int* nsteps, double nocc, double tscale,
+                               double threshold, double occErrLimit, double traceLimit,
+                               bml_matrix_t* x_bml, double* mu, double* beta, double* h1,
+                               double* hN, int* sgnlist, int verbose);
+
+/* prg_sp2_entropy_function (src/prg_c_interface.F90:977-990; sp2b_sp2_entropy_function).
+ * The reference header declares sgnlist, GG and ee as scalars; its Fortran binding takes
+ * arrays, sgnlist(nsteps), GG(1001) and ee(1001), and assigns the 10001-point results to
+ * them, which stores their first 1001 points: this export writes those 1001 entries. */
+void prg_sp2_entropy_function(double mu, double h1, double hN, int nsteps, int* sgnlist,
+                              double* GG, double* ee);
+
 /* prg_normalize (src/prg_normalize_mod.F90:32-46) and prg_check_idempotency
  * (src/prg_densitymatrix_mod.F90:862-880), the two helpers the SP2 tests call. */
 void prg_normalize(bml_matrix_t* h_bml);

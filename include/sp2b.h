@@ -213,6 +213,24 @@ int sp2b_sp2_fermi(const double* h, int n, int osteps, int nsteps, double nocc, 
                    double beta, double h1, double hN, const int* sgnlist, double threshold,
                    double eps, double trace_limit, double* x, const sp2b_opts* opts);
 
+/* prg_sp2_fermi_init_norecs, src/prg_sp2_fermi_mod.F90:198-372: as sp2b_sp2_fermi_init,
+ * but *beta enters as the target inverse temperature and *nsteps as the most steps; the
+ * recursion ends at the first step whose probe temperature (the steepest slope of the
+ * sequence applied to the grid 0.999, 0.998, ..., 0, times 4/(max - min), :256-310)
+ * exceeds it, which is returned in *nsteps with sgnlist[0 .. *nsteps - 1]. */
+int sp2b_sp2_fermi_init_norecs(const double* h, int n, int* nsteps, double nocc, double tscale,
+                               double threshold, double occ_err_limit, double trace_limit,
+                               double* x, double* mu, double* beta, double* h1, double* hN,
+                               int* sgnlist, const sp2b_opts* opts);
+
+/* prg_sp2_entropy_function, src/prg_sp2_fermi_mod.F90:482-532: the SP2 entropy function
+ * GG on the mesh ee = 0, 1e-4, ..., 1 (10001 points), the running two-point Gauss-Legendre
+ * integral of the inverse SP2 map (sp2_inverse, :592-611) minus GG(end) ee.  Writes the
+ * first npoints (1..10001) entries of gg and ee; host memory, host arithmetic (a table of
+ * scalars, as in the reference). */
+int sp2b_sp2_entropy_function(double mu, double h1, double hN, int nsteps, const int* sgnlist,
+                              double* gg, double* ee, int npoints);
+
 /* Graph of the sub-graph loop on the GPU: the pattern of |H^2| > gthreshold (the H^2
  * graph the sub-graph benchmark partitions,
  * benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65, formed there

@@ -636,6 +636,105 @@ def sp2_fermi_init(h, nsteps, nocc, tscale, occ_err_limit, trace_limit, max_oute
     return x, mu, beta, h1, hN, sgn
 
 
+def _probe_beta(probe, gmin, gmax):
+    """4 max_j |p_(j+1) - p_j| / 0.001 / (gmax - gmin): ``absmaxderivative``
+    (``src/prg_sp2_fermi_mod.F90:617-630``) of the probe, scaled as at :306."""
+    maxder = -10000.0
+    for d in np.abs(np.diff(probe)) / 0.001:
+        if d > maxder:
+            maxder = d
+    return (4.0 * maxder) / (gmax - gmin)
+
+
+def sp2_fermi_init_norecs(h, nsteps, nocc, tscale, occ_err_limit, trace_limit, beta0,
+                          max_outer=200):
+    """``prg_sp2_fermi_init_norecs`` (``src/prg_sp2_fermi_mod.F90:198-372``): as
+    ``sp2_fermi_init``, but each pass ends the recursion at the first step whose probe
+    temperature passes the guess beta0, which sets nsteps (the probe depends on the sequence
+    alone, so every pass ends at the same step); sgnlist is written up to that step.
+    Returns (x, nsteps, mu, beta, h1, hN, sgnlist)."""
+    h = np.asarray(h, dtype=np.float64)
+    n = h.shape[0]
+    gmin, gmax = gershgorin(h)                                     # :229
+    mu = 0.5 * (gmax + gmin)                                       # :230
+    h1, hN = tscale * gmin, tscale * gmax                          # :231-232
+    occ_err = 1.0
+    first = True
+    sgn = [0] * nsteps
+    outer = 0
+    x = x1 = None
+    while occ_err > occ_err_limit:                                 # :250
+        outer += 1
+        if outer > max_outer:
+            raise SP2NotConverging("sp2_fermi_init_norecs: occupation did not converge")
+        x = normalize_fermi(h, h1, hN, mu)                         # :252-253
+        x1 = -np.eye(n) / (hN - h1)                                # :261-263
+        # the probe p_j = 1 - 0.001 j, a grid of X0 values, follows the sequence (:256-258)
+        probe = 1.0 - np.arange(1, 1001, dtype=np.float64) * 0.001
+        steps = nsteps
+        for i in range(nsteps):                                    # :265
+            x2 = x @ x
+            tr0, tr2 = float(np.trace(x)), float(np.trace(x2))
+            p2 = probe * probe                                     # :266
+            if first:                                              # :273-279
+                sgn[i] = -1 if abs(tr2 - nocc) < abs(2.0 * tr0 - tr2 - nocc) else 1
+            tmp = x @ x1 + x1 @ x                                  # :287-288
+            x1 = 2.0 * x1 - tmp if sgn[i] == 1 else tmp            # :290-295
+            if sgn[i] == 1:                                        # :297-303
+                x = 2.0 * x - x2
+                probe = 2.0 * probe - p2
+            else:
+                x = x2
+                probe = p2
+            if _probe_beta(probe, gmin, gmax) > beta0:             # :305-310
+                steps = i + 1
+                break
+        nsteps = steps
+        first = False
+        tr0, tr1 = float(np.trace(x)), float(np.trace(x1))         # :325-326
+        occ_err = abs(nocc - tr0)                                  # :327
+        lam = (nocc - tr0) / tr1 if abs(tr1) > trace_limit else 0.0   # :329-333
+        mu += lam                                                  # :334
+    trx = float(np.trace(x @ (np.eye(n) - x)))                     # :342-351
+    tr1 = float(np.trace(x1))
+    beta = -tr1 / trx if abs(trx) > trace_limit else -1000.0       # :353-358
+    return x, nsteps, mu, beta, h1, hN, sgn[:nsteps]
+
+
+def sp2_inverse(f, mu, h1, hN, nsteps, sgnlist):
+    """``sp2_inverse`` (``src/prg_sp2_fermi_mod.F90:592-611``): the energy whose SP2 image
+    is the occupation f, through the sequence backwards."""
+    ee = f
+    for i in range(nsteps - 1, -1, -1):
+        sgn = float(sgnlist[i])
+        c = (1.0 + sgn) / 2.0
+        ee = c - sgn * math.sqrt(abs(c - sgn * ee))
+    return hN - mu - ee * (hN - h1)
+
+
+def sp2_entropy_function(mu, h1, hN, nsteps, sgnlist):
+    """``prg_sp2_entropy_function`` (``src/prg_sp2_fermi_mod.F90:482-532``): on the mesh
+    ee = 0, 1e-4, ..., 1 (10001 points), GG = the running two-point Gauss-Legendre integral
+    of sp2_inverse over each mesh interval, minus GG(end) * ee.  Returns (GG, ee)."""
+    dh = 0.0001
+    x1 = 0.5773502691896257
+    x2 = -x1
+    n = 10001
+    ee = np.arange(n, dtype=np.float64) * dh                       # :510-512
+    gg = np.zeros(n)
+    iint = 0.0
+    for i in range(n - 1):                                         # :516-525
+        a, b = ee[i], ee[i + 1]
+        c_1 = 1.0 * (b - a) / 2.0
+        c_2 = 1.0 * (b - a) / 2.0
+        x_1 = ((b - a) * x1 + (b + a)) / 2.0
+        x_2 = ((b - a) * x2 + (b + a)) / 2.0
+        iint = iint + c_1 * sp2_inverse(x_1, mu, h1, hN, nsteps, sgnlist)
+        iint = iint + c_2 * sp2_inverse(x_2, mu, h1, hN, nsteps, sgnlist)
+        gg[i + 1] = iint
+    return gg - gg[n - 1] * ee, ee                                 # :528
+
+
 def sp2_fermi(h, osteps, nsteps, nocc, mu, beta, h1, hN, sgnlist, eps, trace_limit,
               max_outer=200):
     """``prg_sp2_fermi`` (``src/prg_sp2_fermi_mod.F90:388-470``): replay sgnlist from

@@ -116,6 +116,14 @@ int fermi_pass(Ctx* c, const double* hdev, int n, int nsteps, double nocc, doubl
   return SP2B_OK;
 }
 
+// The generated branches as the reference's sgnlist (1: X <- 2X - X^2, -1: X <- X^2)
+int fermi_read_sequence(Ctx* c, int nsteps, int* sgnlist) {
+  std::vector<int> pp(nsteps);
+  SP2B_CUDA_TRY(cudaMemcpy(pp.data(), c->pp_dev, nsteps * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < nsteps; ++i) sgnlist[i] = pp[i] == BR_2X_MINUS_X2 ? 1 : -1;
+  return SP2B_OK;
+}
+
 struct FermiSetup {
   Ctx* c;
   cudaStream_t st;
@@ -173,6 +181,68 @@ int fermi_output(FermiSetup& s, int n, int nsteps, double* x, bool correct, doub
   return SP2B_OK;
 }
 
+// Newton passes on mu with X1 = dX/dmu until |nocc - Tr X| <= occ_err_limit
+// (src/prg_sp2_fermi_mod.F90:89-152): the first pass generates the sequence when gen (into
+// sgnlist), later passes replay it; then beta = -Tr X1 / Tr X (I - X) (:157-166) and X.
+int fermi_init_passes(FermiSetup& s, int n, int nsteps, double nocc, double h1, double hN,
+                      double occ_err_limit, double trace_limit, bool gen, double* mu,
+                      double* beta, int* sgnlist, double* x, const char* who) {
+  FermiPass f{};
+  double occ_err = 1.0;
+  int rc;
+  for (int pass = 0; occ_err > occ_err_limit; ++pass) {
+    if (pass >= 1000) {
+      set_last_error("%s: occupation did not converge in 1000 passes", who);
+      return SP2B_NOT_CONVERGED;
+    }
+    const bool g = gen && pass == 0;
+    if ((rc = fermi_pass(s.c, s.hdev, n, nsteps, nocc, h1, hN, *mu, g, true, s.st, &f)) != SP2B_OK)
+      return rc;
+    if (g && (rc = fermi_read_sequence(s.c, nsteps, sgnlist)) != SP2B_OK) return rc;
+    occ_err = std::fabs(nocc - f.trx);
+    const double lambda = std::fabs(f.trx1) > trace_limit ? (nocc - f.trx) / f.trx1 : 0.0;
+    *mu += lambda;
+  }
+  const double trx = f.trx - f.fro2;
+  *beta = std::fabs(trx) > trace_limit ? -f.trx1 / trx : -1000.0;
+  return fermi_output(s, n, nsteps, x, false, 0.0);
+}
+
+// The step at which prg_sp2_fermi_init_norecs ends the recursion
+// (src/prg_sp2_fermi_mod.F90:256-310): the probe p_j = 1 - 0.001 j (j = 1..1000), a grid of
+// X0 values, follows the sequence; after step i its steepest slope gives the inverse
+// temperature 4 max_j |p_(j+1) - p_j| / 0.001 / (gmax - gmin) (absmaxderivative, :617-630),
+// and the first step where that exceeds beta0 is the last.  The probe depends on the
+// sequence alone, so every pass of the reference ends at the same step.
+int fermi_probe_steps(const int* sgnlist, int nsteps, double gmin, double gmax, double beta0) {
+  std::vector<double> p(1000);
+  for (int j = 0; j < 1000; ++j) p[j] = 1.0 - (double)(j + 1) * 0.001;
+  for (int i = 0; i < nsteps; ++i) {
+    for (int j = 0; j < 1000; ++j) {
+      const double p2 = p[j] * p[j];
+      p[j] = sgnlist[i] == 1 ? 2.0 * p[j] - p2 : p2;
+    }
+    double maxder = -10000.0;
+    for (int j = 0; j < 999; ++j) {
+      const double d = std::fabs(p[j + 1] - p[j]) / 0.001;
+      if (d > maxder) maxder = d;
+    }
+    if ((4.0 * maxder) / (gmax - gmin) > beta0) return i + 1;
+  }
+  return nsteps;
+}
+
+// sp2_inverse (src/prg_sp2_fermi_mod.F90:592-611): the energy whose SP2 image is f
+double fermi_sp2_inverse(double f, double mu, double h1, double hN, int nsteps, const int* sgnlist) {
+  double e = f;
+  for (int i = nsteps - 1; i >= 0; --i) {
+    const double sgn = (double)sgnlist[i];
+    const double c = (1.0 + sgn) / 2.0;
+    e = c - sgn * std::sqrt(std::fabs(c - sgn * e));
+  }
+  return hN - mu - e * (hN - h1);
+}
+
 }  // namespace
 
 }  // namespace sp2b
@@ -202,30 +272,8 @@ extern "C" int sp2b_sp2_fermi_init(const double* h, int n, int nsteps, double no
   FermiSetup s;
   std::unique_lock<std::mutex> lk;
   if ((rc = fermi_setup(h, n, nsteps, true, opts, &s, &lk)) != SP2B_OK) return rc;
-  // Newton passes on mu until the occupation error is below the limit (:89-152)
-  FermiPass f{};
-  double occ_err = 1.0;
-  for (int pass = 0; occ_err > occ_err_limit; ++pass) {
-    if (pass >= 1000) {
-      set_last_error("sp2b_sp2_fermi_init: occupation did not converge in 1000 passes");
-      return SP2B_NOT_CONVERGED;
-    }
-    if ((rc = fermi_pass(s.c, s.hdev, n, nsteps, nocc, *h1, *hN, *mu, pass == 0, true, s.st, &f)) !=
-        SP2B_OK)
-      return rc;
-    if (pass == 0) {
-      std::vector<int> pp(nsteps);
-      SP2B_CUDA_TRY(cudaMemcpy(pp.data(), s.c->pp_dev, nsteps * sizeof(int), cudaMemcpyDeviceToHost));
-      for (int i = 0; i < nsteps; ++i) sgnlist[i] = pp[i] == BR_2X_MINUS_X2 ? 1 : -1;
-    }
-    occ_err = std::fabs(nocc - f.trx);
-    const double lambda = std::fabs(f.trx1) > trace_limit ? (nocc - f.trx) / f.trx1 : 0.0;
-    *mu += lambda;
-  }
-  // beta = -Tr X1 / Tr X (I - X) (:157-166)
-  const double trx = f.trx - f.fro2;
-  *beta = std::fabs(trx) > trace_limit ? -f.trx1 / trx : -1000.0;
-  return fermi_output(s, n, nsteps, x, false, 0.0);
+  return fermi_init_passes(s, n, nsteps, nocc, *h1, *hN, occ_err_limit, trace_limit, true, mu, beta,
+                           sgnlist, x, "sp2b_sp2_fermi_init");
 }
 
 extern "C" int sp2b_sp2_fermi(const double* h, int n, int osteps, int nsteps, double nocc,
@@ -269,4 +317,79 @@ extern "C" int sp2b_sp2_fermi(const double* h, int n, int osteps, int nsteps, do
     *mu += lambda;
   }
   return fermi_output(s, n, nsteps, x, it > 0, lambda * beta);
+}
+
+extern "C" int sp2b_sp2_fermi_init_norecs(const double* h, int n, int* nsteps, double nocc,
+                                          double tscale, double threshold, double occ_err_limit,
+                                          double trace_limit, double* x, double* mu, double* beta,
+                                          double* h1, double* hN, int* sgnlist,
+                                          const sp2b_opts* opts) {
+  (void)threshold;
+  if (!h || !x || n <= 0 || !nsteps || *nsteps < 1 || !mu || !beta || !h1 || !hN || !sgnlist ||
+      !(occ_err_limit >= 0.0)) {
+    set_last_error("sp2b_sp2_fermi_init_norecs: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  sp2b_opts dflt;
+  sp2b_opts_default(&dflt);
+  if (!opts) opts = &dflt;
+  // Gershgorin bounds (src/prg_sp2_fermi_mod.F90:229-232); beta enters as the target
+  double gmin = 0.0, gmax = 0.0;
+  int rc = sp2b_gershgorin(h, n, &gmin, &gmax, opts);
+  if (rc != SP2B_OK) return rc;
+  const double beta0 = *beta;
+  *mu = 0.5 * (gmax + gmin);
+  *h1 = tscale * gmin;
+  *hN = tscale * gmax;
+  FermiSetup s;
+  std::unique_lock<std::mutex> lk;
+  if ((rc = fermi_setup(h, n, *nsteps, true, opts, &s, &lk)) != SP2B_OK) return rc;
+  // The reference's first pass generates the branches and stops at the probe's step.  Here
+  // one pass of X alone generates all nsteps branches at the starting mu (step i's branch
+  // depends on the steps before it only), the probe picks the step, and the Newton passes
+  // replay that prefix, the first of them at the same mu as the reference's first pass.
+  FermiPass f{};
+  if ((rc = fermi_pass(s.c, s.hdev, n, *nsteps, nocc, *h1, *hN, *mu, true, false, s.st, &f)) !=
+      SP2B_OK)
+    return rc;
+  std::vector<int> gen(*nsteps);
+  if ((rc = fermi_read_sequence(s.c, *nsteps, gen.data())) != SP2B_OK) return rc;
+  const int steps = fermi_probe_steps(gen.data(), *nsteps, gmin, gmax, beta0);
+  for (int i = 0; i < steps; ++i) sgnlist[i] = gen[i];
+  *nsteps = steps;
+  return fermi_init_passes(s, n, steps, nocc, *h1, *hN, occ_err_limit, trace_limit, false, mu, beta,
+                           sgnlist, x, "sp2b_sp2_fermi_init_norecs");
+}
+
+extern "C" int sp2b_sp2_entropy_function(double mu, double h1, double hN, int nsteps,
+                                         const int* sgnlist, double* gg, double* ee, int npoints) {
+  constexpr int kMesh = 10001;   // ee = 0, 1e-4, ..., 1 (src/prg_sp2_fermi_mod.F90:494-512)
+  if (nsteps < 0 || (nsteps > 0 && !sgnlist) || !gg || !ee || npoints < 1 || npoints > kMesh) {
+    set_last_error("sp2b_sp2_entropy_function: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  // Running two-point Gauss-Legendre integral of the inverse SP2 map over each mesh interval
+  // (:514-525), then GG - GG(end) ee (:528).  A table of 10001 scalars, built on the host as
+  // the reference does.
+  const double dh = 0.0001, c1 = 1.0, c2 = 1.0;
+  const double x1 = 0.5773502691896257, x2 = -x1;
+  std::vector<double> e(kMesh), g(kMesh);
+  for (int i = 0; i < kMesh; ++i) e[i] = i * dh;
+  g[0] = 0.0;
+  double iint = 0.0;
+  for (int i = 0; i < kMesh - 1; ++i) {
+    const double a = e[i], b = e[i + 1];
+    const double c_1 = c1 * (b - a) / 2.0, c_2 = c2 * (b - a) / 2.0;
+    const double x_1 = ((b - a) * x1 + (b + a)) / 2.0;
+    const double x_2 = ((b - a) * x2 + (b + a)) / 2.0;
+    iint = iint + c_1 * fermi_sp2_inverse(x_1, mu, h1, hN, nsteps, sgnlist);
+    iint = iint + c_2 * fermi_sp2_inverse(x_2, mu, h1, hN, nsteps, sgnlist);
+    g[i + 1] = iint;
+  }
+  const double gend = g[kMesh - 1];
+  for (int i = 0; i < npoints; ++i) {
+    gg[i] = g[i] - gend * e[i];
+    ee[i] = e[i];
+  }
+  return SP2B_OK;
 }

@@ -201,6 +201,25 @@ void prg_sp2_fermi(bml_matrix_t* h, int osteps, int nsteps, double nocc, double*
          "prg_sp2_fermi");
 }
 
+void prg_sp2_fermi_init_norecs(bml_matrix_t* h, int* nsteps, double nocc, double tscale,
+                               double threshold, double occErrLimit, double traceLimit,
+                               bml_matrix_t* x, double* mu, double* beta, double* h1, double* hN,
+                               int* sgnlist, int verbose) {
+  (void)verbose;
+  if (!same_n(h, x) || !nsteps || !mu || !beta || !h1 || !hN || !sgnlist)
+    return finish(SP2B_BAD_ARG, "prg_sp2_fermi_init_norecs");
+  sp2b_opts o = defaults();
+  finish(sp2b_sp2_fermi_init_norecs(h->data, h->n, nsteps, nocc, tscale, threshold, occErrLimit,
+                                    traceLimit, x->data, mu, beta, h1, hN, sgnlist, &o),
+         "prg_sp2_fermi_init_norecs");
+}
+
+void prg_sp2_entropy_function(double mu, double h1, double hN, int nsteps, int* sgnlist,
+                              double* GG, double* ee) {
+  finish(sp2b_sp2_entropy_function(mu, h1, hN, nsteps, sgnlist, GG, ee, 1001),
+         "prg_sp2_entropy_function");
+}
+
 void prg_normalize(bml_matrix_t* h) {
   if (!h || !h->data) return finish(SP2B_BAD_ARG, "prg_normalize");
   sp2b_opts o = defaults();

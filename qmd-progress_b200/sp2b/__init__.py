@@ -25,7 +25,8 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "equal_partition", "PREC_FP64", "PREC_MIXED_FP16", "PREC_MIXED_BF16", "PREC_EXACT_INT8",
            "MCW_INT8",
            "MCW_FP64", "last_refinement_info", "compute_response_sp2", "subgraph_sp2_loop",
-           "last_subgraph_refined", "sp2_fermi_init", "sp2_fermi"]
+           "last_subgraph_refined", "sp2_fermi_init", "sp2_fermi",
+           "sp2_fermi_init_norecs", "sp2_entropy_function"]
 
 
 @dataclass
@@ -106,6 +107,41 @@ def sp2_fermi(h, osteps, nsteps, nocc, mu, beta, h1, hN, sgnlist, eps=1e-4, trac
                                sgn.ctypes.data_as(C.POINTER(C.c_int)), threshold, eps,
                                trace_limit, _ptr(x), C.byref(o)), "sp2_fermi")
     return x, m.value
+
+
+def sp2_fermi_init_norecs(h, nsteps, nocc, beta, tscale=1.0, occ_err_limit=1e-9,
+                          trace_limit=1e-12, threshold=0.0):
+    """prg_sp2_fermi_init_norecs (src/prg_sp2_fermi_mod.F90:198-372), FP64 on the GPU: beta
+    is the target inverse temperature, nsteps the most steps.  Returns
+    (x, nsteps, mu, beta, h1, hN, sgnlist) with the step count the probe chose."""
+    h = _f64(h)
+    n = h.shape[0]
+    x = np.empty_like(h)
+    sgn = np.zeros(max(nsteps, 1), dtype=np.int32)
+    ns = C.c_int(nsteps)
+    mu, b, h1, hN = C.c_double(), C.c_double(beta), C.c_double(), C.c_double()
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_sp2_fermi_init_norecs(_ptr(h), n, C.byref(ns), nocc, tscale, threshold,
+                                           occ_err_limit, trace_limit, _ptr(x), C.byref(mu),
+                                           C.byref(b), C.byref(h1), C.byref(hN),
+                                           sgn.ctypes.data_as(C.POINTER(C.c_int)), C.byref(o)),
+          "sp2_fermi_init_norecs")
+    k = ns.value
+    return x, k, mu.value, b.value, h1.value, hN.value, sgn[:k].tolist()
+
+
+def sp2_entropy_function(mu, h1, hN, sgnlist, npoints=10001):
+    """prg_sp2_entropy_function (src/prg_sp2_fermi_mod.F90:482-532): (GG, ee) on the mesh
+    0, 1e-4, ..., 1 (the first npoints of its 10001 points)."""
+    sgn = np.ascontiguousarray(sgnlist, dtype=np.int32)
+    gg = np.empty(npoints)
+    ee = np.empty(npoints)
+    check(lib().sp2b_sp2_entropy_function(mu, h1, hN, len(sgn),
+                                          sgn.ctypes.data_as(C.POINTER(C.c_int)),
+                                          gg.ctypes.data_as(C.POINTER(C.c_double)),
+                                          ee.ctypes.data_as(C.POINTER(C.c_double)), npoints),
+          "sp2_entropy_function")
+    return gg, ee
 
 
 def last_refinement_info():

@@ -56,7 +56,7 @@ def build(verbose: bool = False, force: bool = False, jobs: int = 8) -> str:
     srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=default", "-I" + INCLUDE, "-I" + CSRC,
-              "--expt-relaxed-constexpr"]
+              "--expt-relaxed-constexpr", "-Xcompiler", "-ffp-contract=off"]
     procs = []
     objs = []
     for s in srcs:

@@ -90,6 +90,9 @@ _SIGS = {
                                  C.POINTER(Opts)]),
     "sp2b_sp2_fermi": (_i, [_vp, _i, _i, _i, _d, _dp, _d, _d, _d, _ip, _d, _d, _d, _vp,
                             C.POINTER(Opts)]),
+    "sp2b_sp2_fermi_init_norecs": (_i, [_vp, _i, _ip, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp,
+                                        _dp, _ip, C.POINTER(Opts)]),
+    "sp2b_sp2_entropy_function": (_i, [_d, _d, _d, _i, _ip, _dp, _dp, _i]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
@@ -118,6 +121,9 @@ _SIGS = {
     "prg_sp2_submatrix_inplace": (None, [_vp, _d, _vp, _ip, _vp, _d, _d, _i]),
     "prg_sp2_fermi_init": (None, [_vp, _i, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp, _dp, _ip]),
     "prg_sp2_fermi": (None, [_vp, _i, _i, _d, _dp, _dp, _dp, _dp, _ip, _d, _d, _d, _vp]),
+    "prg_sp2_fermi_init_norecs": (None, [_vp, _ip, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp, _dp,
+                                          _ip, _i]),
+    "prg_sp2_entropy_function": (None, [_d, _d, _d, _i, _ip, _dp, _dp]),
     "prg_normalize": (None, [_vp]),
     "prg_check_idempotency": (None, [_vp, _d, _dp]),
 }

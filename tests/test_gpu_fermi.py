@@ -102,3 +102,20 @@ def test_progress_named_fermi_exports(cuda):
     assert np.linalg.norm(x - xf_r) <= 1e-10 * np.linalg.norm(xf_r)
     for b in (hb, xb):
         L.sp2b_bml_free(b)
+
+
+@pytest.mark.parametrize("beta0", [40.0, 1e12])
+def test_fermi_init_norecs_matches_oracle(cuda, beta0):
+    """prg_sp2_fermi_init_norecs: the probe's step count, the sequence up to it, mu and beta
+    to 1e-9 and X to 1e-10 relative Frobenius of the oracle."""
+    h = _lattice(8)
+    n = h.shape[0]
+    nocc = 0.5 * n
+    xr, kr, mur, betar, h1r, hNr, sgnr = O.sp2_fermi_init_norecs(h, 24, nocc, 1.0, 1e-9, 1e-12,
+                                                                 beta0)
+    x, k, mu, beta, h1, hN, sgn = sp2b.sp2_fermi_init_norecs(h, 24, nocc, beta0, 1.0, 1e-9, 1e-12)
+    assert k == kr and sgn == sgnr
+    assert abs(mu - mur) <= 1e-9 * max(1.0, abs(mur))
+    assert abs(beta - betar) <= 1e-9 * abs(betar)
+    assert np.linalg.norm(x - xr) <= 1e-10 * np.linalg.norm(xr)
+    assert abs(np.trace(x) - nocc) <= 1e-8
