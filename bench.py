@@ -36,6 +36,17 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "qmd-progress_b200"))
 
 
+def _tuning():
+    """The launch configurations the library measured in this run: key -> [choice, ms...]."""
+    import sp2b
+    out = {}
+    for k in sp2b.tune_keys():
+        got = sp2b.tune_get(k)
+        if got:
+            out[k] = [got[0]] + [round(m, 4) for m in got[1]]
+    return out
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,7 +379,8 @@ def main():
                # algorithmic: 2N^3 per SP2 step + 4N^3 for the McWeeny step (mixed)
                "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
                "fp64": fp64, "e2e": e2e, "roofline": roofline, "refinement": refinement,
-               "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches}
+               "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+               "tuning": _tuning()}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -514,7 +526,7 @@ def run_subgraph(args, rank, world, local):
                "fp64": {"solves_per_s": world * max(1, args.fp64_steps) / (t64 / 1e3),
                         "ms_per_solve": t64 / max(1, args.fp64_steps)},
                "err_vs_fp64": {"fro_over_n": err_vs_fp64, "rel_fro": rel_vs_fp64},
-               "clocks": clk.summary(), "gpu_launches": launches}
+               "clocks": clk.summary(), "gpu_launches": launches, "tuning": _tuning()}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()

@@ -231,6 +231,25 @@ int sp2b_sp2_fermi_init_norecs(const double* h, int n, int* nsteps, double nocc,
 int sp2b_sp2_entropy_function(double mu, double h1, double hN, int nsteps, const int* sgnlist,
                               double* gg, double* ee, int npoints);
 
+/* ---- Launch-configuration autotuner ---------------------------------------------------
+ * The first solve of a new shape on a device times the equivalent launch configurations of
+ * its step kernel with CUDA events and keeps the fastest:
+ *   "f64-step/sm<S>/np<np>"          dense FP64 step tile edge, 128 or 64;
+ *   "subgraph/f64/sm<S>/<np>x<k>,..." batched FP64 sub-graph tile edge, 64 or 32;
+ *   "subgraph/split/sm<S>/<np>x<k>,..." batched split tile order, 0 (largest parts first) or
+ *                                     1 (every other wave reversed: balanced over the CTAs).
+ * (<np>x<k>: k parts of padded size np.)  The candidates compute the same products (same k
+ * order per element; independent tiles), so a choice changes speed, not results, except
+ * the order in which the per-iteration sums vv of a split batch are added.  SP2B_TUNE=0
+ * keeps the built-in rules; SP2B_TUNE_FILE=path is read on first use and appended to.
+ * sp2b_tune_set records a choice (it applies to solves that start afterwards);
+ * sp2b_tune_get returns SP2B_BAD_ARG for an unknown key; sp2b_tune_keys writes the keys,
+ * one per line, and returns the length needed including the terminator. */
+int sp2b_tune_get(const char* key, int* choice, float* ms, int max_ms, int* nms);
+int sp2b_tune_set(const char* key, int choice);
+int sp2b_tune_keys(char* buf, int cap);
+int sp2b_tune_clear(void);
+
 /* Graph of the sub-graph loop on the GPU: the pattern of |H^2| > gthreshold (the H^2
  * graph the sub-graph benchmark partitions,
  * benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65, formed there

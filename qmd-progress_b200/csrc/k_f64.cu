@@ -1,8 +1,12 @@
 // FP64 kernels: Gershgorin bounds, normalisation, and the symmetric-tile DMMA product
 // with the fused SP2 epilogue.  This is the parity form of the SP2 step (1e-10).
 #include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
 
 #include "reduce.cuh"
+#include "sp2b_tune.h"
 
 namespace sp2b {
 
@@ -593,9 +597,17 @@ cudaError_t launch_f64_multistep(const MultiStepArgs& a, cudaStream_t st) {
   return e;
 }
 
+// Tile edge of the dense FP64 step for np: the measured choice when one was made for this
+// device and size (tune_f64_tile), else 128 once its tiles fill the SMs twice, else 64.
 int f64_tile(int np) {
+  int c = 0;
+  if (tune_lookup(f64_tune_key(np), &c) && (c == 64 || c == 128)) return c;
   const int t128 = np / 128;
   return (t128 * (t128 + 1) / 2 >= 2 * 148) ? 128 : 64;
+}
+
+std::string f64_tune_key(int np) {
+  return "f64-step/sm" + std::to_string(device_sms()) + "/np" + std::to_string(np);
 }
 
 int f64_ntiles(int np) {
@@ -632,7 +644,43 @@ cudaError_t launch_sym_gemm_f64(const StepArgs& a0, cudaStream_t st) {
   if (a.ld == 0) a.ld = a.np;
   const int bt = f64_tile(a.np);
   const int t = a.np / bt;
-  return launch_f64_bt(a, bt, t * (t + 1) / 2, st);
+  a.ntiles = t * (t + 1) / 2;   // the partial sums the last CTA reduces: one per launched tile
+  return launch_f64_bt(a, bt, a.ntiles, st);
+}
+
+// Measures the dense step's tile edges 128 and 64 at np (one plain product each on
+// x_in -> x_out, the same k order per element in both) and records the faster one for
+// f64_tile.  partials must hold 4 doubles per 64-edge tile.
+int tune_f64_tile(int np, const double* x_in, double* x_out, double* partials, unsigned* counter,
+                  double* sums_out, cudaStream_t st) {
+  int c = 0;
+  const std::string key = f64_tune_key(np);
+  if (!tune_enabled() || tune_lookup(key, &c)) return 0;
+  const int edges[2] = {128, 64};
+  StepArgs q;
+  memset(&q, 0, sizeof(q));
+  q.np = np;
+  q.ld = np;
+  q.A = q.B = q.E = x_in;
+  q.out = x_out;
+  q.alpha = 1.0;
+  q.beta = 0.0;
+  q.partials = partials;
+  q.counter = counter;
+  q.sums_out = sums_out;
+  std::vector<float> ms;
+  int best = 0;
+  const int rc = tune_measure(2, 2, st, [&](int cand) -> int {
+    const int t = np / edges[cand];
+    q.ntiles = t * (t + 1) / 2;
+    if (cudaMemsetAsync(counter, 0, 4 * sizeof(unsigned), st) != cudaSuccess ||
+        launch_f64_bt(q, edges[cand], q.ntiles, st) != cudaSuccess)
+      return 3;   // SP2B_CUDA_ERROR
+    return 0;
+  }, &ms, &best);
+  if (rc != 0) return rc;
+  tune_store(key, edges[best], ms);
+  return 0;
 }
 
 cudaError_t launch_sym_gemm_f64_batched(const StepArgs& a, int bt, cudaStream_t st) {

@@ -1,5 +1,6 @@
 // Launch interfaces shared by the sp2b translation units.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "sp2b_common.cuh"
@@ -60,6 +61,10 @@ struct StepArgs {
 
 // FP64 path ---------------------------------------------------------------------------
 int f64_tile(int np);  // tile edge chosen for this size (64 or 128)
+std::string f64_tune_key(int np);
+int tune_f64_tile(int np, const double* x_in, double* x_out, double* partials, unsigned* counter,
+                  double* sums_out, cudaStream_t st);
+int device_sms();       // SM count of the current device
 int f64_ntiles(int np);
 cudaError_t launch_gersh(const double* h, int n, int ld, double* rowsum, int nsplit,
                          double* bounds, double* partials, unsigned* counter, cudaStream_t st);

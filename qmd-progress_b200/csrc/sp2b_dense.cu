@@ -103,7 +103,10 @@ cudaError_t Ctx::ensure_common(size_t nin, int np, int maxlaunch, int n) {
     e = grow(hin, hin_cap, nin);
     if (e != cudaSuccess) return e;
   }
-  const size_t parts = 4 * (size_t)std::max(std::max(f64_ntiles(np), tc_ntiles(np)), 148 * 8);
+  // one partial set per tile of the smallest FP64 edge (64) the step may use
+  const long long t64 = np / 64;
+  const size_t parts =
+      4 * (size_t)std::max<long long>(std::max<long long>(t64 * (t64 + 1) / 2, tc_ntiles(np)), 148 * 8);
   if ((e = grow(partials, partials_cap, parts)) != cudaSuccess) return e;
   if ((e = grow(rec, rec_cap, (size_t)maxlaunch + 2)) != cudaSuccess) return e;
   if ((e = grow(pp_dev, pp_cap, (size_t)maxlaunch + 2)) != cudaSuccess) return e;
@@ -227,6 +230,15 @@ int dense_solve(const DenseJob& j) {
   SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
   SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : (resp ? 5 : 2)));
   if (split) SP2B_CUDA_TRY(c->ensure_split(np));
+  // FP64 steps: the measured tile edge for this size (first solve at np on this device)
+  if (!split && !exact) {
+    const int trc = tune_f64_tile(np, c->x64[0], c->x64[1], c->partials, c->counter,
+                                  c->small + 16, st);
+    if (trc != SP2B_OK) {
+      set_last_error("FP64 tile tuning failed");
+      return trc;
+    }
+  }
   if (oz || exact) {
     if (np > 65536) {
       set_last_error("bad argument: n=%d above the INT8 products' limit", n);

@@ -9,11 +9,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "kernels_subgraph.cuh"
 #include "sp2b_ctx.h"
+#include "sp2b_tune.h"
 
 namespace sp2b {
 
@@ -58,7 +61,7 @@ struct SubBufs {
   std::vector<long long> last_hp;
   std::vector<int> last_lls, last_hidx;
   std::vector<PartDesc> P;
-  int ld = 0, ntiles = 0, layout_bt = 0;
+  int ld = 0, ntiles = 0, layout_bt = 0, layout_order = 0;
   long long rows = 0, coff = 0;
   bool layout_valid = false;
   // instantiated graph of the last call and the inputs it was captured with
@@ -92,6 +95,9 @@ struct SubJob {
   bool clear_dense;      // zero `dense` before the scatter
   bool part_idem;        // split only: per-part idempotency sums into b.idem
   bool multistep;        // FP64 only: all steps in one cooperative launch when it fits
+  // measured launch configuration (-1: the built-in rule).  FP64: the tile edge (32 or 64);
+  // split: the order of the tile list (0 largest parts first, 1 balanced over the CTAs)
+  int variant = -1;
 };
 
 // Builds (or reuses) the layout, buffers and CUDA graph of `j` in `b`, launches the
@@ -119,9 +125,11 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       t64 += t * (t + 1) / 2;
     }
     bt = (t64 < 148 || j.multistep) ? 32 : 64;
+    if (!j.multistep && (j.variant == 32 || j.variant == 64)) bt = j.variant;
   }
-  const bool same_layout = b.layout_valid && b.layout_bt == bt && b.last_hp == hp &&
-                           b.last_lls == lls && b.last_hidx == hidx;
+  const int tile_order = (split && j.variant == 1) ? 1 : 0;
+  const bool same_layout = b.layout_valid && b.layout_bt == bt && b.layout_order == tile_order &&
+                           b.last_hp == hp && b.last_lls == lls && b.last_hidx == hidx;
   if (!same_layout) {
     b.layout_valid = false;
     std::vector<PartDesc>& P = b.P;
@@ -187,6 +195,14 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
                                     P[p].ncore > 0 ? P[p].ncore : -1));
     }
     const int ntiles = (int)tiles.size();
+    if (tile_order == 1) {
+      // balanced: CTA c of the persistent grid (G CTAs) takes tiles c, c + G, ...; reversing
+      // every other wave of the cost-sorted list pairs each CTA's expensive tiles with cheap
+      // ones (the tiles' costs fall along the list: parts largest first)
+      const int G = std::min(ntiles, device_sms());
+      for (int w0 = G; w0 < ntiles; w0 += 2 * G)
+        std::reverse(tiles.begin() + w0, tiles.begin() + std::min(ntiles, w0 + G));
+    }
     if (bt == 32) {
       // the multi-step launch: one CTA per tile, the part index in place of the core count
       std::vector<int4> ms;
@@ -224,6 +240,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     b.last_lls = lls;
     b.last_hidx = hidx;
     b.layout_bt = bt;
+    b.layout_order = tile_order;
     b.layout_valid = true;
   }
   const int ld = b.ld;
@@ -449,6 +466,39 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   return SP2B_OK;
 }
 
+// The measured configuration of a batched solve (FP64: tile edge 64 or 32; split: tile
+// order), chosen once per device, precision and multiset of padded part sizes by timing
+// whole solves of this job; sets j.variant.
+static int tune_subgraph(Ctx* c, SubBufs& b, SubJob& j, cudaStream_t st) {
+  j.variant = -1;
+  if (!tune_enabled() || j.maxiter <= 0 || j.multistep) return SP2B_OK;
+  const bool split = j.prec != SP2B_PREC_FP64;
+  const std::vector<long long>& hp = *j.hp;
+  std::map<int, int> hist;
+  for (size_t p = 0; p + 1 < hp.size(); ++p) ++hist[padded((int)(hp[p + 1] - hp[p]))];
+  std::string key = std::string("subgraph/") + (split ? "split" : "f64") + "/sm" +
+                    std::to_string(device_sms()) + "/";
+  for (const auto& kv : hist) key += std::to_string(kv.first) + "x" + std::to_string(kv.second) + ",";
+  int choice = -1;
+  if (tune_lookup(key, &choice)) {
+    j.variant = choice;
+    return SP2B_OK;
+  }
+  const int cands[2] = {split ? 0 : 64, split ? 1 : 32};
+  std::vector<double> vtmp;
+  std::vector<float> ms;
+  int best = 0;
+  const int rc = tune_measure(2, 2, st, [&](int k) {
+    SubJob jc = j;
+    jc.variant = cands[k];
+    return batched_solve(c, b, jc, st, vtmp);
+  }, &ms, &best);
+  if (rc != SP2B_OK) return rc;
+  tune_store(key, cands[best], ms);
+  j.variant = cands[best];
+  return SP2B_OK;
+}
+
 }  // namespace sp2b
 
 using namespace sp2b;
@@ -539,7 +589,9 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   SubJob j{n, rp_d, col_d, val_d, &hp, &lls, &hidx, pp, maxiter, mineval, maxeval, prec,
            core_d, dense_d, true, refine, false};
   std::vector<double> vvh;
-  int rc = batched_solve(c, b, j, st, vvh);
+  int rc = tune_subgraph(c, b, j, st);
+  if (rc != SP2B_OK) return rc;
+  rc = batched_solve(c, b, j, st, vvh);
   if (rc != SP2B_OK) return rc;
 
   // ---- FP64 re-solve of the parts left with a half-occupied state ----

@@ -26,7 +26,8 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "MCW_INT8",
            "MCW_FP64", "last_refinement_info", "compute_response_sp2", "subgraph_sp2_loop",
            "last_subgraph_refined", "sp2_fermi_init", "sp2_fermi",
-           "sp2_fermi_init_norecs", "sp2_entropy_function"]
+           "sp2_fermi_init_norecs", "sp2_entropy_function",
+           "tune_keys", "tune_get", "tune_set", "tune_clear"]
 
 
 @dataclass
@@ -142,6 +143,33 @@ def sp2_entropy_function(mu, h1, hN, sgnlist, npoints=10001):
                                           ee.ctypes.data_as(C.POINTER(C.c_double)), npoints),
           "sp2_entropy_function")
     return gg, ee
+
+
+def tune_keys():
+    """Keys of the launch-configuration decisions made (or loaded) in this process."""
+    need = lib().sp2b_tune_keys(None, 0)
+    buf = C.create_string_buffer(need)
+    lib().sp2b_tune_keys(buf, need)
+    return [k for k in buf.value.decode().split("\n") if k]
+
+
+def tune_get(key):
+    """(choice, [median ms per candidate]) of a decision, or None for an unknown key."""
+    ch, nms = C.c_int(0), C.c_int(0)
+    ms = (C.c_float * 8)()
+    if lib().sp2b_tune_get(key.encode(), C.byref(ch), ms, 8, C.byref(nms)) != 0:
+        return None
+    return ch.value, list(ms[:min(nms.value, 8)])
+
+
+def tune_set(key, choice):
+    """Record a launch-configuration choice for the solves that start afterwards."""
+    check(lib().sp2b_tune_set(key.encode(), int(choice)), "tune_set")
+
+
+def tune_clear():
+    """Forget every decision (the next solve of each shape measures again)."""
+    check(lib().sp2b_tune_clear(), "tune_clear")
 
 
 def last_refinement_info():

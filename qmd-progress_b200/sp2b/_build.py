@@ -29,6 +29,7 @@ SOURCES = [
     "sp2b_noalloc.cu",
     "sp2b_adjoint.cu",
     "sp2b_host.cpp",
+    "sp2b_tune.cpp",
     "sp2b_prg.cpp",
 ]
 

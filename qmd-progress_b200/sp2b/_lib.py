@@ -93,6 +93,10 @@ _SIGS = {
     "sp2b_sp2_fermi_init_norecs": (_i, [_vp, _i, _ip, _d, _d, _d, _d, _d, _vp, _dp, _dp, _dp,
                                         _dp, _ip, C.POINTER(Opts)]),
     "sp2b_sp2_entropy_function": (_i, [_d, _d, _d, _i, _ip, _dp, _dp, _i]),
+    "sp2b_tune_get": (_i, [C.c_char_p, _ip, C.POINTER(C.c_float), _i, _ip]),
+    "sp2b_tune_set": (_i, [C.c_char_p, _i]),
+    "sp2b_tune_keys": (_i, [C.c_char_p, _i]),
+    "sp2b_tune_clear": (_i, []),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
