@@ -166,6 +166,42 @@ def cpu_baseline_sample(n, iters_per_solve, max_seconds=20.0):
                       f"DGEMM, {os.cpu_count()} threads), extrapolated to {iters_per_solve} iterations per solve"}
 
 
+def subgraph_cpu_sample(rp, col, val, n, hp, hidx, lls, seq, maxiter, emin, emax,
+                        max_seconds=15.0):
+    """The oracle's FP64 prg_sp2_submatrix per part (numpy with the host BLAS, all host
+    cores), parts in order until ~max_seconds, extrapolated by the parts' n^3 to the whole
+    serial part loop."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+    import sp2_oracle as O
+    pos = np.full(n, -1, dtype=np.int64)
+    total = float(sum((hp[p + 1] - hp[p]) ** 3 for p in range(len(lls))))
+    done_w = 0.0
+    done = 0
+    t0 = time.perf_counter()
+    for p in range(len(lls)):
+        idx = np.asarray(hidx[hp[p]:hp[p + 1]], dtype=np.int64)
+        m = len(idx)
+        pos[idx] = np.arange(m)
+        sub = np.zeros((m, m))
+        for r, i in enumerate(idx):
+            c = col[rp[i]:rp[i + 1]]
+            keep = pos[c] >= 0
+            sub[r, pos[c[keep]]] = val[rp[i]:rp[i + 1]][keep]
+        vv = np.zeros(max(maxiter, 1))
+        O.sp2_submatrix(sub, seq, maxiter, vv, emin, emax, int(lls[p]))
+        pos[idx] = -1
+        done_w += float(m) ** 3
+        done += 1
+        if time.perf_counter() - t0 > max_seconds:
+            break
+    el = time.perf_counter() - t0
+    t_solve = el * total / done_w
+    return {"value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{done} of {len(lls)} parts (prg_sp2_submatrix, {maxiter} steps, numpy/OpenBLAS "
+                      f"DGEMM, {os.cpu_count()} threads), extrapolated by n^3 to the serial part loop"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -468,13 +504,24 @@ def run_subgraph(args, rank, world, local):
     vvo = np.zeros(max(maxiter, 1))
     stream = torch.cuda.current_stream()
 
-    def solve(prec):
-        oo = _lib.make_opts(precision=prec, device_ptrs=True, stream=stream.cuda_stream)
+    def solve(prec, iters=None, refine_tol=None):
+        oo = _lib.make_opts(precision=prec, device_ptrs=True, stream=stream.cuda_stream,
+                            refine_tol=refine_tol)
         _lib.check(Lb.sp2b_subgraph_sp2_loop(n, rp_d.data_ptr(), col_d.data_ptr(), val_d.data_ptr(),
                                              len(parts), hp_d.data_ptr(), hidx_d.data_ptr(),
-                                             lls_d.data_ptr(), seq_a.ctypes.data, maxiter, emin, emax,
+                                             lls_d.data_ptr(), seq_a.ctypes.data,
+                                             maxiter if iters is None else iters, emin, emax,
                                              core_d.data_ptr(), None, vvo.ctypes.data, C.byref(oo)),
                    "subgraph_sp2_loop")
+
+    def events_ms(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
 
     def timed(prec, steps):
         for _ in range(args.warmup):
@@ -503,6 +550,64 @@ def run_subgraph(args, rank, world, local):
     core_mixed = core_d.clone()
     nref = C.c_int(0)
     Lb.sp2b_last_subgraph_refined(C.byref(nref), None, 0, None, 0)
+    # ---- roofline of the batched SP2 step (one launch covers every part) ----
+    # average step-launch duration = (solve - the same solve with no SP2 steps) / maxIter,
+    # both without the FP64 re-solve of flagged parts, CUDA events on the launch stream
+    # (each form warmed up right before it is timed: the library re-captures its graph when
+    # the step count or the outputs change)
+    solve(prec, refine_tol=0.0)
+    t_steps = events_ms(lambda: solve(prec, refine_tol=0.0), 3)
+    solve(prec, iters=0, refine_tol=0.0)
+    t_none = events_ms(lambda: solve(prec, iters=0, refine_tol=0.0), 3)
+    step_avg_ms = max(t_steps - t_none, 1e-6) / max(maxiter, 1)
+    flops_launch = 2.0 * float(np.sum(ls.astype(np.float64) ** 3))
+    peaks, psrc = load_peaks()
+    peak_key = "bf16_tflops_sustained" if "bf16_tflops_sustained" in peaks else "bf16_tflops"
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            ent = json.load(f).get(f"sp2_step_batched_{args.precision}_cubic20_64parts")
+        if ent:
+            # captured on the 20^3 / 64-part case; DRAM bytes scale with the tiles' work
+            traffic = ent["bytes_per_launch"] * flops_launch / ent["flops_per_launch"]
+    achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
+                "frac": achieved / peaks[peak_key], "traffic": traffic,
+                "peak_source": f"{psrc} {peak_key}",
+                "kernel": "k_tc_persist<T,0,1> (batched SP2 step, all parts)",
+                "avg_launch_ms": step_avg_ms, "flops_per_launch": flops_launch,
+                "timing": "(solve - solve with no steps) / maxIter, FP64 re-solve off"}
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        rp_h = torch.from_numpy(rp).pin_memory()
+        col_h = torch.from_numpy(col).pin_memory()
+        val_h = torch.from_numpy(val).pin_memory()
+        core_h = torch.empty(core_d.numel(), dtype=torch.float64).pin_memory()
+        oh = _lib.make_opts(precision=prec, device_ptrs=False, stream=stream.cuda_stream)
+        hp_a = np.ascontiguousarray(hp, dtype=np.int64)
+        hidx_a = np.ascontiguousarray(hidx, dtype=np.int32)
+        lls_a = np.ascontiguousarray(lls, dtype=np.int32)
+
+        def solve_host():
+            _lib.check(Lb.sp2b_subgraph_sp2_loop(n, rp_h.data_ptr(), col_h.data_ptr(), val_h.data_ptr(),
+                                                 len(parts), hp_a.ctypes.data, hidx_a.ctypes.data,
+                                                 lls_a.ctypes.data, seq_a.ctypes.data, maxiter, emin,
+                                                 emax, core_h.data_ptr(), None, vvo.ctypes.data,
+                                                 C.byref(oh)), "subgraph_sp2_loop(host)")
+        solve_host()
+        te = events_ms(solve_host, args.steps)
+        # H (CSR) and pp in; the core rows and vv out, every call
+        h2d = rp.nbytes + col.nbytes + val.nbytes + seq_a.nbytes
+        e2e = {"value": world / (te / 1e3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(core_d.numel() * 8 + maxiter * 8)}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = subgraph_cpu_sample(rp, col, val, n, hp, hidx, lls, seq, maxiter, emin, emax)
+
     t64, _ = timed(_lib.PREC_FP64, max(1, args.fp64_steps))
     err_vs_fp64 = float((core_mixed - core_d).norm().item()) / n
     rel_vs_fp64 = float((core_mixed - core_d).norm().item() / core_d.norm().item())
@@ -526,6 +631,7 @@ def run_subgraph(args, rank, world, local):
                "fp64": {"solves_per_s": world * max(1, args.fp64_steps) / (t64 / 1e3),
                         "ms_per_solve": t64 / max(1, args.fp64_steps)},
                "err_vs_fp64": {"fro_over_n": err_vs_fp64, "rel_fro": rel_vs_fp64},
+               "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
                "clocks": clk.summary(), "gpu_launches": launches, "tuning": _tuning()}
         print(json.dumps(out), flush=True)
     if dist:

@@ -471,7 +471,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
 // whole solves of this job; sets j.variant.
 static int tune_subgraph(Ctx* c, SubBufs& b, SubJob& j, cudaStream_t st) {
   j.variant = -1;
-  if (!tune_enabled() || j.maxiter <= 0 || j.multistep) return SP2B_OK;
+  if (!tune_enabled() || j.multistep) return SP2B_OK;
   const bool split = j.prec != SP2B_PREC_FP64;
   const std::vector<long long>& hp = *j.hp;
   std::map<int, int> hist;
@@ -484,6 +484,7 @@ static int tune_subgraph(Ctx* c, SubBufs& b, SubJob& j, cudaStream_t st) {
     j.variant = choice;
     return SP2B_OK;
   }
+  if (j.maxiter <= 0) return SP2B_OK;   // no steps to time
   const int cands[2] = {split ? 0 : 64, split ? 1 : 32};
   std::vector<double> vtmp;
   std::vector<float> ms;
