@@ -668,6 +668,10 @@ int tune_f64_tile(int np, const double* x_in, double* x_out, double* partials, u
   q.partials = partials;
   q.counter = counter;
   q.sums_out = sums_out;
+  // timed on zeros (the buffer may not hold data yet; DMMA time does not depend on values)
+  if (cudaMemsetAsync(const_cast<double*>(x_in), 0, (size_t)np * np * sizeof(double), st) !=
+      cudaSuccess)
+    return 3;   // SP2B_CUDA_ERROR
   std::vector<float> ms;
   int best = 0;
   const int rc = tune_measure(2, 2, st, [&](int cand) -> int {
