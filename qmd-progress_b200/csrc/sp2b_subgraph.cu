@@ -71,6 +71,29 @@ struct SubBufs {
 static SubBufs g_sub[64];
 static SubBufs g_sub_ref[64];  // the FP64 re-solve of the parts a split call flags
 
+// True for page-locked (pinned or registered) host memory, which a copy on another
+// stream can fill while kernels run.
+static bool host_locked(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// A second stream per device for output copies that overlap the FP64 re-solve.
+static cudaError_t copy_stream(int dev, cudaStream_t* s) {
+  static cudaStream_t streams[64] = {};
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!streams[dev]) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  *s = streams[dev];
+  return cudaSuccess;
+}
+
 // Parts of the last sub-graph call of this thread solved again in FP64, and every
 // part's core-row idempotency sum.
 static thread_local std::vector<int> t_refined;
@@ -587,6 +610,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   }
 
   const bool refine = split && opts->refine_tol > 0.0 && maxiter > 0;
+  bool core_out_done = false;   // the core rows already reached rho_core (host calls)
   SubJob j{n, rp_d, col_d, val_d, &hp, &lls, &hidx, pp, maxiter, mineval, maxeval, prec,
            core_d, dense_d, true, refine, false};
   std::vector<double> vvh;
@@ -621,10 +645,26 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         SP2B_CUDA_TRY(grow_buf(rb.core, rb.core_cap, (size_t)std::max(rcoff, 1LL)));
         rcore = rb.core;
       }
+      // A host-pointer call whose core output is page-locked: the split solve's core rows
+      // (final but for the re-solved parts' blocks) leave on a second stream while the
+      // re-solve runs, and the re-solved blocks follow from its output once they are out.
+      cudaStream_t cs = nullptr;
+      if (!dev && rho_core && host_locked(rho_core)) {
+        SP2B_CUDA_TRY(copy_stream(c->dev, &cs));
+        SP2B_CUDA_TRY(cudaMemcpyAsync(rho_core, b.core, coff * sizeof(double),
+                                      cudaMemcpyDeviceToHost, cs));
+      }
       SubJob rj{n, rp_d, col_d, val_d, &rhp, &rlls, &ridx, pp, maxiter, mineval, maxeval,
                 SP2B_PREC_FP64, rcore, dense_d, false, false, true};
       std::vector<double> rvv;
       rc = batched_solve(c, rb, rj, st, rvv);
+      if (cs) {
+        const cudaError_t ce = cudaStreamSynchronize(cs);
+        if (rc == SP2B_OK && ce != cudaSuccess) {
+          set_last_error("core-row copy failed: %s", cudaGetErrorString(ce));
+          return SP2B_CUDA_ERROR;
+        }
+      }
       if (rc != SP2B_OK) return rc;
       if (core_d) {
         // part p's block sits at sum_{q<p} llsize[q]*lsize[q] in both packings
@@ -634,12 +674,17 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
           long long dst = 0;
           for (int r = 0; r < p; ++r) dst += (long long)lls[r] * (hp[r + 1] - hp[r]);
           const long long m = (long long)lls[p] * (hp[p + 1] - hp[p]);
-          SP2B_CUDA_TRY(cudaMemcpyAsync(core_d + dst, rcore + src, m * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, st));
+          if (cs)
+            SP2B_CUDA_TRY(cudaMemcpyAsync(rho_core + dst, rcore + src, m * sizeof(double),
+                                          cudaMemcpyDeviceToHost, st));
+          else
+            SP2B_CUDA_TRY(cudaMemcpyAsync(core_d + dst, rcore + src, m * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
           src += m;
         }
         SP2B_CUDA_TRY(cudaStreamSynchronize(st));
       }
+      core_out_done = cs != nullptr;
     }
   }
 
@@ -649,7 +694,7 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     std::memcpy(vv, vvh.data(), maxiter * sizeof(double));
   }
   if (!dev) {
-    if (rho_core)
+    if (rho_core && !core_out_done)
       SP2B_CUDA_TRY(cudaMemcpy(rho_core, b.core, coff * sizeof(double), cudaMemcpyDeviceToHost));
     if (rho_dense)
       SP2B_CUDA_TRY(cudaMemcpy(rho_dense, b.dense, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost));

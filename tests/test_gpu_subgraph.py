@@ -182,3 +182,39 @@ def test_subgraph_refinement_replaces_flagged_parts_with_fp64(cuda):
             assert np.array_equal(core[blk], c0[blk])
         idx = hi[hp[p]:hp[p + 1]]
         assert np.array_equal(rho[np.ix_(idx[:lls[p]], idx)], core[blk].reshape(lls[p], ls[p]))
+
+
+def test_subgraph_refinement_into_pinned_host_output(cuda):
+    """A host-pointer call with a page-locked core output copies the split rows out while
+    the FP64 re-solve runs, then the re-solved blocks: the result equals the call with a
+    pageable output bit for bit."""
+    import ctypes as C
+    from sp2b import _lib
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    mi = maxiter - 6
+    rp, col, val = sp2b.dense_to_csr(h)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, (rp, col, val))
+    # the per-part sums (computed when refinement is on; the default threshold)
+    sp2b.subgraph_sp2_loop(n, (rp, col, val), hp, hi, lls, pp[:mi], mi, emin, emax, dense=False,
+                           core=True)
+    _, idem = sp2b.last_subgraph_refined(len(lls))
+    assert idem.max() > 0
+    tol = float(np.median(idem[idem > 0]))
+    _, core_pageable, _ = sp2b.subgraph_sp2_loop(n, (rp, col, val), hp, hi, lls, pp[:mi], mi, emin,
+                                                 emax, dense=False, core=True, refine_tol=tol)
+    flagged, _ = sp2b.last_subgraph_refined(len(lls))
+    assert flagged
+    core_pinned = cuda.zeros(core_pageable.size, dtype=cuda.float64).pin_memory()
+    hp_a = np.ascontiguousarray(hp, np.int64)
+    hi_a = np.ascontiguousarray(hi, np.int32)
+    lls_a = np.ascontiguousarray(lls, np.int32)
+    pp_a = np.ascontiguousarray(pp[:mi], np.int32)
+    vv = np.zeros(mi)
+    o = _lib.make_opts(precision=_lib.PREC_MIXED_FP16, refine_tol=tol)
+    _lib.check(_lib.lib().sp2b_subgraph_sp2_loop(
+        n, rp.ctypes.data, col.ctypes.data, val.ctypes.data, len(lls), hp_a.ctypes.data,
+        hi_a.ctypes.data, lls_a.ctypes.data, pp_a.ctypes.data, mi, emin, emax,
+        core_pinned.data_ptr(), None, vv.ctypes.data, C.byref(o)), "subgraph_sp2_loop")
+    assert sp2b.last_subgraph_refined(len(lls))[0] == flagged
+    assert np.array_equal(core_pinned.numpy(), core_pageable)
