@@ -250,6 +250,18 @@ int sp2b_tune_set(const char* key, int choice);
 int sp2b_tune_keys(char* buf, int cap);
 int sp2b_tune_clear(void);
 
+/* ELLPACK -> CSR, the sparse input of the sub-graph calls and of the graph builder.
+ * ELLPACK as BML stores it on the C side (bml_matrix_ellpack): width m, row i's entries
+ * at [i*m, i*m + nnz[i]) of idx (0-based columns) and val.  Output: row_ptr (n+1, int64),
+ * col (int32) and csr_val, capacity cap.  Returns SP2B_BAD_ARG with the needed capacity
+ * in *needed (row_ptr filled) when col / csr_val are NULL or too small, SP2B_BAD_INPUT
+ * for nnz[i] outside [0, m] or a column outside [0, n).  Host pointers: converted on the
+ * host; device pointers (opts.device_ptrs): one warp per row on the GPU, ordered on
+ * opts.stream. */
+int sp2b_ellpack_to_csr(int n, int m, const int* nnz, const int* idx, const double* val,
+                        long long* row_ptr, int* col, double* csr_val, long long cap,
+                        long long* needed, const sp2b_opts* opts);
+
 /* Graph of the sub-graph loop on the GPU: the pattern of |H^2| > gthreshold (the H^2
  * graph the sub-graph benchmark partitions,
  * benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65, formed there

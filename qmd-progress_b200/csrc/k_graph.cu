@@ -113,6 +113,27 @@ static size_t graph_smem() {
   return (size_t)kGraphWarps * kGraphSlots * (2 * sizeof(int) + sizeof(double));
 }
 
+// ELLPACK rows to CSR: row i's entries sit at [i*m, i*m + nnz[i]) of idx / val (0-based
+// columns; the row-major ELLPACK layout of BML's C storage) and go to [rp[i], rp[i+1]).
+// One warp per row.  A column outside [0, n) is flagged in *bad and written as 0.
+__global__ void __launch_bounds__(256)
+    k_ell_to_csr(int n, int m, const int* __restrict__ nnz, const int* __restrict__ idx,
+                 const double* __restrict__ val, const long long* __restrict__ rp,
+                 int* __restrict__ col, double* __restrict__ cval, int* __restrict__ bad) {
+  const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const int k = nnz[i];   // 0 <= k <= m, checked by the host
+  const long long src = (long long)i * m, dst = rp[i];
+  for (int t = lane; t < k; t += 32) {
+    const int j = idx[src + t];
+    const bool ok = j >= 0 && j < n;
+    if (!ok) atomicExch(bad, 1);
+    col[dst + t] = ok ? j : 0;
+    cval[dst + t] = val[src + t];
+  }
+}
+
 }  // namespace sp2b
 
 using namespace sp2b;
@@ -234,6 +255,89 @@ extern "C" int sp2b_graph_square_threshold(int n, const long long* h_row_ptr, co
   if (e != cudaSuccess) {
     set_last_error("sp2b_graph_square_threshold: %s", cudaGetErrorString(e));
     return SP2B_CUDA_ERROR;
+  }
+  return SP2B_OK;
+}
+
+extern "C" int sp2b_ellpack_to_csr(int n, int m, const int* nnz, const int* idx, const double* val,
+                                   long long* row_ptr, int* col, double* csr_val, long long cap,
+                                   long long* needed, const sp2b_opts* opts) {
+  if (n <= 0 || m < 0 || !nnz || (m > 0 && (!idx || !val)) || !row_ptr) {
+    set_last_error("sp2b_ellpack_to_csr: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  sp2b_opts dflt;
+  sp2b_opts_default(&dflt);
+  if (!opts) opts = &dflt;
+  const bool dev = opts->device_ptrs != 0;
+  // row counts (device calls: fetched), checked and summed on the host
+  std::vector<int> cnt(n);
+  int status = SP2B_OK;
+  Ctx* c = nullptr;
+  cudaStream_t st = nullptr;
+  std::unique_lock<std::mutex> lk;
+  if (dev) {
+    c = get_ctx(&status);
+    if (!c) return status;
+    lk = std::unique_lock<std::mutex>(c->mu);
+    st = opts->stream ? (cudaStream_t)opts->stream : (cudaStream_t)0;
+    SP2B_CUDA_TRY(cudaMemcpyAsync(cnt.data(), nnz, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  } else {
+    std::memcpy(cnt.data(), nnz, n * sizeof(int));
+  }
+  std::vector<long long> rp(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    if (cnt[i] < 0 || cnt[i] > m) {
+      set_last_error("sp2b_ellpack_to_csr: row %d has %d entries (width %d)", i, cnt[i], m);
+      return SP2B_BAD_INPUT;
+    }
+    rp[i + 1] = rp[i] + cnt[i];
+  }
+  const long long total = rp[n];
+  if (needed) *needed = total;
+  if (dev) SP2B_CUDA_TRY(cudaMemcpyAsync(row_ptr, rp.data(), (n + 1) * sizeof(long long),
+                                         cudaMemcpyHostToDevice, st));
+  else std::memcpy(row_ptr, rp.data(), (n + 1) * sizeof(long long));
+  if (total > 0 && (!col || !csr_val || cap < total)) {
+    if (dev) SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    set_last_error("sp2b_ellpack_to_csr: col / val need %lld entries", total);
+    return SP2B_BAD_ARG;
+  }
+  if (!dev) {
+    // host arrays: a host copy (this is input formatting, not SP2 arithmetic)
+    for (int i = 0; i < n; ++i)
+      for (int t = 0; t < cnt[i]; ++t) {
+        const long long s = (long long)i * m + t;
+        if (idx[s] < 0 || idx[s] >= n) {
+          set_last_error("sp2b_ellpack_to_csr: row %d column %d out of range", i, idx[s]);
+          return SP2B_BAD_INPUT;
+        }
+        col[rp[i] + t] = idx[s];
+        csr_val[rp[i] + t] = val[s];
+      }
+    return SP2B_OK;
+  }
+  if (total == 0) {
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    return SP2B_OK;
+  }
+  int* bad = c->err;   // the context's device status word, cleared again below
+  SP2B_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+  const long long threads = (long long)n * 32;
+  const int block = 256;
+  k_ell_to_csr<<<(unsigned)((threads + block - 1) / block), block, 0, st>>>(n, m, nnz, idx, val,
+                                                                             row_ptr, col, csr_val,
+                                                                             bad);
+  note_launch();
+  SP2B_CUDA_TRY(cudaGetLastError());
+  int hbad = 0;
+  SP2B_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  SP2B_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), st));
+  if (hbad) {
+    set_last_error("sp2b_ellpack_to_csr: a column index is outside [0, %d)", n);
+    return SP2B_BAD_INPUT;
   }
   return SP2B_OK;
 }

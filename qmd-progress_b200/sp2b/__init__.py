@@ -27,7 +27,7 @@ __all__ = ["SP2Result", "SP2Error", "sp2_alg2", "sp2_alg2_genseq", "sp2_alg2_seq
            "MCW_FP64", "last_refinement_info", "compute_response_sp2", "subgraph_sp2_loop",
            "last_subgraph_refined", "sp2_fermi_init", "sp2_fermi",
            "sp2_fermi_init_norecs", "sp2_entropy_function",
-           "tune_keys", "tune_get", "tune_set", "tune_clear"]
+           "tune_keys", "tune_get", "tune_set", "tune_clear", "ellpack_to_csr"]
 
 
 @dataclass
@@ -378,6 +378,24 @@ def equal_partition(nodes_per_part, nnodes):
 # ----------------------------------------------------------------------------------
 # Graph-partitioned SP2 (prg_subgraphSP2Loop, src/prg_subgraphloop_mod.F90:36-126)
 # ----------------------------------------------------------------------------------
+
+def ellpack_to_csr(nnz, idx, val):
+    """CSR (row_ptr int64, col int32, val float64) of an ELLPACK matrix: idx / val of shape
+    (n, m) with row i's entries in its first nnz[i] slots (0-based columns)."""
+    idx = np.ascontiguousarray(idx, np.int32)
+    val = np.ascontiguousarray(val, np.float64)
+    nnz = np.ascontiguousarray(nnz, np.int32)
+    n, m = idx.shape
+    rp = np.zeros(n + 1, np.int64)
+    need = C.c_longlong(0)
+    cap = int(max(int(nnz.sum()), 1)) if len(nnz) else 1
+    col = np.zeros(cap, np.int32)
+    cv = np.zeros(cap)
+    check(lib().sp2b_ellpack_to_csr(n, m, _ptr(nnz), _ptr(idx), _ptr(val), _ptr(rp), _ptr(col),
+                                    _ptr(cv), cap, C.byref(need), None), "ellpack_to_csr")
+    k = int(need.value)
+    return rp, col[:k], cv[:k]
+
 
 def dense_to_csr(a):
     """CSR (row_ptr int64, col int32, val float64) of the nonzeros of a dense matrix."""

@@ -97,6 +97,8 @@ _SIGS = {
     "sp2b_tune_set": (_i, [C.c_char_p, _i]),
     "sp2b_tune_keys": (_i, [C.c_char_p, _i]),
     "sp2b_tune_clear": (_i, []),
+    "sp2b_ellpack_to_csr": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, C.c_longlong,
+                                 C.POINTER(C.c_longlong), C.POINTER(Opts)]),
     "sp2b_launch_count": (C.c_longlong, []),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
