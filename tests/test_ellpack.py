@@ -112,3 +112,22 @@ def test_subgraph_from_ellpack_equals_csr(cuda):
     r2, _, v2 = sp2b.subgraph_sp2_loop(n, csr2, hp, hi, lls, pp, len(pp), emin, emax,
                                        precision=sp2b.PREC_FP64)
     assert np.array_equal(r1, r2) and np.array_equal(v1, v2)
+
+
+def test_ellpack_to_csr_random_shapes():
+    """Random widths, fill and sizes (including empty rows, full rows, one row)."""
+    rng = np.random.default_rng(7)
+    for _ in range(40):
+        n = int(rng.integers(1, 200))
+        m = int(rng.integers(0, 12))
+        nnz = rng.integers(0, min(m, n) + 1, n).astype(np.int32)
+        idx = np.full((n, max(m, 1)), 12345, np.int32)[:, :m] if m else np.zeros((n, 0), np.int32)
+        val = rng.standard_normal((n, m))
+        for i in range(n):
+            idx[i, :nnz[i]] = rng.choice(n, nnz[i], replace=False)
+        rp, col, v = sp2b.ellpack_to_csr(nnz, idx, val)
+        if nnz.sum() == 0:
+            assert np.array_equal(rp, np.zeros(n + 1, np.int64))
+            continue
+        rr, cr, vr = _csr_ref(nnz, idx, val)
+        assert np.array_equal(rp, rr) and np.array_equal(col, cr) and np.array_equal(v, vr)
