@@ -202,6 +202,18 @@ def subgraph_cpu_sample(rp, col, val, n, hp, hidx, lls, seq, maxiter, emin, emax
                       f"DGEMM, {os.cpu_count()} threads), extrapolated by n^3 to the serial part loop"}
 
 
+def dense_metric(n):
+    return "SP2 solves/s (dense two-band N=%d)" % n
+
+
+def dense_config(args, n, world):
+    """The dense workload's config, the same on both arms (the reference arm times the
+    same solve H -> D on the host cores)."""
+    return {"workload": f"two_band_1d_n{n}_{args.precision}_alg2_mcweeny1", "n": n,
+            "bndfil": 0.5, "idemtol": 1e-10, "seed": "rank r solves seed r",
+            "parallelism": f"replicas{world}", "l2": "inputs 512 MiB > L2, no flush"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -216,11 +228,11 @@ def run_reference(args, rank, world):
         vals.append(r["value"])
     el = time.perf_counter() - t0
     v = statistics.median(vals)
-    out = {"metric": "SP2 solves/s (dense two-band N=%d)" % n, "value": v, "unit": "solves/s",
+    out = {"metric": dense_metric(n), "value": v, "unit": "solves/s",
            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"two_band_1d_n{n}_alg2", "n": n, "bndfil": 0.5, "seed": 0},
+           "config": dense_config(args, n, world),
            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port",
                             "sample": r["sample"]},
            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -403,15 +415,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(n, iters, max_seconds=20.0)
     if rank == 0:
-        out = {"metric": "SP2 solves/s (dense two-band N=%d, mixed precision)" % n, "value": value,
+        out = {"metric": dense_metric(n), "value": value,
                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": {_lib.PREC_MIXED_FP16: "f16", _lib.PREC_MIXED_BF16: "bf16",
                                               _lib.PREC_EXACT_INT8: "i8"}.get(prec, "f64"),
                "data": "synthetic",
-               "config": {"workload": f"two_band_1d_n{n}_{args.precision}_alg2_mcweeny1", "n": n,
-                          "bndfil": 0.5, "idemtol": 1e-10, "sp2_iters": iters,
-                          "parallelism": f"replicas{world}", "l2": "inputs 512 MiB > L2, no flush"},
+               "config": dense_config(args, n, world), "sp2_iters": iters,
                # algorithmic: 2N^3 per SP2 step + 4N^3 for the McWeeny step (mixed)
                "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
                "fp64": fp64, "e2e": e2e, "roofline": roofline, "refinement": refinement,
