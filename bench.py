@@ -132,6 +132,27 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def host_info():
+    """CPU model and the BLAS numpy calls, recorded beside every CPU figure."""
+    import numpy as np
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    blas = None
+    try:
+        b = np.show_config(mode="dicts").get("Build Dependencies", {}).get("blas", {})
+        blas = f"{b.get('name')} {b.get('version')}"
+    except Exception:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count(), "blas": blas}
+
+
 def cpu_baseline_sample(n, iters_per_solve, max_seconds=20.0):
     """Oracle FP64 alg2 loop on the host cores: time whole SP2 iterations of the N x N
     workload (bounded to ~max_seconds) and extrapolate to solves/s."""
@@ -161,7 +182,7 @@ def cpu_baseline_sample(n, iters_per_solve, max_seconds=20.0):
             break
     t_iter = el / done
     return {"value": 1.0 / (t_iter * iters_per_solve), "unit": "solves/s", "cores": os.cpu_count(),
-            "kind": "port", "t_iter_s": t_iter,
+            "kind": "port", "t_iter_s": t_iter, "host": host_info(),
             "sample": f"{done} FP64 SP2 iteration(s) of the N={n} two-band alg2 loop (numpy/OpenBLAS "
                       f"DGEMM, {os.cpu_count()} threads), extrapolated to {iters_per_solve} iterations per solve"}
 
@@ -198,6 +219,7 @@ def subgraph_cpu_sample(rp, col, val, n, hp, hidx, lls, seq, maxiter, emin, emax
     el = time.perf_counter() - t0
     t_solve = el * total / done_w
     return {"value": 1.0 / t_solve, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+            "host": host_info(),
             "sample": f"{done} of {len(lls)} parts (prg_sp2_submatrix, {maxiter} steps, numpy/OpenBLAS "
                       f"DGEMM, {os.cpu_count()} threads), extrapolated by n^3 to the serial part loop"}
 
@@ -234,7 +256,7 @@ def run_reference(args, rank, world):
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": dense_config(args, n, world),
            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port",
-                            "sample": r["sample"]},
+                            "sample": r["sample"], "host": r["host"]},
            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
