@@ -2,8 +2,8 @@
 qmd-progress_b200/csrc/sp2b_common.cuh), compiled for the host and driven on a diagonal
 X, against the oracle (CPU, no GPU).
 
-* alg2 and alg2_genseq on a diagonal H: the same branch sequence and iteration count as
-  the oracle's `prg_sp2_alg2` / `prg_sp2_alg2_genseq`.
+* alg2, alg2_genseq, alg1, alg1_genseq (Rel and Abs) and basic on a diagonal H: the same
+  branch sequence and iteration count as the oracle's routines.
 * The mixed-precision rule with products short by a relative bias (the tensor cores'
   FP32 accumulation loses low-order bits toward zero; ~1e-4 of an element at
   N = 32768): the bias-corrected branch rule keeps the exact recursion's sequence and
@@ -47,13 +47,13 @@ def ctl(tmp_path_factory):
 
 
 def run(lib, algo, eig0, occ, bias=0.0, conv=CONV_NONE, maxit=100, idemtol=1e-10, mixed_tol=1e-3,
-        stag_tol=0.0, uncorrected=False):
+        stag_tol=0.0, uncorrected=False, minit=0):
     eig0 = np.ascontiguousarray(eig0, dtype=np.float64)
     n = len(eig0)
     pp = np.full(maxit + 2, -1, dtype=np.int32)
     it, nupd, st = C.c_int(0), C.c_int(0), C.c_int(0)
     out = np.zeros(n)
-    lib.ctl_run(algo, conv, 0, maxit, occ, idemtol, mixed_tol, stag_tol, n, eig0.ctypes.data, bias,
+    lib.ctl_run(algo, conv, minit, maxit, occ, idemtol, mixed_tol, stag_tol, n, eig0.ctypes.data, bias,
                 1 if uncorrected else 0, pp.ctypes.data, C.byref(it), C.byref(nupd), C.byref(st),
                 out.ctypes.data)
     return [int(b) for b in pp[:nupd.value]], it.value, st.value, out
@@ -125,3 +125,35 @@ def test_mixed_rule_keeps_occupation_on_dense_spectrum(ctl):
     _, _, _, xu = run(ctl, ALGO_MIXED, x0, occ, uncorrected=True, **kw)
     yu = 3 * xu ** 2 - 2 * xu ** 3
     assert abs(int(np.sum(yu > 0.5)) - nocc) >= 10
+
+
+ALGO_ALG1, ALGO_ALG1_GENSEQ, ALGO_BASIC = 2, 3, 4
+CONV_ABS = 2
+
+
+@pytest.mark.parametrize("seed", [0, 3, 5])
+@pytest.mark.parametrize("variant", ["alg1_rel", "alg1_genseq_rel", "alg1_genseq_abs", "basic"])
+def test_alg1_and_basic_rules_match_oracle(ctl, seed, variant):
+    """prg_sp2_alg1, prg_sp2_alg1_genseq (Rel and Abs) and prg_sp2_basic on a diagonal H:
+    the branch sequence and iteration count of the oracle."""
+    n = 64
+    e = spectrum(n, seed, gap=0.05 * (seed + 1))
+    h = np.diag(e)
+    emin, emax = O.gershgorin(h)
+    x0 = (emax - e) / (emax - emin)
+    occ = 0.5 * n
+    if variant == "basic":
+        ref = O.sp2_basic(h, 0.5, 10, 100, "Rel", 1e-10)
+        pp, it, st, _ = run(ctl, ALGO_BASIC, x0, occ, conv=CONV_REL, idemtol=1e-10,
+                            minit=10)
+    elif variant == "alg1_rel":
+        ref = O.sp2_alg1(h, 0.5, 0, 100, "Rel", 1e-10)
+        pp, it, st, _ = run(ctl, ALGO_ALG1, x0, occ, conv=CONV_REL)
+    else:
+        conv = "Rel" if variant.endswith("rel") else "Abs"
+        ref = O.sp2_alg1_genseq(h, 0.5, 0, 100, conv, 1e-10)
+        pp, it, st, _ = run(ctl, ALGO_ALG1_GENSEQ, x0, occ,
+                            conv=CONV_REL if conv == "Rel" else CONV_ABS)
+    assert st == 0
+    assert it == ref.iters
+    assert pp[:len(ref.pp)] == ref.pp
