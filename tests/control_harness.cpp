@@ -13,11 +13,12 @@ using namespace sp2b;
 
 extern "C" int ctl_run(int algo, int conv, int minit, int maxit, double occ, double idemtol,
                        double mixed_tol, double stag_tol, int n, const double* eig0, double bias,
-                       int uncorrected, int* pp_out, int* iters_out, int* nupd_out,
+                       int uncorrected, int icount, int* pp_out, int* iters_out, int* nupd_out,
                        int* status_out, double* eig_out) {
   SP2Ctl c;
   std::memset(&c, 0, sizeof(c));
   c.algo = algo;
+  c.icount = icount;
   c.conv = conv;
   c.minit = minit;
   c.maxit = maxit;

@@ -3,7 +3,8 @@ qmd-progress_b200/csrc/sp2b_common.cuh), compiled for the host and driven on a d
 X, against the oracle (CPU, no GPU).
 
 * alg2, alg2_genseq, alg1, alg1_genseq (Rel and Abs) and basic on a diagonal H: the same
-  branch sequence and iteration count as the oracle's routines.
+  branch sequence and iteration count as the oracle's routines; SP2-Fermi's generating
+  pass: the oracle's sgnlist.
 * The mixed-precision rule with products short by a relative bias (the tensor cores'
   FP32 accumulation loses low-order bits toward zero; ~1e-4 of an element at
   N = 32768): the bias-corrected branch rule keeps the exact recursion's sequence and
@@ -41,21 +42,21 @@ def ctl(tmp_path_factory):
     lib = C.CDLL(out)
     lib.ctl_run.restype = C.c_int
     lib.ctl_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                            C.c_double, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
-                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+                            C.c_double, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     return lib
 
 
 def run(lib, algo, eig0, occ, bias=0.0, conv=CONV_NONE, maxit=100, idemtol=1e-10, mixed_tol=1e-3,
-        stag_tol=0.0, uncorrected=False, minit=0):
+        stag_tol=0.0, uncorrected=False, minit=0, icount=0):
     eig0 = np.ascontiguousarray(eig0, dtype=np.float64)
     n = len(eig0)
     pp = np.full(maxit + 2, -1, dtype=np.int32)
     it, nupd, st = C.c_int(0), C.c_int(0), C.c_int(0)
     out = np.zeros(n)
     lib.ctl_run(algo, conv, minit, maxit, occ, idemtol, mixed_tol, stag_tol, n, eig0.ctypes.data, bias,
-                1 if uncorrected else 0, pp.ctypes.data, C.byref(it), C.byref(nupd), C.byref(st),
-                out.ctypes.data)
+                1 if uncorrected else 0, icount, pp.ctypes.data, C.byref(it), C.byref(nupd),
+                C.byref(st), out.ctypes.data)
     return [int(b) for b in pp[:nupd.value]], it.value, st.value, out
 
 
@@ -157,3 +158,24 @@ def test_alg1_and_basic_rules_match_oracle(ctl, seed, variant):
     assert st == 0
     assert it == ref.iters
     assert pp[:len(ref.pp)] == ref.pp
+
+
+ALGO_FERMI_GEN = 8
+
+
+@pytest.mark.parametrize("seed,nsteps", [(0, 12), (2, 20), (4, 16)])
+def test_fermi_generation_rule_matches_oracle(ctl, seed, nsteps):
+    """The first pass of prg_sp2_fermi_init (the device rule ALGO_FERMI_GEN) on a diagonal
+    H from X0 = ((hN - mu) I - H)/(hN - h1) at the starting mu: the oracle's sgnlist, and
+    exactly nsteps updates."""
+    n = 64
+    e = spectrum(n, seed, gap=0.1)
+    h = np.diag(e)
+    nocc = 0.5 * n
+    _, _, _, h1, hN, sgn_ref = O.sp2_fermi_init(h, nsteps, nocc, 1.0, 1e-9, 1e-12)
+    gmin, gmax = O.gershgorin(h)
+    mu0 = 0.5 * (gmax + gmin)
+    x0 = np.diag(O.normalize_fermi(h, h1, hN, mu0))
+    pp, it, st, _ = run(ctl, ALGO_FERMI_GEN, x0, nocc, maxit=nsteps + 1, icount=nsteps)
+    assert st == 0 and len(pp) == nsteps and it == nsteps
+    assert [1 if b == 0 else -1 for b in pp] == list(sgn_ref)
