@@ -268,3 +268,32 @@ def test_host_path_reads_one_triangle(cuda):
     g[np.tril_indices(n, -1)] = 1e3
     got = sp2b.sp2_alg2(g, 0.5, 0, 100, "None", 1e-10)
     assert np.array_equal(got.rho, ref.rho)
+
+
+@pytest.mark.parametrize("case", ["alg1_seq", "alg2_seq", "alg1_seq_inplace", "alg2_seq_inplace"])
+def test_poly512_sequence_cases_of_the_reference_suite(cuda, poly512, case):
+    """The reference suite's sequence cases on poly.512.mtx (tests/src/main.F90:496-738):
+    genseq with minsp2iter 25, "Rel", idemtol 1e-10, then the *_seq or *_seq_inplace
+    replay (the in-place cases with the Gershgorin bounds of H and the alg2 sequence, as
+    the reference's in-place cases do), accepted at idempotency of rho/2 <= 1e-6.  The
+    replay follows the generating solve's branches from the same bounds, so it also
+    equals that solve's density (1e-10; 1e-9 for alg1's update replaying alg2's
+    sequence)."""
+    h = poly512["h"]
+    tol = FP64_TOL
+    if case == "alg1_seq":
+        g = sp2b.sp2_alg1_genseq(h, 0.5, 25, 100, "Rel", 1e-10)
+        r = sp2b.sp2_alg1_seq(h, g.pp, g.icount)
+    elif case == "alg2_seq":
+        g = sp2b.sp2_alg2_genseq(h, 0.5, 25, 100, "Rel", 1e-10)
+        r = sp2b.sp2_alg2_seq(h, g.pp, g.icount)
+    else:
+        g = sp2b.sp2_alg2_genseq(h, 0.5, 25, 100, "Rel", 1e-10)
+        lo, hi = sp2b.gershgorin(h)
+        if case == "alg1_seq_inplace":
+            r = sp2b.sp2_alg1_seq_inplace(h, g.pp, g.icount, lo, hi)
+            tol = 1e-9
+        else:
+            r = sp2b.sp2_alg2_seq_inplace(h, g.pp, g.icount, lo, hi)
+    assert sp2b.check_idempotency(r.rho / 2) <= 1e-6
+    assert rel(r.rho, g.rho) <= tol
