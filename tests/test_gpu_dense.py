@@ -299,13 +299,15 @@ def test_poly512_sequence_cases_of_the_reference_suite(cuda, poly512, case):
     assert rel(r.rho, g.rho) <= tol
 
 
-@pytest.mark.parametrize("alg", ["alg1", "alg2"])
+@pytest.mark.parametrize("alg", ["alg1", "alg2", "basic"])
 def test_poly512_plain_cases_of_the_reference_suite(cuda, poly512, alg):
     """prg_sp2_alg1_ellpack / prg_sp2_alg2_ellpack of the reference suite
     (tests/src/main.F90:336-395): alg1 / alg2 on poly.512.mtx with minsp2iter 25, "Rel",
-    idemtol 1e-10, accepted at idempotency of rho/2 <= 1e-6; Tr rho = N_occ * 2 to 1e-8."""
+    idemtol 1e-10, accepted at idempotency of rho/2 <= 1e-6; Tr rho = N_occ * 2 to 1e-8.
+    prg_sp2_basic (its suite case, :260-280, reads a file the reference does not ship)
+    under the same settings and criterion."""
     h = poly512["h"]
-    fn = sp2b.sp2_alg1 if alg == "alg1" else sp2b.sp2_alg2
+    fn = {"alg1": sp2b.sp2_alg1, "alg2": sp2b.sp2_alg2, "basic": sp2b.sp2_basic}[alg]
     r = fn(h, 0.5, 25, 100, "Rel", 1e-10)
     assert sp2b.check_idempotency(r.rho / 2) <= 1e-6
     assert abs(np.trace(r.rho) - h.shape[0]) <= 1e-8 * h.shape[0]
