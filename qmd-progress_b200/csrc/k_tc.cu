@@ -1350,8 +1350,7 @@ static int pair_clusters() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return num_sms() / 2;
   if (per_dev[dev] > 0) return per_dev[dev];
-  cudaLaunchConfig_t cfg;
-  memset(&cfg, 0, sizeof(cfg));
+  cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(num_sms() & ~1, 1, 1);
   cfg.blockDim = dim3(tcp::NTHR, 1, 1);
   cfg.dynamicSmemBytes = tcq::SMEM_BYTES;

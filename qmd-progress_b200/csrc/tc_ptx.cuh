@@ -287,7 +287,7 @@ static bool make_tmap_box(CUtensorMap* tm, const void* base, long long rows, lon
   return r == CUDA_SUCCESS;
 }
 // 16-bit operand map with the 64 x 128 box of the split-precision kernels.
-static bool make_tmap(CUtensorMap* tm, const void* base, long long rows, long long cols,
+inline bool make_tmap(CUtensorMap* tm, const void* base, long long rows, long long cols,
                       long long ld, bool bf16) {
   return make_tmap_box(tm, base, rows, cols, ld, bf16 ? TMAP_BF16 : TMAP_F16, 128);
 }
