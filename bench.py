@@ -64,6 +64,11 @@ def parse():
                          "cubic_dense: the 32^3 lattice solved densely (N=32768)")
     ap.add_argument("--L", type=int, default=32, help="subgraph: lattice edge")
     ap.add_argument("--parts", type=int, default=256, help="subgraph: number of parts")
+    ap.add_argument("--subgraph-precision", default="mixed_fp16",
+                    choices=["mixed_fp16", "mixed_bf16", "exact_int8", "fp64"],
+                    help="precision of the sub-graph solve nested in the default line")
+    ap.add_argument("--no-subgraph", action="store_true",
+                    help="default workload: leave out the nested sub-graph measurement")
     return ap.parse_args()
 
 
@@ -77,59 +82,121 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed regions."""
+    """SM clocks and clock-event (throttle) reasons of the bench's GPU, read through NVML
+    every 5 ms on a host thread (queries only; no setting is touched).  The bench marks
+    its timed regions with begin()/end(); summary() reports the samples taken inside
+    them, so even a timed region of a few tens of milliseconds gets several samples.
+    Falls back to nvidia-smi at 100 ms when NVML is not available."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
+        self.samples = []          # (t, sm_mhz, max_mhz, reasons set)
+        self.windows = []
+        self._open = None
+        self._stop = threading.Event()
         self.proc = None
-        self.lines = []
+        self.thread = None
+        self.source = None
+
+    def _nvml_handle(self, nv):
+        import torch
+        try:
+            u = str(torch.cuda.get_device_properties(self.index).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            pass
+        try:
+            p = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    except Exception:
+                        break
+                    self.samples.append((time.perf_counter(), sm, mx,
+                                         {k for k, b in bits.items() if r & b}))
+                    self._stop.wait(0.005)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            self.source = "nvml 5 ms"
+        except Exception:
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._read_smi, daemon=True)
+                self.thread.start()
+                self.source = "nvidia-smi 100 ms"
+            except OSError:
+                self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            f = [x.strip() for x in line.strip().split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm, mx = float(f[1]), float(f[2])
+            except ValueError:
+                continue
+            self.samples.append((time.perf_counter(), sm, mx,
+                                 {nm for nm, v in zip(self.NAMES, f[5:9]) if v.lower().startswith("active")}))
+
+    def begin(self):
+        self._open = time.perf_counter()
+
+    def end(self):
+        if self._open is not None:
+            self.windows.append((self._open, time.perf_counter()))
+            self._open = None
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        win = self.windows or ([(self.samples[0][0], self.samples[-1][0])] if self.samples else [])
+        inside = [s for s in self.samples if any(a <= s[0] <= b for a, b in win)]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": self.source}
+        reasons = set()
+        for s in inside:
+            reasons |= s[3]
+        return {"sm_mhz": statistics.median(s[1] for s in inside), "sm_max_mhz": inside[-1][2],
+                "sm_min_mhz": min(s[1] for s in inside), "reasons": sorted(reasons),
+                "samples": len(inside), "timed_s": round(sum(b - a for a, b in win), 3),
+                "source": self.source}
 
 
 def host_info():
@@ -228,19 +295,43 @@ def dense_metric(n):
     return "SP2 solves/s (dense two-band N=%d)" % n
 
 
+L2_BYTES = 126e6
+
+
 def dense_config(args, n, world):
     """The dense workload's config, the same on both arms (the reference arm times the
     same solve H -> D on the host cores)."""
+    mib = n * n * 8 / 2 ** 20
+    l2 = (f"inputs {mib:.0f} MiB > L2 (126 MB), no flush" if n * n * 8 > 2 * L2_BYTES else
+          f"inputs {mib:.1f} MiB fit in L2: 256 MiB written between timed solves, each solve timed alone")
     return {"workload": f"two_band_1d_n{n}_{args.precision}_alg2_mcweeny1", "n": n,
             "bndfil": 0.5, "idemtol": 1e-10, "seed": "rank r solves seed r",
-            "parallelism": f"replicas{world}", "l2": "inputs 512 MiB > L2, no flush"}
+            "parallelism": f"replicas{world}", "l2": l2}
+
+
+def oracle_solve(n, seed=0):
+    """One complete FP64 alg2 genseq solve of the workload by the oracle (None stop rule,
+    idemtol 1e-10, at most 100 iterations) on the host cores: the iteration count every CPU
+    figure extrapolates by, and a check of its output (Tr D = N)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+    import sp2_oracle as O
+    from sp2b import modelham as M
+    h = M.two_band_1d(n, seed=seed)
+    t0 = time.perf_counter()
+    r = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    el = time.perf_counter() - t0
+    tr = float(np.trace(r.rho))
+    if not abs(tr - n) <= 1e-6 * n:
+        raise RuntimeError(f"oracle solve of the bench workload: Tr D = {tr} != {n}")
+    return r.icount, el
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     n = args.n
-    iters = 12  # alg2 iterations of this workload (FP64 genseq, seed 0, any N >= 1024 of the model)
+    iters, full_s = oracle_solve(n)   # untimed: the workload's FP64 iteration count
     vals = []
     for _ in range(args.warmup):
         cpu_baseline_sample(min(n, 2048), 1, 5.0)
@@ -256,9 +347,18 @@ def run_reference(args, rank, world):
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": dense_config(args, n, world),
            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["cores"], "kind": "port",
-                            "sample": r["sample"], "host": r["host"]},
+                            "sample": r["sample"], "host": r["host"], "sp2_iters": iters,
+                            "full_solve_s": full_s},
            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def roofline_peak(peaks, clocks):
+    """The bf16 denominator for a kernel timed inside this run: the burst figure unless the
+    clocks of the timed region show the power cap, then the sustained one."""
+    capped = "sw_power_cap" in (clocks.get("reasons") or [])
+    key = "bf16_tflops_sustained" if capped and "bf16_tflops_sustained" in peaks else "bf16_tflops"
+    return key, peaks[key]
 
 
 def main():
@@ -275,7 +375,6 @@ def main():
 
     import numpy as np
     import torch
-    import sp2b
     from sp2b import _lib, modelham as M
 
     torch.cuda.set_device(local)
@@ -296,6 +395,9 @@ def main():
     pp = np.zeros(128, dtype=np.int32)
     vv = np.zeros(128)
     ic = C.c_int(0)
+    # inputs that fit in L2 get it flushed between timed solves (each solve timed alone)
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device="cuda") \
+        if n * n * 8 <= 2 * L2_BYTES else None
 
     def solve_dev(precision):
         o = _lib.make_opts(precision=precision, device_ptrs=True, stream=stream.cuda_stream)
@@ -317,19 +419,39 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    def timed_ms(fn, reps):
+        """Device time of reps calls on the launch stream: one event pair around all of
+        them, or, when L2 is flushed between calls, one pair per call (summed)."""
+        if flush is None:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1), out
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot, out
+
+    clk = ClockSampler(local).__enter__()
     # ---- warm-up ----
     for _ in range(args.warmup):
         iters = solve_dev(prec)
     # ---- timed region: device-resident ----
     L.sp2b_set_step_timing(1)
     launches0 = L.sp2b_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
-    clk = ClockSampler(local).__enter__()   # covers every timed region below
-    ev0.record(stream)
-    for _ in range(args.steps):
-        iters = solve_dev(prec)
-    ev1.record(stream)
+    clk.begin()
+    t_ms, iters = timed_ms(lambda: solve_dev(prec), args.steps)
+    clk.end()
     barrier()
     launches = L.sp2b_launch_count() - launches0
     step_ms = C.c_double(0)
@@ -339,7 +461,7 @@ def main():
     ref_n = C.c_longlong(0)
     L.sp2b_refinement_timing(ref_ms, C.byref(ref_n))
     L.sp2b_set_step_timing(0)
-    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    t_ms = max_over_ranks(t_ms)
     value = world * args.steps / (t_ms / 1e3)
 
     # ---- end to end through the C ABI with host buffers ----
@@ -355,13 +477,11 @@ def main():
                                               C.byref(o)), "sp2_alg2_genseq(host)")
         solve_host()
         barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            solve_host()
-        e1.record(stream)
+        clk.begin()
+        te, _ = timed_ms(solve_host, args.steps)
+        clk.end()
         barrier()
-        te = max_over_ranks(e0.elapsed_time(e1))
+        te = max_over_ranks(te)
         # H crosses as its upper triangle (one 2D copy per 128-row panel, the library
         # rebuilds the rest on the device); D comes back whole, with pp and vv
         h2d = sum((n - r0) * min(128, n - r0) * 8 for r0 in range(0, n, 128))
@@ -370,20 +490,20 @@ def main():
 
     # ---- FP64 (parity form) beside it ----
     fp64 = None
+    it64 = iters if prec == _lib.PREC_FP64 else None
     rho_mixed = rho_dev.clone() if prec != _lib.PREC_FP64 else None
     if prec != _lib.PREC_FP64 and args.fp64_steps > 0:
         solve_dev(_lib.PREC_FP64)
         barrier()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.fp64_steps):
-            it64 = solve_dev(_lib.PREC_FP64)
-        f1.record(stream)
+        clk.begin()
+        tf, it64 = timed_ms(lambda: solve_dev(_lib.PREC_FP64), args.fp64_steps)
+        clk.end()
         barrier()
-        tf = max_over_ranks(f0.elapsed_time(f1))
+        tf = max_over_ranks(tf)
         fp64 = {"solves_per_s": world * args.fp64_steps / (tf / 1e3), "iters": it64,
                 "ms_per_solve": tf / args.fp64_steps,
-                "tflops": world * args.fp64_steps * 2.0 * n ** 3 * it64 / (tf / 1e3) / 1e12}
+                "tflops": world * args.fp64_steps * 2.0 * n ** 3 * it64 / (tf / 1e3) / 1e12,
+                "kernel": "k_sym_gemm_f64 (FP64 DMMA SP2 step)"}
         # accuracy of the mixed solve against the FP64 one (same H): ||dD||_F / N
         dd = float((rho_mixed - rho_dev).norm().item())
         fp64["mixed_err_fro_over_n"] = dd / n
@@ -397,8 +517,16 @@ def main():
     step_avg_ms = step_ms.value / max(step_n.value, 1)
     flops_launch = 2.0 * n ** 3          # one N x N x N product per SP2 step (algorithmic)
     achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
-    peak_key = "bf16_tflops_sustained" if "bf16_tflops_sustained" in peaks else "bf16_tflops"
-    peak = peaks[peak_key] if prec != _lib.PREC_FP64 else None
+    npad = -(-n // 128) * 128
+    nb = npad // 128
+    if prec != _lib.PREC_FP64:
+        peak_key, peak = roofline_peak(peaks, clocks)
+        kernel = "k_tc_pair (SP2 step, CTA pairs)" if npad % 256 == 0 else "k_tc_persist (SP2 step)"
+        if prec == _lib.PREC_EXACT_INT8:
+            kernel = "k_oz_gemm (exact INT8 SP2 step: 9 residue products)"
+    else:
+        peak_key, peak = None, None
+        kernel = "k_sym_gemm_f64 (FP64 DMMA SP2 step)"
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -409,15 +537,15 @@ def main():
             traffic = ent.get("bytes_per_launch")
     # executed tensor work: upper 128 x 128 tiles (incl. the diagonal), three 16-bit
     # products each (hi*hi, hi*lo, lo*hi) over the padded K
-    npad = -(-n // 128) * 128
-    nb = npad // 128
-    exec_flops = 3 * 2.0 * 128 * 128 * npad * (nb * (nb + 1) // 2) if prec != _lib.PREC_FP64 else None
+    exec_flops = 3 * 2.0 * 128 * 128 * npad * (nb * (nb + 1) // 2) \
+        if prec in (_lib.PREC_MIXED_FP16, _lib.PREC_MIXED_BF16) else None
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if peak else None, "traffic": traffic,
-                "peak_source": f"{src} {peak_key}",
-                "kernel": "k_tc_pair (SP2 step, CTA pairs)" if npad % 256 == 0 else "k_tc_persist (SP2 step)",
-                "avg_launch_ms": step_avg_ms, "launches_timed": step_n.value,
+                "peak_source": f"{src} {peak_key}" if peak_key else "no bf16 denominator for FP64",
+                "kernel": kernel, "avg_launch_ms": step_avg_ms, "launches_timed": step_n.value,
                 "flops_per_launch": flops_launch,
+                "frac_of_sustained": (achieved / peaks["bf16_tflops_sustained"])
+                if peak and "bf16_tflops_sustained" in peaks else None,
                 "executed_tflops": (exec_flops / (step_avg_ms / 1e3) / 1e12) if exec_flops else None,
                 "executed_frac": (exec_flops / (step_avg_ms / 1e3) / 1e12 / peak) if exec_flops and peak else None}
     refinement = None
@@ -435,7 +563,15 @@ def main():
                       "int8_frac_of_nominal": int8_ops / (per[1] / 1e3) / 1e12 / 4500.0}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline_sample(n, iters, max_seconds=20.0)
+        if it64 is None:
+            it64, _ = oracle_solve(n)
+        cpu = cpu_baseline_sample(n, it64, max_seconds=20.0)
+        cpu["sp2_iters"] = it64
+    sub = None
+    if args.workload == "two_band" and not args.no_subgraph:
+        del h_dev, rho_dev, rho_mixed
+        torch.cuda.empty_cache()
+        sub = measure_subgraph(args, rank, world, local, dist)
     if rank == 0:
         out = {"metric": dense_metric(n), "value": value,
                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -448,7 +584,7 @@ def main():
                "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
                "fp64": fp64, "e2e": e2e, "roofline": roofline, "refinement": refinement,
                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-               "tuning": _tuning()}
+               "tuning": _tuning(), "subgraph": sub}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -456,6 +592,24 @@ def main():
 
 
 def run_subgraph(args, rank, world, local):
+    """bench.py --workload subgraph: the batched sub-graph measurement as its own line."""
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    out = measure_subgraph(args, rank, world, local, dist, args.precision)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_subgraph(args, rank, world, local, dist, precision):
     """Batched graph-partitioned SP2 (prg_subgraphSP2Loop) on the L^3 cubic lattice.
 
     Setup (untimed), as the reference's sub-graph test does
@@ -471,13 +625,6 @@ def run_subgraph(args, rank, world, local):
     import torch
     import sp2b
     from sp2b import _lib, graph as G, modelham as M
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
     L = args.L
     n = L ** 3
     Lb = _lib.lib()
@@ -555,20 +702,24 @@ def run_subgraph(args, rank, world, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    flush = torch.empty(64 * 2 ** 20, dtype=torch.float32, device="cuda")
+
     def timed(prec, steps):
-        for _ in range(args.warmup):
-            solve(prec)
+        """Device time of `steps` solves: the inputs (CSR H, 13 MB) fit in L2, so 256 MiB
+        are written between solves and each solve is timed alone (summed)."""
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = Lb.sp2b_launch_count()
-        e0.record(stream)
+        t = 0.0
         for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             solve(prec)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        t = e0.elapsed_time(e1)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t += e0.elapsed_time(e1)
         if dist:
             tt = torch.tensor([t], device="cuda", dtype=torch.float64)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -576,9 +727,14 @@ def run_subgraph(args, rank, world, local):
         return t, Lb.sp2b_launch_count() - l0
 
     prec = {"mixed_fp16": _lib.PREC_MIXED_FP16, "mixed_bf16": _lib.PREC_MIXED_BF16,
-            "exact_int8": _lib.PREC_EXACT_INT8, "fp64": _lib.PREC_FP64}[args.precision]
-    with ClockSampler(local) as clk:
-        t_ms, launches = timed(prec, args.steps)
+            "exact_int8": _lib.PREC_EXACT_INT8, "fp64": _lib.PREC_FP64}[precision]
+    clk = ClockSampler(local).__enter__()
+    for _ in range(args.warmup):
+        solve(prec)
+    torch.cuda.synchronize()
+    clk.begin()
+    t_ms, launches = timed(prec, args.steps)
+    clk.end()
     core_mixed = core_d.clone()
     nref = C.c_int(0)
     Lb.sp2b_last_subgraph_refined(C.byref(nref), None, 0, None, 0)
@@ -594,18 +750,19 @@ def run_subgraph(args, rank, world, local):
     step_avg_ms = max(t_steps - t_none, 1e-6) / max(maxiter, 1)
     flops_launch = 2.0 * float(np.sum(ls.astype(np.float64) ** 3))
     peaks, psrc = load_peaks()
-    peak_key = "bf16_tflops_sustained" if "bf16_tflops_sustained" in peaks else "bf16_tflops"
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            ent = json.load(f).get(f"sp2_step_batched_{args.precision}_cubic20_64parts")
+            ent = json.load(f).get(f"sp2_step_batched_{precision}_cubic20_64parts")
         if ent:
             # captured on the 20^3 / 64-part case; DRAM bytes scale with the tiles' work
             traffic = ent["bytes_per_launch"] * flops_launch / ent["flops_per_launch"]
     achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
-                "frac": achieved / peaks[peak_key], "traffic": traffic,
+    peak_key, peak = roofline_peak(peaks, clk.summary())
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "frac_of_sustained": achieved / peaks.get("bf16_tflops_sustained", peak),
                 "peak_source": f"{psrc} {peak_key}",
                 "kernel": "k_tc_persist<T,0,1> (batched SP2 step, all parts)",
                 "avg_launch_ms": step_avg_ms, "flops_per_launch": flops_launch,
@@ -630,7 +787,9 @@ def run_subgraph(args, rank, world, local):
                                                  emax, core_h.data_ptr(), None, vvo.ctypes.data,
                                                  C.byref(oh)), "subgraph_sp2_loop(host)")
         solve_host()
+        clk.begin()
         te = events_ms(solve_host, args.steps)
+        clk.end()
         # H (CSR) and pp in; the core rows and vv out, every call
         h2d = rp.nbytes + col.nbytes + val.nbytes + seq_a.nbytes
         e2e = {"value": world / (te / 1e3), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
@@ -640,7 +799,12 @@ def run_subgraph(args, rank, world, local):
     if rank == 0 and not args.no_cpu:
         cpu = subgraph_cpu_sample(rp, col, val, n, hp, hidx, lls, seq, maxiter, emin, emax)
 
+    for _ in range(args.warmup):
+        solve(_lib.PREC_FP64)
+    clk.begin()
     t64, _ = timed(_lib.PREC_FP64, max(1, args.fp64_steps))
+    clk.end()
+    clk.__exit__(None, None, None)
     err_vs_fp64 = float((core_mixed - core_d).norm().item()) / n
     rel_vs_fp64 = float((core_mixed - core_d).norm().item() / core_d.norm().item())
     flops = 2.0 * float(np.sum(ls.astype(np.float64) ** 3)) * maxiter
@@ -649,14 +813,15 @@ def run_subgraph(args, rank, world, local):
         out = {"metric": "sub-graph SP2 solves/s (32^3 lattice, 256 parts, batched)", "value": value,
                "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-               "config": {"workload": f"cubic{L}_subgraph_{len(parts)}parts_{args.precision}",
+               "vs_baseline": None, "dtype": precision, "data": "synthetic",
+               "config": {"workload": f"cubic{L}_subgraph_{len(parts)}parts_{precision}",
                           "n": n, "parts": len(parts), "lsize_min": int(ls.min()),
                           "lsize_max": int(ls.max()), "lsize_mean": float(ls.mean()),
                           "maxiter": maxiter, "full_genseq_iters": full_iters,
                           "homo": eh, "lumo": el, "sequence": seq_source,
                           "graph": "|H^2| > 0.6", "halo": "one jump",
                           "partition": "RCB U[0.4,0.6]", "setup_s": setup_s,
+                          "l2": "CSR H 13 MB fits in L2: 256 MiB written between timed solves",
                           "graph_s": graph_s,
                           "parts_resolved_fp64": nref.value},
                "tflops": value * flops / 1e12, "flops_per_solve": flops,
@@ -665,10 +830,8 @@ def run_subgraph(args, rank, world, local):
                "err_vs_fp64": {"fro_over_n": err_vs_fp64, "rel_fro": rel_vs_fp64},
                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
                "clocks": clk.summary(), "gpu_launches": launches, "tuning": _tuning()}
-        print(json.dumps(out), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+        return out
+    return None
 
 
 def run_cubic_dense(args, rank, local):

@@ -131,15 +131,17 @@ int sp2b_sp2_submatrix_inplace(double* rho, int n, double threshold, const int* 
                                const sp2b_opts* opts);
 
 /* No counterpart in the reference.  The same SP2 on one core+halo block as
- * sp2b_sp2_submatrix_inplace, for callers that cannot allocate GPU memory when they
- * call it: code running inside an open CUDA stream capture (where cudaMalloc is not
- * allowed) or an application whose device memory is reserved by its own pool.  It
- * calls no cudaMalloc / cudaFree / allocating library routine: its working buffers
- * live in one fixed device array (about 4.2 MB, held by every GPU that loads the
- * library until exit).  x_dev is a DEVICE pointer to the n x n block (H in, rho out);
- * pp and vv (accumulated, as in the reference) are host arrays; work runs on `stream`.
- * Limits: n <= 512 and icount <= 100, otherwise SP2B_BAD_ARG.  All calls share the one
- * array, so calls whose GPU work overlaps race; the first call on a device looks up
+ * sp2b_sp2_submatrix_inplace, for callers that must not allocate GPU memory when they
+ * call it: typically a simulation code that reserves its device memory up front in its
+ * own pool allocator (a library cudaMalloc would fail or break the pool's accounting),
+ * or a time-step loop that may not stall on cudaMalloc / cudaFree, which synchronise
+ * the device.  It calls no cudaMalloc / cudaFree / allocating library routine: its
+ * working buffers live in one fixed device array (about 4.2 MB, held by every GPU that
+ * loads the library until exit).  x_dev is a DEVICE pointer to the n x n block (H in,
+ * rho out); pp and vv (accumulated, as in the reference; untouched when core_size is 0)
+ * are host arrays; work runs on `stream`.  Limits: n <= 512 and icount <= 100,
+ * otherwise SP2B_BAD_ARG.  All calls share the one array and it keeps the last call's
+ * contents, so calls whose GPU work overlaps race; the first call on a device looks up
  * the array's address and should come before any stream capture. */
 int sp2b_sp2_submatrix_inplace_noalloc(double* x_dev, int n, const int* pp, int icount,
                                        double* vv, double mineval, double maxeval, int core_size,

@@ -419,6 +419,12 @@ int dense_solve(const DenseJob& j) {
     set_last_error("non-finite or degenerate spectral bounds (%g, %g)", emin, emax);
     return SP2B_BAD_INPUT;
   }
+  // ||X0||_F^2 of the normalised input: a NaN / Inf in H shows here even when no SP2
+  // step runs (icount = 0) to flag it
+  if (!(c->h_small[11] == c->h_small[11]) || c->h_small[11] > 1e300) {
+    set_last_error("non-finite values in the input matrix");
+    return SP2B_BAD_INPUT;
+  }
   if (!done && maxlaunch > 0) {
     set_last_error("SP2 loop ended without a final state");
     return SP2B_CUDA_ERROR;
@@ -772,8 +778,10 @@ int sp2b_sp2_submatrix_inplace(double* rho, int n, double threshold, const int* 
     set_last_error("bad argument: core_size=%d n=%d", core_size, n);
     return SP2B_BAD_ARG;
   }
-  return seq_job(nullptr, rho, n, pp, icount, vv, true, mineval, maxeval,
-                 core_size > 0 ? core_size : -1, 1, opts);
+  // core_size = 0: bml_sum_squares_submatrix over no rows adds nothing, so vv is left
+  // as the caller passed it
+  return seq_job(nullptr, rho, n, pp, icount, core_size > 0 ? vv : nullptr, true, mineval,
+                 maxeval, core_size > 0 ? core_size : -1, 1, opts);
 }
 
 int sp2b_sp2_submatrix(const double* ham, double* rho, int n, double threshold, const int* pp,
@@ -788,7 +796,7 @@ int sp2b_sp2_submatrix(const double* ham, double* rho, int n, double threshold, 
   j.ctl.algo = ALGO_SEQ;
   j.ctl.icount = icount;
   j.pp_in = pp;
-  j.vv_out = vv;
+  j.vv_out = core_size > 0 ? vv : nullptr;   // no core rows: vv gains nothing
   j.given_bounds = true;
   j.mineval = mineval;
   j.maxeval = maxeval;

@@ -1,12 +1,13 @@
 // SP2 on one core+halo block without any memory allocation.
 //
-// Who needs this: code that cannot call cudaMalloc at the moment it wants a density
-// block.  Two common cases: a solver step that runs while the caller holds an open
-// CUDA stream capture (cudaMalloc is not allowed inside a capture), and an
-// application whose GPU memory is claimed up front by its own pool allocator, where a
-// library allocation would fail or break the pool's accounting.  Such callers pass
-// their own device block (in/out) and host pp/vv; every working buffer this entry
-// needs lives in the fixed device array below.
+// Who needs this: code that must not call cudaMalloc (or any allocator) at the moment
+// it wants a density block.  The usual case is a simulation code that claims its GPU
+// memory up front through its own pool allocator and hands slices of it to the
+// libraries it calls: a library allocation there either fails because the pool holds
+// the memory, or breaks the pool's accounting.  Another is a time-step loop that may
+// not stall on cudaMalloc / cudaFree, which synchronise the device.  Such callers pass
+// their own device block (in/out) and host pp/vv; every working buffer this entry needs
+// lives in the fixed device array below.
 //
 // Limits and sharing:
 //  * block size n <= kNoAllocMaxN (512) and icount <= kNoAllocMaxIter (100, the size of
@@ -126,7 +127,8 @@ extern "C" int sp2b_sp2_submatrix_inplace_noalloc(double* x_dev, int n, const in
   SP2B_CUDA_TRY(cudaMemcpyAsync(small, bounds, sizeof(bounds), cudaMemcpyHostToDevice, st));
   if (icount > 0) {
     SP2B_CUDA_TRY(cudaMemcpyAsync(pp_d, pp, icount * sizeof(int), cudaMemcpyHostToDevice, st));
-    SP2B_CUDA_TRY(cudaMemcpyAsync(vv_d, vv, icount * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (core_size > 0)
+      SP2B_CUDA_TRY(cudaMemcpyAsync(vv_d, vv, icount * sizeof(double), cudaMemcpyHostToDevice, st));
   }
   // X0 = (maxeval I - x)/(maxeval - mineval) into the padded scratch block
   SP2B_CUDA_TRY(launch_normalize_f64(x_dev, n, n, np, small, x[0], partials, counter, rec,
@@ -141,7 +143,7 @@ extern "C" int sp2b_sp2_submatrix_inplace_noalloc(double* x_dev, int n, const in
   a.ctl.n = n;
   a.rec = rec;
   a.pp_in = pp_d;
-  a.vv_out = vv_d;
+  a.vv_out = core_size > 0 ? vv_d : nullptr;   // no core rows: vv gains nothing
   a.vv_accumulate = 1;
   a.core = core_size > 0 ? core_size : -1;
   a.sout = sout;
@@ -157,11 +159,19 @@ extern "C" int sp2b_sp2_submatrix_inplace_noalloc(double* x_dev, int n, const in
   SP2B_CUDA_TRY(launch_finish_f64(x[icount & 1], np, n, 2.0, x_dev, n, st));
   SolveOut so;
   memset(&so, 0, sizeof(so));
-  if (icount > 0) {
+  double norm[4] = {0.0, 0.0, 0.0, 0.0};
+  if (icount > 0 && core_size > 0)
     SP2B_CUDA_TRY(cudaMemcpyAsync(vv, vv_d, icount * sizeof(double), cudaMemcpyDeviceToHost, st));
-    SP2B_CUDA_TRY(cudaMemcpyAsync(&so, sout, sizeof(SolveOut), cudaMemcpyDeviceToHost, st));
-  }
+  SP2B_CUDA_TRY(cudaMemcpyAsync(&so, sout, sizeof(SolveOut), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(norm, small + 4, sizeof(norm), cudaMemcpyDeviceToHost, st));
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  // the same checks as the regular entry: bounds as used, and ||X0||_F^2 of the
+  // normalised block, which shows a NaN / Inf input even when no step runs
+  if (!(norm[1] - norm[0] > 0.0) || !(norm[3] == norm[3]) || norm[3] > 1e300) {
+    set_last_error("non-finite values in the input block or degenerate bounds (%g, %g)",
+                   norm[0], norm[1]);
+    return SP2B_BAD_INPUT;
+  }
   if (so.status != SP2B_OK) {
     set_last_error("non-finite values during SP2");
     return so.status;

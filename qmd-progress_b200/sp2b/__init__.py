@@ -316,8 +316,18 @@ def sp2_submatrix_inplace(x, pp, icount, vv, mineval, maxeval, core_size):
 
 
 def sp2_submatrix(ham, pp, icount, vv, mineval, maxeval, core_size):
-    """prg_sp2_submatrix (src/prg_sp2_mod.F90:1190-1246)."""
-    return sp2_submatrix_inplace(ham, pp, icount, vv, mineval, maxeval, core_size)
+    """prg_sp2_submatrix (src/prg_sp2_mod.F90:1190-1246): rho from a separate input block
+    (sp2b_sp2_submatrix); vv is accumulated in place."""
+    h = _f64(ham)
+    n = h.shape[0]
+    rho = np.empty_like(h)
+    pp_a = np.ascontiguousarray(pp, dtype=np.int32)
+    if not (isinstance(vv, np.ndarray) and vv.dtype == np.float64 and vv.flags.c_contiguous):
+        raise TypeError("vv must be a contiguous float64 numpy array (accumulated in place)")
+    o = _opts(PREC_FP64, 1, 1e-3)
+    check(lib().sp2b_sp2_submatrix(_ptr(h), _ptr(rho), n, 0.0, _ptr(pp_a), icount, _ptr(vv),
+                                   mineval, maxeval, core_size, C.byref(o)), "sp2_submatrix")
+    return rho
 
 
 def gershgorin(h):

@@ -67,7 +67,7 @@ def test_seq_variants_fp64_parity(cuda):
         assert np.allclose(gpu.vv, ora.vv, rtol=1e-9, atol=1e-12)
 
 
-@pytest.mark.parametrize("core", [1, 50, 200])
+@pytest.mark.parametrize("core", [0, 1, 50, 200])
 def test_submatrix_inplace_fp64_parity(cuda, core):
     n = 200
     h = M.two_band_1d(n, seed=8)
@@ -79,6 +79,39 @@ def test_submatrix_inplace_fp64_parity(cuda, core):
     d = sp2b.sp2_submatrix_inplace(h, g.pp, g.icount, vv, emin - 0.1, emax + 0.2, core)
     assert rel(d, d_ref) <= FP64_TOL
     assert np.allclose(vv, vv_ref, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("n,core", [(200, 0), (200, 73), (257, 257), (64, 1)])
+def test_submatrix_fp64_parity(cuda, n, core):
+    """prg_sp2_submatrix (src/prg_sp2_mod.F90:1190-1246): separate input block, output
+    rho, vv accumulated over the first core_size rows (core_size 0 adds nothing)."""
+    h = M.two_band_1d(n, seed=11)
+    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    emin, emax = O.gershgorin(h)
+    vv_ref = [0.25] * g.icount
+    d_ref = O.sp2_submatrix(h, g.pp, g.icount, vv_ref, emin, emax, core)
+    vv = np.full(g.icount, 0.25)
+    h_in = h.copy()
+    d = sp2b.sp2_submatrix(h_in, g.pp, g.icount, vv, emin, emax, core)
+    assert np.array_equal(h_in, h)              # the input block is not modified
+    assert rel(d, d_ref) <= FP64_TOL
+    assert np.allclose(vv, vv_ref, rtol=1e-9, atol=1e-12)
+    if core == 0:
+        assert np.all(vv == 0.25)
+
+
+def test_submatrix_zero_steps_and_nan_input(cuda):
+    n = 96
+    h = M.two_band_1d(n, seed=3)
+    emin, emax = O.gershgorin(h)
+    d = sp2b.sp2_submatrix(h, [], 0, np.zeros(1), emin, emax, 10)
+    assert rel(d, 2.0 * O.normalize_bounds(h, emin, emax)) <= 1e-15
+    bad = h.copy()
+    bad[5, 7] = bad[7, 5] = np.nan
+    for icount in (0, 3):
+        with pytest.raises(_lib.SP2Error) as e:
+            sp2b.sp2_submatrix(bad, [0, 1, 0], icount, np.zeros(3), emin, emax, 10)
+        assert e.value.status == _lib.SP2B_BAD_INPUT
 
 
 def test_normalize_gershgorin_idempotency(cuda):
@@ -311,3 +344,16 @@ def test_poly512_plain_cases_of_the_reference_suite(cuda, poly512, alg):
     r = fn(h, 0.5, 25, 100, "Rel", 1e-10)
     assert sp2b.check_idempotency(r.rho / 2) <= 1e-6
     assert abs(np.trace(r.rho) - h.shape[0]) <= 1e-8 * h.shape[0]
+
+
+def test_alg2_genseq_fp64_parity_config1_size(cuda):
+    """The bench's dense workload at full size (two-band, N = 8192, seed 0): the FP64 GPU
+    solve takes the oracle's branch sequence and iteration count, D within 1e-10."""
+    n = 8192
+    h = M.two_band_1d(n, seed=0)
+    ref = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    got = sp2b.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    assert got.pp == ref.pp
+    assert got.icount == ref.icount
+    assert rel(got.rho, ref.rho) <= FP64_TOL
+    assert np.allclose(got.vv, ref.vv, rtol=1e-9, atol=1e-12)
