@@ -41,11 +41,14 @@ extern "C" {
 #define SP2B_PREC_MIXED_FP16 1  /* FP16 hi+lo split products on tcgen05, FP32 accumulate,
                                    FP64 traces, final FP64 McWeeny step */
 #define SP2B_PREC_MIXED_BF16 2  /* same with BF16 hi+lo operands */
-#define SP2B_PREC_EXACT_INT8 3  /* every SP2 step's X^2 from exact INT8 residue products on
-                                   the tensor cores (X rounded to 2^-S, S ~ 35, then squared
-                                   exactly), X kept in FP64; stops on the alg2 rule or when
-                                   Tr(X - X^2) stagnates; no McWeeny step.  Dense entries
-                                   only; the sub-graph entry computes such calls in FP64. */
+#define SP2B_PREC_EXACT_INT8 3  /* every SP2 step's X^2 from exact integer products on the
+                                   INT8 tensor cores.  Dense entries: X rounded to 2^-S
+                                   (S ~ 35) and squared exactly from residue products, X
+                                   kept in FP64; stops on the alg2 rule or when
+                                   Tr(X - X^2) stagnates; no McWeeny step.  Sub-graph
+                                   entry: X - I/2 held in fixed point on the 2^-31 grid as
+                                   four 8-bit digits, X^2 from 13 exact digit products
+                                   (terms below ~2^-36 dropped), one rounding per step. */
 
 /* Products of the McWeeny refinement that ends a mixed solve. */
 #define SP2B_MCW_INT8 0  /* X^2 exact from INT8 residue products (tcgen05 kind::i8) and CRT,
@@ -65,6 +68,12 @@ typedef struct sp2b_opts {
   double refine_tol; /* sub-graph mixed only: parts whose core rows end with
                         sum (X - X^2)_ii > refine_tol are solved again in FP64
                         (default 1e-3; <= 0 turns this off) */
+  int exact_switch;  /* dense mixed only: a nearly gapless input, whose split-precision
+                        loop is still running after exact_switch steps or stops on the
+                        stagnation test (its products cannot resolve the states at the
+                        chemical potential), is solved again from H in the exact INT8
+                        form, which follows the FP64 recursion; the outputs are those of
+                        the exact solve (default 40; 0 turns this off) */
 } sp2b_opts;
 
 /* Fill opts with defaults (FP64, host pointers). */
@@ -75,6 +84,10 @@ int sp2b_opts_default(sp2b_opts* opts);
  * first use. */
 int sp2b_set_default_opts(const sp2b_opts* opts);
 int sp2b_get_default_opts(sp2b_opts* opts);
+
+/* 1 when the last dense solve of this thread started in split precision and was solved
+ * again in the exact INT8 form (sp2b_opts.exact_switch), else 0. */
+int sp2b_last_exact_switch(void);
 
 /* Message describing the last non-OK status of this thread. */
 const char* sp2b_last_error(void);
@@ -296,12 +309,15 @@ int sp2b_graph_square_threshold(int n, const long long* h_row_ptr, const int* h_
  *             through sqrt as prg_fnormGraph does (src/prg_graph_mod.F90:933-971).
  * Host or device pointers per opts.device_ptrs.
  *
- * Split precisions: a part whose final iterate still has a state half-way between
- * occupied and empty (core-row sum of (X - X^2)_ii above opts.refine_tol) is one whose
- * density depends on rounding far below the split products' (a level within ~1e-5 of
- * the chemical potential on a nearly gapless lattice); those parts are solved again
- * in FP64 and their rows replaced, so they equal the FP64 call's.  vv stays that of
- * the split-precision solve. */
+ * Precisions: FP64 (parity), MIXED_FP16 / MIXED_BF16 (hi + lo split products), and
+ * EXACT_INT8 (the INT8 digit form: within ~1e-7 relative Frobenius of FP64 on nearly
+ * gapless lattices, where the hi + lo split ends ~1e-5 away).  In the non-FP64 forms a
+ * part whose final iterate still has a state half-way between occupied and empty
+ * (core-row sum of (X - X^2)_ii above opts.refine_tol) is one whose density depends on
+ * rounding far below the products' (a level within ~1e-5 of the chemical potential);
+ * those parts are solved again in FP64 and their rows replaced, so they equal the FP64
+ * call's.  vv stays that of the first solve.  A part with llsize 0 contributes to
+ * neither output and is not solved. */
 int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
                            const double* h_val, int nparts, const long long* halo_ptr,
                            const int* halo_idx, const int* llsize, const int* pp, int maxiter,

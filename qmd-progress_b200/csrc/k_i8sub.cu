@@ -1,0 +1,552 @@
+// Batched sub-graph SP2 step on the INT8 tensor cores with exact integer products
+// ("INT8 digit split").
+//
+// The iterate is held in fixed point, shifted so that every entry fits the same range:
+// X' = X - I/2 has its spectrum in [-1/2, 1/2] (Gershgorin-normalised X has it in [0, 1]),
+// so |X'_ij| <= 1/2 and M = rint(2^31 X') is an integer with |M| <= 2^30.  M is stored
+// as four balanced base-256 digits,
+//     M = d0 2^24 + d1 2^16 + d2 2^8 + d3,   d1, d2, d3 in [-128, 127], |d0| <= 65,
+// in four signed 8-bit planes.  Then 2^62 X'^2 = sum_{s,t} (D_s D_t) 2^{48 - 8(s+t)}, and
+// every plane product D_s D_t is exact in the 32-bit accumulators (|d| <= 128, K <= 512).
+// Products are grouped by u = s + t into five accumulators A_u (u = 0..4: thirteen
+// products); the three terms with u >= 5 lie below 2^-36 (typical) and are dropped.  The
+// epilogue forms P = 2^46 X'^2 = sum_u A_u 2^{32 - 8u} exactly in 64-bit integers and
+// applies the SP2 branch in the shifted variable,
+//     X^2 branch:      X'_{k+1} = X'^2 + X' - I/4,
+//     2X - X^2 branch: X'_{k+1} = X' - X'^2 + I/4,
+// as M_{k+1} = M_k +- rint(2^31 X'^2) -+ 2^29 [i == j].  The only rounding per step is
+// that of X'^2 to the 2^-31 grid: the recursion follows the FP64 one to ~1e-9 of the
+// entries, which keeps the near-gapless lattice parts within 1e-7 relative Frobenius of
+// the FP64 batch where the FP16 hi + lo products (22 significant bits, accumulations
+// truncated toward zero) end ~1e-5 away.  The residual (X - X^2) = I/4 - X'^2 of the
+// prg_sp2_submatrix bookkeeping (src/prg_sp2_mod.F90:1286-1291) comes from the same P.
+//
+// Layout: the four planes of a ping-pong buffer are four packed R x ld byte arrays
+// (plane s at base + s R ld), so one TMA map over 4R rows covers them all.  Tiles are
+// 128 rows x 64 columns (the five accumulators take 5 x 64 TMEM columns) of the upper
+// part of each part's block: {row0, bi << 16 | bj64, K extent, core rows}.  Padding
+// rows and columns of a part hold X = 0, i.e. X' = -I/2 on the padding diagonal, which
+// the recursion keeps.
+#include "kernels_subgraph.cuh"
+#include "reduce.cuh"
+#include "tc_ptx.cuh"
+
+namespace sp2b {
+namespace i8s {
+constexpr int BM = 128;                         // tile rows (TMEM lanes)
+constexpr int BN = 64;                          // tile columns
+constexpr int BK = 128;                         // K bytes per stage
+constexpr int UK = 32;                          // K per kind::i8 MMA
+constexpr int ND = 4;                           // digit planes
+constexpr int NU = 5;                           // accumulators, u = s + t = 0..4
+constexpr int A_PLANE = BM * BK;                // 16 KB
+constexpr int B_PLANE = BN * BK;                // 8 KB
+constexpr int STAGE_BYTES = ND * (A_PLANE + B_PLANE);   // 96 KB
+constexpr int ST = 2;
+constexpr int EPI_WARPS = 16;                   // 4 lane quarters x 4 groups of 16 columns
+constexpr int NWARP = 2 + EPI_WARPS;
+constexpr int NTHR = NWARP * 32;
+constexpr int SCR_WARP = 16 * 32;               // mirror staging, one plane at a time
+constexpr int SCR_OFF = ST * STAGE_BYTES;
+constexpr int SMEM_BYTES = SCR_OFF + EPI_WARPS * SCR_WARP + 1024;
+constexpr int TMEM_COLS = 512;                  // 5 x 64 used
+constexpr int SHIFT = 31;                       // M = rint(2^31 X')
+}  // namespace i8s
+
+// The thirteen plane products (s, t) with s + t <= 4, grouped by u = s + t; product q
+// multiplies A plane pa(q) by B plane pb(q), and starts its accumulator if first(q).
+__device__ __forceinline__ constexpr int i8_pa(int q) {
+  return q == 0 ? 0 : q == 1 ? 0 : q == 2 ? 1 : q == 3 ? 0 : q == 4 ? 1 : q == 5 ? 2
+       : q == 6 ? 0 : q == 7 ? 1 : q == 8 ? 2 : q == 9 ? 3 : q == 10 ? 1 : q == 11 ? 2 : 3;
+}
+__device__ __forceinline__ constexpr int i8_pb(int q) {
+  return q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 0 : q == 3 ? 2 : q == 4 ? 1 : q == 5 ? 0
+       : q == 6 ? 3 : q == 7 ? 2 : q == 8 ? 1 : q == 9 ? 0 : q == 10 ? 3 : q == 11 ? 2 : 1;
+}
+__device__ __forceinline__ constexpr bool i8_first(int q) {
+  return q == 0 || q == 1 || q == 3 || q == 6 || q == 10;
+}
+
+// Byte j (0..15) of a 16-byte register vector, sign-extended (j is a constant after
+// unrolling, so this folds to one shift pair).
+__device__ __forceinline__ int i8_byte(const uint4& v, int j) {
+  const uint32_t w = (j >> 2) == 0 ? v.x : (j >> 2) == 1 ? v.y : (j >> 2) == 2 ? v.z : v.w;
+  return (int)(int8_t)(uint8_t)(w >> (8 * (j & 3)));
+}
+__device__ __forceinline__ void i8_put(uint4& v, int j, int b) {
+  const uint32_t m = (uint32_t)(uint8_t)b << (8 * (j & 3));
+  if ((j >> 2) == 0) v.x |= m;
+  else if ((j >> 2) == 1) v.y |= m;
+  else if ((j >> 2) == 2) v.z |= m;
+  else v.w |= m;
+}
+
+struct I8Tile {
+  int row0, i0, j0, kb, core;
+  bool ok;
+};
+
+__device__ __forceinline__ I8Tile i8_tile(const StepArgs& p, int t) {
+  const int4 v = p.tiles[t];
+  I8Tile ti;
+  ti.row0 = v.x;
+  ti.i0 = (v.y >> 16) * i8s::BM;
+  ti.j0 = (v.y & 0xffff) * i8s::BN;
+  ti.core = v.w;
+  ti.ok = ti.i0 < v.z && ti.j0 < v.z && v.z % i8s::BK == 0;
+  ti.kb = ti.ok ? v.z / i8s::BK : 0;
+  return ti;
+}
+
+// Balanced base-256 digits of M (|M| < 2^31): d3, d2, d1 in [-128, 127], d0 the rest.
+__device__ __forceinline__ void i8_digits(int m, int8_t& d0, int8_t& d1, int8_t& d2, int8_t& d3) {
+  const int e3 = ((m + 128) & 255) - 128;
+  m = (m - e3) >> 8;
+  const int e2 = ((m + 128) & 255) - 128;
+  m = (m - e2) >> 8;
+  const int e1 = ((m + 128) & 255) - 128;
+  m = (m - e1) >> 8;
+  d0 = (int8_t)max(-127, min(127, m));
+  d1 = (int8_t)e1;
+  d2 = (int8_t)e2;
+  d3 = (int8_t)e3;
+}
+
+__device__ __forceinline__ int i8_value(int8_t d0, int8_t d1, int8_t d2, int8_t d3) {
+  return (((int)d0 * 256 + (int)d1) * 256 + (int)d2) * 256 + (int)d3;
+}
+
+// One SP2 step of every part: out = branch(in) in digit form.  A = B = E = in (4 planes),
+// out: the other buffer.  warp 0: TMA producer; warp 1: TMEM owner and MMA issuer;
+// warps 2..17: epilogue (warp w reads TMEM lane quarter w & 3, columns 16 ((w - 2) >> 2)..).
+__global__ void __launch_bounds__(i8s::NTHR, 1)
+    k_i8_batch(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+               const StepArgs p, long long rows, int ntiles) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full[i8s::ST];
+  __shared__ __align__(8) uint64_t bar_empty[i8s::ST];
+  __shared__ __align__(8) uint64_t bar_tfull;
+  __shared__ __align__(8) uint64_t bar_tempty;
+  __shared__ __align__(8) uint64_t bar_final;
+  __shared__ uint32_t tmem_holder;
+  __shared__ double red[32 * 4];
+  __shared__ int s_flag;
+  __shared__ volatile int s_abort;
+
+  const int br = control_prologue(p);
+  if (br < 0) return;
+  const long long sgn = br == BR_X2 ? 1 : -1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const uint32_t sbase = smem_u32(smem);
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < i8s::ST; ++s) {
+      mbar_init(smem_u32(&bar_full[s]), 1);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    mbar_init(smem_u32(&bar_tfull), 1);
+    mbar_init(smem_u32(&bar_tempty), i8s::EPI_WARPS);
+    mbar_init(smem_u32(&bar_final), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), i8s::TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_holder;
+  double sums[4] = {0.0, 0.0, 0.0, 0.0};
+  const int R = (int)rows;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer ----------------
+      int issued_phase[i8s::ST];
+      for (int s = 0; s < i8s::ST; ++s) issued_phase[s] = -1;
+      bool ok = true;
+      uint32_t g = 0;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const I8Tile ti = i8_tile(p, t);
+        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+          const int s = g % i8s::ST;
+          const uint32_t u = g / i8s::ST;
+          if (g >= (uint32_t)i8s::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          const uint32_t fb = smem_u32(&bar_full[s]);
+          const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+          mbar_expect_tx(fb, i8s::STAGE_BYTES);
+#pragma unroll
+          for (int d = 0; d < i8s::ND; ++d) {
+            tma_load_2d(st + d * i8s::A_PLANE, &tm_a, fb, kb * i8s::BK, d * R + ti.row0 + ti.i0);
+            tma_load_2d(st + i8s::ND * i8s::A_PLANE + d * i8s::B_PLANE, &tm_b, fb, kb * i8s::BK,
+                        d * R + ti.row0 + ti.j0);
+          }
+          issued_phase[s] = u & 1;
+        }
+      }
+      if (!ok) {  // abort: wait (bounded) for this CTA's copies still in flight
+        for (int s = 0; s < i8s::ST; ++s)
+          if (issued_phase[s] >= 0)
+            for (uint32_t i = 0; i < kSpinLimit; ++i)
+              if (mbar_try(smem_u32(&bar_full[s]), issued_phase[s])) break;
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer ----------------
+      constexpr uint32_t idesc = make_idesc_s8(i8s::BM, i8s::BN);
+      bool ok = true;
+      uint32_t g = 0, tl = 0;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const I8Tile ti = i8_tile(p, t);
+        if (!ti.ok) continue;
+        // the accumulators are single-buffered: wait until the epilogue has read the
+        // previous tile's
+        if (tl >= 1 && !mbar_wait(smem_u32(&bar_tempty), (tl - 1) & 1, &s_abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+          const int s = g % i8s::ST;
+          if (!mbar_wait(smem_u32(&bar_full[s]), (g / i8s::ST) & 1, &s_abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < i8s::BK / i8s::UK; ++kk) {
+            const uint64_t off = (uint64_t)((kk * i8s::UK) >> 4);
+#pragma unroll
+            for (int q = 0; q < 13; ++q) {
+              const int sa = i8_pa(q), sb = i8_pb(q);
+              // the first product of each u at k = 0 starts its accumulator
+              const uint64_t da = sw128_desc(st + sa * i8s::A_PLANE) + off;
+              const uint64_t db = sw128_desc(st + i8s::ND * i8s::A_PLANE + sb * i8s::B_PLANE) + off;
+              umma_i8(tmem + (sa + sb) * i8s::BN, da, db, idesc,
+                      (kb > 0 || kk > 0 || !i8_first(q)) ? 1u : 0u);
+            }
+          }
+          umma_commit(smem_u32(&bar_empty[s]));
+        }
+        if (!ok) break;
+        umma_commit(smem_u32(&bar_tfull));
+        ++tl;
+      }
+      umma_commit(smem_u32(&bar_final));
+      for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try(smem_u32(&bar_final), 0)) break;
+      if (!ok) s_abort = 1;
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (16 warps) ----------------
+    const int q = warp & 3;                   // TMEM lane quarter
+    const int grp = (warp - 2) >> 2;          // 16-column group of the 64-column tile
+    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const int ld = p.ld;
+    const size_t plane = (size_t)R * ld;
+    const int8_t* X = (const int8_t*)p.A;
+    int8_t* O = (int8_t*)p.out;
+    uint8_t* scr = smem + i8s::SCR_OFF + (warp - 2) * i8s::SCR_WARP;
+    uint32_t tl = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const I8Tile ti = i8_tile(p, t);
+      if (!ti.ok) continue;
+      const int rl = q * 32 + lane;             // row inside the tile
+      const int r = ti.i0 + rl;                 // row inside the part
+      const int c0 = ti.j0 + grp * 16;          // first column of this thread's 16
+      const size_t rowoff = ((size_t)ti.row0 + r) * ld + c0;
+      // X_k digits of this thread's 16 elements (read before the accumulators are ready)
+      uint4 xd[i8s::ND];
+#pragma unroll
+      for (int d = 0; d < i8s::ND; ++d)
+        xd[d] = *reinterpret_cast<const uint4*>(X + d * plane + rowoff);
+      if (!mbar_wait_idle(smem_u32(&bar_tfull), tl & 1, &s_abort)) break;
+      tc_fence_after();
+      long long P[16];
+      {
+        uint32_t acc[16];
+        const uint32_t ta = tmem + lane_base + grp * 16;
+        tmem_ld16(ta, acc);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) P[j] = (long long)(int)acc[j] * (1ll << 32);
+#pragma unroll
+        for (int u = 1; u < i8s::NU; ++u) {
+          tmem_ld16(ta + u * i8s::BN, acc);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 16; ++j) P[j] += (long long)(int)acc[j] * (1ll << (32 - 8 * u));
+        }
+      }
+      tc_fence_before();   // TMEM reads ordered before the release
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bar_tempty));
+      ++tl;
+
+      uint4 nd[i8s::ND];
+#pragma unroll
+      for (int d = 0; d < i8s::ND; ++d) nd[d] = make_uint4(0u, 0u, 0u, 0u);
+      double s_res = 0.0, s_tr = 0.0, s_trp = 0.0;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = c0 + j;
+        const bool dg = r == c;
+        const long long m = (long long)((((i8_byte(xd[0], j) * 256 + i8_byte(xd[1], j)) * 256 +
+                                          i8_byte(xd[2], j)) * 256) + i8_byte(xd[3], j));
+        const long long qv = (P[j] + (1ll << 14)) >> 15;            // rint(2^31 X'^2)
+        const long long mn = m + sgn * qv - (dg ? sgn * (1ll << 29) : 0ll);
+        int8_t b0, b1, b2, b3;
+        i8_digits((int)mn, b0, b1, b2, b3);
+        i8_put(nd[0], j, b0);
+        i8_put(nd[1], j, b1);
+        i8_put(nd[2], j, b2);
+        i8_put(nd[3], j, b3);
+        // weight of (r, c) in the full-matrix sums: itself and its mirror above the
+        // diagonal, once on it, nothing below it (the mirror of another tile carries it)
+        const int w = r < c ? 2 : (dg ? 1 : 0);
+        const int cw = core_weight(w, r, c, ti.core);
+        const double res = (double)((dg ? (1ll << 44) : 0ll) - P[j]);   // 2^46 (X - X^2)
+        s_res = fma((double)cw * res, res, s_res);
+        if (dg) {
+          s_tr += (double)mn * 0x1p-31 + 0.5;
+          s_trp += (double)P[j] * 0x1p-46 + (double)m * 0x1p-31 + 0.25;   // Tr X^2
+        }
+      }
+      sums[1] += s_tr;
+      sums[2] = fma(s_res, 0x1p-92, sums[2]);
+      sums[3] += s_trp;
+      // X_{k+1}: this thread's 16 bytes per plane, and the warp's 32 x 16 block mirrored
+      // (rows c0.., columns of this warp's 32 rows) through shared memory.  Mirror values
+      // that land on or above the diagonal equal the ones stored there directly (the
+      // integer products are exactly symmetric), so no element needs masking.
+#pragma unroll
+      for (int d = 0; d < i8s::ND; ++d) {
+        *reinterpret_cast<uint4*>(O + d * plane + rowoff) = nd[d];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) scr[j * 32 + lane] = (uint8_t)i8_byte(nd[d], j);
+        __syncwarp();
+        const int jj = lane >> 1, hf = lane & 1;
+        const uint4 v = *reinterpret_cast<const uint4*>(scr + jj * 32 + hf * 16);
+        *reinterpret_cast<uint4*>(O + d * plane + ((size_t)ti.row0 + c0 + jj) * ld + ti.i0 +
+                                  q * 32 + hf * 16) = v;
+        __syncwarp();
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tmem_dealloc(tmem, i8s::TMEM_COLS);
+  if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+  __threadfence();
+  publish_and_finalize(p, sums, red, &s_flag);
+}
+
+cudaError_t launch_i8_batched(const StepArgs& a, long long rows, cudaStream_t st) {
+  if (!a.tiles || a.ntiles <= 0 || a.ld % i8s::BK != 0 || rows % i8s::BM != 0 || !a.A ||
+      !a.out || 4 * rows > 0x7fffffffLL)
+    return cudaErrorInvalidValue;
+  CUtensorMap ma, mb;
+  if (!make_tmap_box(&ma, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BM) ||
+      !make_tmap_box(&mb, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BN))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(k_i8_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       i8s::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  const int grid = std::min(a.ntiles, device_sms());
+  k_i8_batch<<<grid, i8s::NTHR, i8s::SMEM_BYTES, st>>>(ma, mb, a, rows, a.ntiles);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------
+// Digit-form extraction, scatter and part idempotency for the batched INT8 mode.
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void i8_store_x(int8_t* base, size_t plane, size_t idx, double xprime) {
+  const int m = (int)llrint(xprime * 0x1p31);
+  int8_t d0, d1, d2, d3;
+  i8_digits(m, d0, d1, d2, d3);
+  base[idx] = d0;
+  base[plane + idx] = d1;
+  base[2 * plane + idx] = d2;
+  base[3 * plane + idx] = d3;
+}
+
+// CSR rows of each part straight to X0' = X0 - I/2 in digits (parts up to 512), with the
+// same row construction as the split extraction: one warp per row in shared memory.
+__global__ void __launch_bounds__(256) k_extract_digits(
+    const long long* __restrict__ rp, const int* __restrict__ col, const double* __restrict__ val,
+    const PartDesc* __restrict__ parts, const int* __restrict__ halo, const int* __restrict__ skey,
+    const int* __restrict__ sval, int ld, long long rows, double emin, double emax,
+    int8_t* __restrict__ dig) {
+  __shared__ double rowbuf[8][512];
+  const PartDesc P = parts[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double mm = emax - emin;
+  const double alpha = -1.0 / mm, beta = emax / mm;
+  const int* hl = halo + P.hoff;
+  const int* sk = skey + P.hoff;
+  const int* sv = sval + P.hoff;
+  const size_t plane = (size_t)rows * ld;
+  double* buf = rowbuf[warp];
+  for (int r = blockIdx.y * 8 + warp; r < P.np; r += gridDim.y * 8) {
+    for (int c = lane; c < P.np; c += 32) buf[c] = 0.0;
+    __syncwarp();
+    if (r < P.n) {
+      const int v = hl[r];
+      for (long long e = rp[v] + lane; e < rp[v + 1]; e += 32) {
+        const int u = col[e];
+        int a = 0, b = P.n - 1;
+        while (a <= b) {
+          const int mid = (a + b) >> 1;
+          const int key = sk[mid];
+          if (key == u) {
+            buf[sv[mid]] = val[e];
+            break;
+          }
+          if (key < u) a = mid + 1;
+          else b = mid - 1;
+        }
+      }
+    }
+    __syncwarp();
+    const size_t ro = ((size_t)P.row0 + r) * ld;
+    for (int c = lane; c < P.np; c += 32) {
+      // separate roundings (no contraction), so a host model forms the same X0'
+      double x = 0.0;
+      if (r < P.n && c < P.n) {
+        x = __dmul_rn(alpha, buf[c]);
+        if (r == c) x = __dadd_rn(x, beta);
+      }
+      i8_store_x(dig, plane, ro + c, r == c ? __dadd_rn(x, -0.5) : x);
+    }
+    __syncwarp();
+  }
+}
+
+// The same from the FP64 packed extraction (parts above 512): X0' digits of every
+// packed element.
+__global__ void k_norm_digits(const double* __restrict__ xs, const int* __restrict__ row_part,
+                              const PartDesc* __restrict__ parts, long long rows, int ld,
+                              double emin, double emax, int8_t* __restrict__ dig) {
+  const double mm = emax - emin;
+  const double alpha = -1.0 / mm, beta = emax / mm;
+  const size_t total = (size_t)rows * ld;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const long long gr = (long long)(idx / ld);
+    const int c = (int)(idx % ld);
+    const PartDesc P = parts[row_part[gr]];
+    const int r = (int)(gr - P.row0);
+    double v = 0.0;
+    if (r < P.n && c < P.n) {
+      v = __dmul_rn(alpha, xs[idx]);
+      if (r == c) v = __dadd_rn(v, beta);
+    }
+    if (c < P.np) i8_store_x(dig, total, idx, r == c ? __dadd_rn(v, -0.5) : v);
+  }
+}
+
+// rho (core rows) = 2 X = 2^-30 M + I.
+__global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
+                                 const PartDesc* __restrict__ parts, const int* __restrict__ halo,
+                                 int ld, double* __restrict__ core_out, double* __restrict__ dense,
+                                 long long n) {
+  const PartDesc P = parts[blockIdx.x];
+  const int* hl = halo + P.hoff;
+  const size_t plane = (size_t)rows * ld;
+  const long long total = (long long)P.ncore * P.n;
+  for (long long q = (long long)blockIdx.y * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.y * blockDim.x) {
+    const int r = (int)(q / P.n), c = (int)(q % P.n);
+    const size_t src = ((size_t)P.row0 + r) * ld + c;
+    const int m = i8_value(dig[src], dig[plane + src], dig[2 * plane + src], dig[3 * plane + src]);
+    const double v = (double)m * 0x1p-30 + (r == c ? 1.0 : 0.0);
+    if (core_out) core_out[P.coff + q] = v;
+    if (dense) dense[(size_t)hl[r] + (size_t)hl[c] * n] = v;
+  }
+}
+
+// Sum over each part's core rows of (X - X^2)_ii = X_ii - sum_j X_ij^2, from the digits.
+__global__ void k_part_idem_digits(const int8_t* __restrict__ dig, long long rows,
+                                   const PartDesc* __restrict__ parts, int ld,
+                                   double* __restrict__ out) {
+  __shared__ double red[32];
+  const PartDesc P = parts[blockIdx.x];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const size_t plane = (size_t)rows * ld;
+  double s = 0.0;
+  for (int r = blockIdx.y * nw + warp; r < P.ncore; r += gridDim.y * nw) {
+    const size_t row = ((size_t)P.row0 + r) * ld;
+    for (int c0 = lane * 16; c0 < P.np; c0 += 512) {
+      uint4 v[4];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) v[d] = *reinterpret_cast<const uint4*>(dig + d * plane + row + c0);
+      const int8_t* b0 = reinterpret_cast<const int8_t*>(&v[0]);
+      const int8_t* b1 = reinterpret_cast<const int8_t*>(&v[1]);
+      const int8_t* b2 = reinterpret_cast<const int8_t*>(&v[2]);
+      const int8_t* b3 = reinterpret_cast<const int8_t*>(&v[3]);
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const double x = (double)i8_value(b0[e], b1[e], b2[e], b3[e]) * 0x1p-31 +
+                         (c0 + e == r ? 0.5 : 0.0);
+        s -= x * x;
+        if (c0 + e == r) s += x;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    out[(size_t)blockIdx.x * gridDim.y + blockIdx.y] = t;
+  }
+}
+
+cudaError_t launch_extract_digits(const long long* rp, const int* col, const double* val,
+                                  const PartDesc* parts, int nparts, const int* halo,
+                                  const int* skey, const int* sval, int ld, long long rows,
+                                  double emin, double emax, int8_t* dig, cudaStream_t st) {
+  if (ld > 512) return cudaErrorInvalidValue;
+  k_extract_digits<<<dim3(nparts, 16), 256, 0, st>>>(rp, col, val, parts, halo, skey, sval, ld,
+                                                     rows, emin, emax, dig);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_norm_digits(const double* xs, const int* row_part, const PartDesc* parts,
+                               long long rows, int ld, double emin, double emax, int8_t* dig,
+                               cudaStream_t st) {
+  size_t g = ((size_t)rows * ld + 255) / 256;
+  if (g > 148 * 8) g = 148 * 8;
+  k_norm_digits<<<(int)(g ? g : 1), 256, 0, st>>>(xs, row_part, parts, rows, ld, emin, emax, dig);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_digits(const int8_t* dig, long long rows, const PartDesc* parts,
+                                  int nparts, const int* halo, int ld, double* core_out,
+                                  double* dense, long long n, cudaStream_t st) {
+  k_scatter_digits<<<dim3(nparts, 16), 256, 0, st>>>(dig, rows, parts, halo, ld, core_out, dense,
+                                                     n);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_part_idem_digits(const int8_t* dig, long long rows, const PartDesc* parts,
+                                    int nparts, int ld, double* out, cudaStream_t st) {
+  k_part_idem_digits<<<dim3(nparts, kPartIdemGroups), 256, 0, st>>>(dig, rows, parts, ld, out);
+  note_launch();
+  return cudaGetLastError();
+}
+
+}  // namespace sp2b

@@ -40,4 +40,22 @@ constexpr int kPartIdemGroups = 16;
 cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const PartDesc* parts,
                              int nparts, int ld, double* out, cudaStream_t st);
 
+// Batched INT8 digit-split form (exact INT8 precision of the sub-graph loop): the
+// iterate as four signed 8-bit planes of M = rint(2^31 (X - I/2)) in each packed buffer
+// (plane s at base + s rows ld).  Tiles {row0, bi << 16 | bj64, K extent, core} of
+// 128 x 64 over the upper part of each part's block.
+cudaError_t launch_i8_batched(const StepArgs& a, long long rows, cudaStream_t st);
+cudaError_t launch_extract_digits(const long long* rp, const int* col, const double* val,
+                                  const PartDesc* parts, int nparts, const int* halo,
+                                  const int* skey, const int* sval, int ld, long long rows,
+                                  double emin, double emax, int8_t* dig, cudaStream_t st);
+cudaError_t launch_norm_digits(const double* xs, const int* row_part, const PartDesc* parts,
+                               long long rows, int ld, double emin, double emax, int8_t* dig,
+                               cudaStream_t st);
+cudaError_t launch_scatter_digits(const int8_t* dig, long long rows, const PartDesc* parts,
+                                  int nparts, const int* halo, int ld, double* core_out,
+                                  double* dense, long long n, cudaStream_t st);
+cudaError_t launch_part_idem_digits(const int8_t* dig, long long rows, const PartDesc* parts,
+                                    int nparts, int ld, double* out, cudaStream_t st);
+
 }  // namespace sp2b

@@ -36,6 +36,7 @@ struct SubBufs {
   double* x2 = nullptr;          size_t x2_cap = 0;     // FP64 ping-pong partner
   __half* hi[2] = {};            size_t hi_cap[2] = {};
   __half* lo[2] = {};            size_t lo_cap[2] = {};
+  int8_t* dig[2] = {};           size_t dig_cap[2] = {};   // INT8 digit planes (4 per buffer)
   PartDesc* parts = nullptr;     size_t parts_cap = 0;
   int4* tiles = nullptr;         size_t tiles_cap = 0;
   int* row_part = nullptr;       size_t row_part_cap = 0;
@@ -61,7 +62,7 @@ struct SubBufs {
   std::vector<long long> last_hp;
   std::vector<int> last_lls, last_hidx;
   std::vector<PartDesc> P;
-  int ld = 0, ntiles = 0, layout_bt = 0, layout_order = 0;
+  int ld = 0, ntiles = 0, layout_bt = 0, layout_order = 0, layout_dig = 0;
   long long rows = 0, coff = 0;
   bool layout_valid = false;
   // instantiated graph of the last call and the inputs it was captured with
@@ -112,11 +113,11 @@ struct SubJob {
   const int* pp;         // host, maxiter entries
   int maxiter;
   double mineval, maxeval;
-  int prec;              // SP2B_PREC_FP64 / _MIXED_FP16 / _MIXED_BF16
+  int prec;              // SP2B_PREC_FP64 / _MIXED_FP16 / _MIXED_BF16 / _EXACT_INT8
   double* core;          // device, packed core rows, or null
   double* dense;         // device, n x n, or null
   bool clear_dense;      // zero `dense` before the scatter
-  bool part_idem;        // split only: per-part idempotency sums into b.idem
+  bool part_idem;        // split and INT8 only: per-part idempotency sums into b.idem
   bool multistep;        // FP64 only: all steps in one cooperative launch when it fits
   // measured launch configuration (-1: the built-in rule).  FP64: the tile edge (32 or 64);
   // split: the order of the tile list (0 largest parts first, 1 balanced over the CTAs)
@@ -132,7 +133,9 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   const std::vector<int>& hidx = *j.hidx;
   const int nparts = (int)lls.size();
   const int maxiter = j.maxiter, n = j.n, prec = j.prec;
-  const bool split = prec != SP2B_PREC_FP64;
+  // split: FP16 / BF16 hi + lo products; dig: INT8 digit-split products
+  const bool dig = prec == SP2B_PREC_EXACT_INT8;
+  const bool split = prec == SP2B_PREC_MIXED_FP16 || prec == SP2B_PREC_MIXED_BF16;
   const long long nhalo = hp[nparts];
   cudaStream_t cap = c->stream;
 
@@ -141,7 +144,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   // ones).  The FP64 sums run in the same k order for every edge, so the results agree
   // bit for bit.
   int bt = 128;
-  if (!split) {
+  if (!split && !dig) {
     long long t64 = 0;
     for (int p = 0; p < nparts; ++p) {
       const long long t = padded((int)(hp[p + 1] - hp[p])) / 64;
@@ -152,7 +155,8 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   }
   const int tile_order = (split && j.variant == 1) ? 1 : 0;
   const bool same_layout = b.layout_valid && b.layout_bt == bt && b.layout_order == tile_order &&
-                           b.last_hp == hp && b.last_lls == lls && b.last_hidx == hidx;
+                           b.layout_dig == (dig ? 1 : 0) && b.last_hp == hp && b.last_lls == lls &&
+                           b.last_hidx == hidx;
   if (!same_layout) {
     b.layout_valid = false;
     std::vector<PartDesc>& P = b.P;
@@ -208,14 +212,27 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     std::stable_sort(order.begin(), order.end(), [&](int a, int b2) { return P[a].np > P[b2].np; });
     std::vector<int4> tiles;
     for (int p : order) {
+      // a part without core rows contributes to neither rho nor vv: no tiles
+      if (P[p].ncore <= 0) continue;
+      if (dig) {
+        // 128 x 64 tiles that reach the diagonal or lie above it; K over the whole
+        // padded block (the padding diagonal holds X' = -1/2, not zero)
+        for (int bi = 0; bi < P[p].np / 128; ++bi)
+          for (int bj = 2 * bi; bj < P[p].np / 64; ++bj)
+            tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj, P[p].np, P[p].ncore));
+        continue;
+      }
       const int T = P[p].np / bt;
       for (int bj = 0; bj < T; ++bj)
         for (int bi = 0; bi <= bj; ++bi)
           // K runs only to the part size rounded up to 64: the rest of the padded
           // block is zero, so those k-blocks contribute nothing
           tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj,
-                                    std::min(P[p].np, (P[p].n + 63) / 64 * 64),
-                                    P[p].ncore > 0 ? P[p].ncore : -1));
+                                    std::min(P[p].np, (P[p].n + 63) / 64 * 64), P[p].ncore));
+    }
+    if (tiles.empty()) {
+      set_last_error("no part has core rows");
+      return SP2B_BAD_ARG;
     }
     const int ntiles = (int)tiles.size();
     if (tile_order == 1) {
@@ -264,6 +281,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     b.last_hidx = hidx;
     b.layout_bt = bt;
     b.layout_order = tile_order;
+    b.layout_dig = dig ? 1 : 0;
     b.layout_valid = true;
   }
   const int ld = b.ld;
@@ -274,16 +292,18 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   const size_t packed = (size_t)rows * ld;
   // parts up to 512: CSR straight to X0 (split: hi/lo, no FP64 block; FP64: no clearing)
   const bool fused = ld <= 512;
-  if (!split || !fused) SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
+  if ((!split && !dig) || !fused) SP2B_CUDA_TRY(grow_buf(b.xs, b.xs_cap, packed));
   if (split) {
     for (int i = 0; i < 2; ++i) {
       SP2B_CUDA_TRY(grow_buf(b.hi[i], b.hi_cap[i], packed));
       SP2B_CUDA_TRY(grow_buf(b.lo[i], b.lo_cap[i], packed));
     }
+  } else if (dig) {
+    for (int i = 0; i < 2; ++i) SP2B_CUDA_TRY(grow_buf(b.dig[i], b.dig_cap[i], 4 * packed));
   } else {
     SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
   }
-  const bool idem = split && j.part_idem;
+  const bool idem = (split || dig) && j.part_idem;
   if (idem) SP2B_CUDA_TRY(grow_buf(b.idem, b.idem_cap, (size_t)nparts * kPartIdemGroups));
   SP2B_CUDA_TRY(grow_buf(b.partials, b.partials_cap, 4 * (size_t)ntiles));
   SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
@@ -295,7 +315,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   double* dense_d = j.dense;
 
   // ---- a few FP64 parts: every step in one cooperative launch ----
-  if (j.multistep && !split && bt == 32 && maxiter > 0) {
+  if (j.multistep && !split && !dig && bt == 32 && maxiter > 0) {
     SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
     SP2B_CUDA_TRY(cudaMemsetAsync(b.ms_bar, 0, nparts * sizeof(unsigned), st));
     if (dense_d && j.clear_dense)
@@ -372,7 +392,8 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     double d[2];
   } key;
   memset(&key, 0, sizeof(key));
-  const void* ptrs[22] = {j.rp, j.col, j.val, core_d, dense_d, b.xs, b.x2, b.hi[0], b.hi[1],
+  const void* ptrs[22] = {j.rp, j.col, j.val, core_d, dense_d, b.xs, b.x2,
+                          dig ? (const void*)b.dig[0] : b.hi[0], dig ? (const void*)b.dig[1] : b.hi[1],
                           b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
                           b.sval, b.partials, b.rec, b.pp, (const void*)cap,
                           idem ? b.idem : nullptr};
@@ -406,7 +427,21 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       if (dense_d && j.clear_dense &&
           (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
         return e;
-      if (fused) {
+      if (dig) {
+        if (fused) {
+          if ((e = launch_extract_digits(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey,
+                                         b.sval, ld, rows, j.mineval, j.maxeval, b.dig[0], cap)) !=
+              cudaSuccess)
+            return e;
+        } else {
+          if ((e = launch_extract_csr(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
+                                      ld, b.xs, cap)) != cudaSuccess)
+            return e;
+          if ((e = launch_norm_digits(b.xs, b.row_part, b.parts, rows, ld, j.mineval, j.maxeval,
+                                      b.dig[0], cap)) != cudaSuccess)
+            return e;
+        }
+      } else if (fused) {
         if ((e = launch_extract_split(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey, b.sval,
                                       ld, j.mineval, j.maxeval, prec, split ? b.hi[0] : nullptr,
                                       split ? b.lo[0] : nullptr, split ? nullptr : b.xs, cap)) !=
@@ -424,7 +459,11 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       for (int k = 0; k < maxiter; ++k) {
         a.k = k;
         const int bin = k & 1, bout = (k + 1) & 1;
-        if (split) {
+        if (dig) {
+          a.A = a.B = a.E = b.dig[bin];
+          a.out = b.dig[bout];
+          e = launch_i8_batched(a, rows, cap);
+        } else if (split) {
           a.A = a.B = a.E = b.hi[bin];
           a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
           a.out = b.hi[bout];
@@ -440,6 +479,14 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
         if (e != cudaSuccess) return e;
       }
       const int fb = maxiter & 1;
+      if (dig) {
+        if ((e = launch_scatter_digits(b.dig[fb], rows, b.parts, nparts, b.halo, ld, core_d,
+                                       dense_d, n, cap)) != cudaSuccess)
+          return e;
+        if (idem)
+          return launch_part_idem_digits(b.dig[fb], rows, b.parts, nparts, ld, b.idem, cap);
+        return cudaSuccess;
+      }
       if ((e = launch_scatter_parts(fb ? b.x2 : b.xs, split ? (void*)b.hi[fb] : nullptr,
                                     split ? (void*)b.lo[fb] : nullptr, prec, b.parts, nparts,
                                     b.halo, ld, core_d, dense_d, n, cap)) != cudaSuccess)
@@ -494,7 +541,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
 // whole solves of this job; sets j.variant.
 static int tune_subgraph(Ctx* c, SubBufs& b, SubJob& j, cudaStream_t st) {
   j.variant = -1;
-  if (!tune_enabled() || j.multistep) return SP2B_OK;
+  if (!tune_enabled() || j.multistep || j.prec == SP2B_PREC_EXACT_INT8) return SP2B_OK;
   const bool split = j.prec != SP2B_PREC_FP64;
   const std::vector<long long>& hp = *j.hp;
   std::map<int, int> hist;
@@ -544,10 +591,14 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   sp2b_opts_default(&dflt);
   dflt.precision = SP2B_PREC_MIXED_FP16;
   if (!opts) opts = &dflt;
-  // the exact INT8 mode has no batched form: such calls run the FP64 batch
-  const int prec = opts->precision == SP2B_PREC_EXACT_INT8 ? SP2B_PREC_FP64 : opts->precision;
+  const int prec = opts->precision;
+  if (prec != SP2B_PREC_FP64 && prec != SP2B_PREC_MIXED_FP16 && prec != SP2B_PREC_MIXED_BF16 &&
+      prec != SP2B_PREC_EXACT_INT8) {
+    set_last_error("sp2b_subgraph_sp2_loop: unknown precision %d", prec);
+    return SP2B_BAD_ARG;
+  }
   const bool dev = opts->device_ptrs != 0;
-  const bool split = prec != SP2B_PREC_FP64;
+  const bool split = prec != SP2B_PREC_FP64;   // every non-FP64 form may re-solve parts
   int status = SP2B_OK;
   Ctx* c = get_ctx(&status);
   if (!c) return status;

@@ -22,6 +22,7 @@ SOURCES = [
     "k_tc.cu",
     "k_ozaki.cu",
     "k_subgraph.cu",
+    "k_i8sub.cu",
     "k_graph.cu",
     "sp2b_dense.cu",
     "sp2b_subgraph.cu",
