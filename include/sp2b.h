@@ -331,6 +331,17 @@ int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const int* h_col,
 int sp2b_last_subgraph_refined(int* count, int* parts, int max_parts, double* idem,
                                int nparts);
 
+/* Assembly step of the multi-rank sub-graph loop (prg_collectMatrixFromParts,
+ * src/prg_subgraphloop_mod.F90:132-161), on the device: part p's packed core rows
+ * (llsize[p] x lsize[p], lsize[p] = halo_ptr[p+1] - halo_ptr[p], row-major, as
+ * sp2b_subgraph_sp2_loop packs them) at src + src_off[p] are written into the dense
+ * column-major n x n rho (entry (halo_idx[halo_ptr[p]+r], halo_idx[halo_ptr[p]+c])).
+ * All pointers are DEVICE pointers; work runs on `stream`; elements of rho outside the
+ * core rows are left as they are. */
+int sp2b_place_core_rows(long long n, int nparts, const long long* halo_ptr, const int* halo_idx,
+                         const int* llsize, const long long* src_off, const double* src,
+                         double* rho, void* stream);
+
 /* ---- device-resident building blocks (used by the torch binding) ------------------ */
 
 /* Split-precision symmetric-operand product on device arrays:

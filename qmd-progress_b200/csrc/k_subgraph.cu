@@ -247,6 +247,36 @@ cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const Par
   return cudaGetLastError();
 }
 
+// Packed core-row blocks (as all-gathered from the ranks) into a dense column-major
+// n x n density: part p's llsize x lsize block starts at src + off[p], row r = node
+// halo[hptr[p] + r], column c = node halo[hptr[p] + c] (prg_collectMatrixFromParts,
+// src/prg_subgraphloop_mod.F90:132-161).  One CTA row per part.
+__global__ void k_place_core(const long long* __restrict__ hptr, const int* __restrict__ halo,
+                             const int* __restrict__ lls, const long long* __restrict__ off,
+                             const double* __restrict__ src, double* __restrict__ rho,
+                             long long n) {
+  const int p = blockIdx.x;
+  const long long h0 = hptr[p];
+  const int m = (int)(hptr[p + 1] - h0);
+  const long long total = (long long)lls[p] * m;
+  const int* hl = halo + h0;
+  const double* s = src + off[p];
+  for (long long q = (long long)blockIdx.y * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.y * blockDim.x) {
+    const int r = (int)(q / m), c = (int)(q % m);
+    rho[(size_t)hl[r] + (size_t)hl[c] * n] = s[q];
+  }
+}
+
+cudaError_t launch_place_core(const long long* hptr, const int* halo, const int* lls,
+                              const long long* off, int nparts, const double* src, double* rho,
+                              long long n, cudaStream_t st) {
+  if (nparts <= 0) return cudaSuccess;
+  k_place_core<<<dim3(nparts, 8), 256, 0, st>>>(hptr, halo, lls, off, src, rho, n);
+  note_launch();
+  return cudaGetLastError();
+}
+
 cudaError_t launch_extract_csr(const long long* rp, const int* col, const double* val,
                                const PartDesc* parts, int nparts, const int* halo,
                                const int* skey, const int* sval, int ld, double* xs,

@@ -40,6 +40,10 @@ constexpr int kPartIdemGroups = 16;
 cudaError_t launch_part_idem(const void* hi, const void* lo, int prec, const PartDesc* parts,
                              int nparts, int ld, double* out, cudaStream_t st);
 
+cudaError_t launch_place_core(const long long* hptr, const int* halo, const int* lls,
+                              const long long* off, int nparts, const double* src, double* rho,
+                              long long n, cudaStream_t st);
+
 // Batched INT8 digit-split form (exact INT8 precision of the sub-graph loop): the
 // iterate as four signed 8-bit planes of M = rint(2^31 (X - I/2)) in each packed buffer
 // (plane s at base + s rows ld).  Tiles {row0, bi << 16 | bj64, K extent, core} of

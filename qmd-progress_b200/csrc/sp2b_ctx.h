@@ -84,6 +84,7 @@ struct DenseJob {
   double* bounds_out;
   int mcweeny;
   int mcweeny_products;  // SP2B_MCW_INT8 or SP2B_MCW_FP64
+  int exact_switch;      // mixed: steps after which a still-running loop restarts exact
   const double* h1;      // forward-mode response: perturbation H1 (nullptr: plain solve)
   double* rsp;           // ... and its output, the response rho1 = 2 Delta
 };

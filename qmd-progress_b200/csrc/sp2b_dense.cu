@@ -183,7 +183,13 @@ static cudaStream_t pick_stream(const sp2b_opts* o, Ctx* c) {
   return (o && o->device_ptrs) ? (cudaStream_t)0 : c->stream;
 }
 
-int dense_solve(const DenseJob& j) {
+static thread_local int t_exact_switch = 0;   // the last solve restarted in the exact form
+
+// One solve.  A mixed trace-driven solve with exact_switch > 0 sets *want_exact and
+// returns without writing its outputs when its loop shows a spectrum the split products
+// cannot resolve: still running after exact_switch steps, or stopped on the stagnation
+// test (the last step's Tr X - Tr P above mixed_tol) or on maxsp2iter.
+static int dense_solve_once(const DenseJob& j, bool* want_exact) {
   if (j.n <= 0 || !j.rho || (!j.h && !j.inplace)) {
     set_last_error("bad argument: n=%d h=%p rho=%p", j.n, (void*)j.h, (void*)j.rho);
     return SP2B_BAD_ARG;
@@ -226,6 +232,8 @@ int dense_solve(const DenseJob& j) {
   // one McWeeny step of a split solve runs on the INT8 tensor cores (exact residue
   // products); more steps, or the FP64 choice, use FP64 DMMA products
   const bool oz = split && j.mcweeny == 1 && j.mcweeny_products == SP2B_MCW_INT8 && np <= 65536;
+  const bool fallback = split && j.ctl.algo == ALGO_MIXED && j.exact_switch > 0 && want_exact &&
+                        np <= 65536;
   const size_t nn = (size_t)n * n;
   SP2B_CUDA_TRY(c->ensure_common(j.dev_ptrs ? 0 : nn, np, maxlaunch, n));
   SP2B_CUDA_TRY(c->ensure_f64(np, split ? (oz ? 1 : 3) : (resp ? 5 : 2)));
@@ -325,7 +333,12 @@ int dense_solve(const DenseJob& j) {
   bool done = (maxlaunch == 0);
   const bool timing = g_step_timing.load() != 0;
   while (!done && k < maxlaunch) {
-    const int kend = std::min(maxlaunch, k + chunk);
+    if (fallback && k >= j.exact_switch) {   // still running: a nearly gapless spectrum
+      *want_exact = true;
+      return SP2B_OK;
+    }
+    int kend = std::min(maxlaunch, k + chunk);
+    if (fallback) kend = std::min(kend, std::max(j.exact_switch, k + 1));
     const int k0 = k;
     if (timing) {
       while ((int)c->ev.size() < 2 * chunk) {
@@ -411,6 +424,22 @@ int dense_solve(const DenseJob& j) {
   c->last_launches = k;
   SolveOut so = *c->h_sout;
   if (maxlaunch == 0) so.nupd = 0;
+  if (fallback && so.nupd > 0) {
+    // the stop reason: Tr X - Tr P of the last update above mixed_tol means the
+    // stagnation test (or maxsp2iter) ended the loop
+    SP2Rec last;
+    SP2B_CUDA_TRY(cudaMemcpyAsync(&last, c->rec + so.nupd, sizeof(SP2Rec), cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    if (so.status == SP2B_OK && (last.err_hist[1] > j.ctl.mixed_tol ||
+                                 !(last.err_hist[1] == last.err_hist[1]))) {
+      *want_exact = true;
+      return SP2B_OK;
+    }
+    if (so.status == SP2B_NOT_CONVERGED) {
+      *want_exact = true;
+      return SP2B_OK;
+    }
+  }
   // normalisation itself may have flagged bad input
   SP2B_CUDA_TRY(cudaMemcpyAsync(c->h_small + 8, norm_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   SP2B_CUDA_TRY(cudaStreamSynchronize(st));
@@ -559,6 +588,19 @@ int dense_solve(const DenseJob& j) {
   return SP2B_OK;
 }
 
+int dense_solve(const DenseJob& j) {
+  t_exact_switch = 0;
+  bool want_exact = false;
+  const int st = dense_solve_once(j, &want_exact);
+  if (st != SP2B_OK || !want_exact) return st;
+  // solved again from the input in the exact INT8 form (the split run wrote no output)
+  DenseJob e = j;
+  e.prec = SP2B_PREC_EXACT_INT8;
+  e.exact_switch = 0;
+  t_exact_switch = 1;
+  return dense_solve_once(e, nullptr);
+}
+
 }  // namespace sp2b
 
 using namespace sp2b;
@@ -580,6 +622,8 @@ int sp2b_last_refinement_info(int* scale_exp, double* r2max) {
   return SP2B_OK;
 }
 
+int sp2b_last_exact_switch(void) { return t_exact_switch; }
+
 int sp2b_opts_default(sp2b_opts* o) {
   if (!o) return SP2B_BAD_ARG;
   memset(o, 0, sizeof(*o));
@@ -588,6 +632,7 @@ int sp2b_opts_default(sp2b_opts* o) {
   o->mixed_tol = 1e-3;
   o->mcweeny_products = SP2B_MCW_INT8;
   o->refine_tol = 1e-3;
+  o->exact_switch = 40;
   return SP2B_OK;
 }
 
@@ -636,6 +681,7 @@ static DenseJob base_job(const double* h, double* rho, int n, const sp2b_opts* o
   j.stream = (cudaStream_t)o->stream;
   j.mcweeny = o->mcweeny;
   j.mcweeny_products = o->mcweeny_products;
+  j.exact_switch = o->exact_switch;
   j.ctl.n = n;
   j.ctl.mixed_tol = o->mixed_tol;
   j.ctl.icount = 0;

@@ -762,3 +762,23 @@ extern "C" int sp2b_last_subgraph_refined(int* count, int* parts, int max_parts,
     for (int p = 0; p < nparts; ++p) idem[p] = p < (int)t_idem.size() ? t_idem[p] : 0.0;
   return SP2B_OK;
 }
+
+extern "C" int sp2b_place_core_rows(long long n, int nparts, const long long* halo_ptr,
+                                    const int* halo_idx, const int* llsize,
+                                    const long long* src_off, const double* src, double* rho,
+                                    void* stream) {
+  if (n <= 0 || nparts < 0 || (nparts > 0 && (!halo_ptr || !halo_idx || !llsize || !src_off ||
+                                              !src || !rho))) {
+    set_last_error("sp2b_place_core_rows: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    set_last_error("no CUDA device available");
+    return SP2B_NO_DEVICE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  SP2B_CUDA_TRY(launch_place_core(halo_ptr, halo_idx, llsize, src_off, nparts, src, rho, n, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return SP2B_OK;
+}

@@ -33,7 +33,8 @@ STATUS_NAMES = {0: "SP2B_OK", 1: "SP2B_NOT_CONVERGED", 2: "SP2B_BAD_ARG", 3: "SP
 class Opts(C.Structure):
     _fields_ = [("precision", C.c_int), ("mcweeny", C.c_int), ("mixed_tol", C.c_double),
                 ("device_ptrs", C.c_int), ("stream", C.c_void_p), ("verbose", C.c_int),
-                ("mcweeny_products", C.c_int), ("refine_tol", C.c_double)]
+                ("mcweeny_products", C.c_int), ("refine_tol", C.c_double),
+                ("exact_switch", C.c_int)]
 
 
 class SP2Error(RuntimeError):
@@ -100,6 +101,8 @@ _SIGS = {
     "sp2b_ellpack_to_csr": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp, C.c_longlong,
                                  C.POINTER(C.c_longlong), C.POINTER(Opts)]),
     "sp2b_launch_count": (C.c_longlong, []),
+    "sp2b_last_exact_switch": (_i, []),
+    "sp2b_place_core_rows": (_i, [C.c_longlong, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sp2b_last_refinement_info": (_i, [_ip, _dp]),
     "sp2b_compute_response_sp2": (_i, [_vp, _vp, _vp, _vp, _i, C.c_double, C.c_double, _i, _i,
                                        C.c_char_p, C.c_double, C.c_double, _i, _vp, _ip, _vp]),
@@ -170,11 +173,13 @@ def check(status: int, where: str):
 
 
 def make_opts(precision=PREC_FP64, mcweeny=1, mixed_tol=1e-3, device_ptrs=False, stream=None,
-              mcweeny_products=MCW_INT8, refine_tol=None):
+              mcweeny_products=MCW_INT8, refine_tol=None, exact_switch=None):
     o = Opts()
     lib().sp2b_opts_default(C.byref(o))
     if refine_tol is not None:
         o.refine_tol = refine_tol
+    if exact_switch is not None:
+        o.exact_switch = exact_switch
     o.precision = precision
     o.mcweeny = mcweeny
     o.mcweeny_products = mcweeny_products

@@ -86,7 +86,7 @@ def test_submatrix_fp64_parity(cuda, n, core):
     """prg_sp2_submatrix (src/prg_sp2_mod.F90:1190-1246): separate input block, output
     rho, vv accumulated over the first core_size rows (core_size 0 adds nothing)."""
     h = M.two_band_1d(n, seed=11)
-    g = O.sp2_alg2_genseq(h, 0.5, 0, 100, "None", 1e-10)
+    g = O.sp2_alg2_genseq(h, (n // 2) / n, 0, 100, "None", 1e-10)   # integer occupancy
     emin, emax = O.gershgorin(h)
     vv_ref = [0.25] * g.icount
     d_ref = O.sp2_submatrix(h, g.pp, g.icount, vv_ref, emin, emax, core)
@@ -218,6 +218,8 @@ def test_mixed_fp16_against_fp64(cuda, n):
     err = np.linalg.norm(got.rho - ref.rho) / n
     assert err <= 1e-6, err
     assert abs(np.trace(got.rho) - n) < 1e-5 * n
+    # a gapped spectrum stays in the split form (no hand-over to the exact INT8 form)
+    assert _lib.lib().sp2b_last_exact_switch() == 0
 
 
 def test_mixed_bf16_runs(cuda):
