@@ -24,9 +24,14 @@
 // Layout: the four planes of a ping-pong buffer are four packed R x ld byte arrays
 // (plane s at base + s R ld), so one TMA map over 4R rows covers them all.  Tiles are
 // 128 rows x 64 columns (the five accumulators take 5 x 64 TMEM columns) of the upper
-// part of each part's block: {row0, bi << 16 | bj64, K extent, core rows}.  Padding
-// rows and columns of a part hold X = 0, i.e. X' = -I/2 on the padding diagonal, which
-// the recursion keeps.
+// part of each part's block, {row0, bi << 16 | bj64, K extent, core rows}, with the K
+// extent n64 = the part size rounded up to 64 and no tile starting at or beyond it.
+// Padding rows and columns hold X = 0, i.e. X' = -I/2 on the padding diagonal; the
+// recursion keeps that for indices below n64 (their own square is in the K range), and
+// products with them add nothing to real entries (their off-diagonal entries stay 0).
+// Entries at or beyond n64 only reach output rows at or beyond n64, which nothing reads.
+// Only the tiles' entries are stored (the upper band: row r from column r & ~127 on);
+// operand blocks left of it are read from their mirrors, transposed by the MMA.
 #include "kernels_subgraph.cuh"
 #include "reduce.cuh"
 #include "tc_ptx.cuh"
@@ -35,22 +40,22 @@ namespace sp2b {
 namespace i8s {
 constexpr int BM = 128;                         // tile rows (TMEM lanes)
 constexpr int BN = 64;                          // tile columns
-constexpr int BK = 128;                         // K bytes per stage
+constexpr int BK = 64;                          // K bytes per stage (64-byte swizzle)
 constexpr int UK = 32;                          // K per kind::i8 MMA
 constexpr int ND = 4;                           // digit planes
 constexpr int NU = 5;                           // accumulators, u = s + t = 0..4
-constexpr int A_PLANE = BM * BK;                // 16 KB
-constexpr int B_PLANE = BN * BK;                // 8 KB
-constexpr int STAGE_BYTES = ND * (A_PLANE + B_PLANE);   // 96 KB
-constexpr int ST = 2;
+constexpr int A_PLANE = BM * BK;                // 8 KB
+constexpr int B_PLANE = BN * BK;                // 4 KB
+constexpr int STAGE_BYTES = ND * (A_PLANE + B_PLANE);   // 48 KB
+constexpr int ST = 4;
 constexpr int EPI_WARPS = 16;                   // 4 lane quarters x 4 groups of 16 columns
 constexpr int NWARP = 2 + EPI_WARPS;
 constexpr int NTHR = NWARP * 32;
-constexpr int SCR_WARP = 16 * 32;               // mirror staging, one plane at a time
-constexpr int SCR_OFF = ST * STAGE_BYTES;
-constexpr int SMEM_BYTES = SCR_OFF + EPI_WARPS * SCR_WARP + 1024;
-constexpr int TMEM_COLS = 512;                  // 5 x 64 used
-constexpr int SHIFT = 31;                       // M = rint(2^31 X')
+constexpr int OUT_PLANE = BM * BN;              // 8 KB: one plane of the output tile
+constexpr int OUT_OFF = ST * STAGE_BYTES;       // output tile staging (64-byte swizzle)
+constexpr int SMEM_BYTES = OUT_OFF + ND * OUT_PLANE + 1024;
+constexpr int TMEM_COLS = 512;
+static_assert(NU * BN <= TMEM_COLS, "the five accumulators fit the TMEM allocation");
 }  // namespace i8s
 
 // The thirteen plane products (s, t) with s + t <= 4, grouped by u = s + t; product q
@@ -93,7 +98,7 @@ __device__ __forceinline__ I8Tile i8_tile(const StepArgs& p, int t) {
   ti.i0 = (v.y >> 16) * i8s::BM;
   ti.j0 = (v.y & 0xffff) * i8s::BN;
   ti.core = v.w;
-  ti.ok = ti.i0 < v.z && ti.j0 < v.z && v.z % i8s::BK == 0;
+  ti.ok = ti.i0 < v.z && ti.j0 < v.z && v.z % i8s::BK == 0;   // z: K extent, multiple of 64
   ti.kb = ti.ok ? v.z / i8s::BK : 0;
   return ti;
 }
@@ -116,11 +121,36 @@ __device__ __forceinline__ int i8_value(int8_t d0, int8_t d1, int8_t d2, int8_t 
   return (((int)d0 * 256 + (int)d1) * 256 + (int)d2) * 256 + (int)d3;
 }
 
+// Named barrier 1 over the 16 epilogue warps (512 threads), and its AND-reduction form.
+__device__ __forceinline__ void epi_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(i8s::EPI_WARPS * 32) : "memory");
+}
+__device__ __forceinline__ bool epi_all(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred a, b;\n\t"
+      "setp.ne.u32 a, %1, 0;\n\t"
+      "bar.red.and.pred b, 1, %2, a;\n\t"
+      "selp.u32 %0, 1, 0, b;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(i8s::EPI_WARPS * 32)
+      : "memory");
+  return r != 0;
+}
+
 // One SP2 step of every part: out = branch(in) in digit form.  A = B = E = in (4 planes),
 // out: the other buffer.  warp 0: TMA producer; warp 1: TMEM owner and MMA issuer;
 // warps 2..17: epilogue (warp w reads TMEM lane quarter w & 3, columns 16 ((w - 2) >> 2)..).
+//
+// Only the upper band of each part is stored: row r holds valid entries in the columns
+// from its 128-row block's first row, c >= (r & ~127), which are exactly the entries of
+// the tiles this kernel writes (bj >= 2 bi).  An operand block left of that (k-block
+// before the block's first row) is read from its mirror X[k, i] = X[i, k] in MN-major
+// form: A^T as a 64 x 128-byte box (128-byte swizzle), B^T as a 64 x 64-byte box.
+// The new tile is staged in shared memory and written by four TMA stores (one per plane).
 __global__ void __launch_bounds__(i8s::NTHR, 1)
-    k_i8_batch(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+    k_i8_batch(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_at,
+               const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_o,
                const StepArgs p, long long rows, int ntiles) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[i8s::ST];
@@ -128,6 +158,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
   __shared__ __align__(8) uint64_t bar_tfull;
   __shared__ __align__(8) uint64_t bar_tempty;
   __shared__ __align__(8) uint64_t bar_final;
+  __shared__ __align__(8) uint64_t bar_xk;    // X_k tile staged for the epilogue
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
@@ -150,6 +181,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
     mbar_init(smem_u32(&bar_tfull), 1);
     mbar_init(smem_u32(&bar_tempty), i8s::EPI_WARPS);
     mbar_init(smem_u32(&bar_final), 1);
+    mbar_init(smem_u32(&bar_xk), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), i8s::TMEM_COLS);
@@ -169,6 +201,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       uint32_t g = 0;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const I8Tile ti = i8_tile(p, t);
+        const int jb = ti.j0 & ~(i8s::BM - 1);   // first row of the block holding B's rows
         for (int kb = 0; kb < ti.kb; ++kb, ++g) {
           const int s = g % i8s::ST;
           const uint32_t u = g / i8s::ST;
@@ -176,14 +209,20 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
             ok = false;
             break;
           }
+          const int k0 = kb * i8s::BK;
+          const bool at = k0 < ti.i0, bt = k0 < jb;
           const uint32_t fb = smem_u32(&bar_full[s]);
           const uint32_t st = sbase + s * i8s::STAGE_BYTES;
           mbar_expect_tx(fb, i8s::STAGE_BYTES);
 #pragma unroll
           for (int d = 0; d < i8s::ND; ++d) {
-            tma_load_2d(st + d * i8s::A_PLANE, &tm_a, fb, kb * i8s::BK, d * R + ti.row0 + ti.i0);
-            tma_load_2d(st + i8s::ND * i8s::A_PLANE + d * i8s::B_PLANE, &tm_b, fb, kb * i8s::BK,
-                        d * R + ti.row0 + ti.j0);
+            const int pr = d * R + ti.row0;
+            if (at)
+              tma_load_2d(st + d * i8s::A_PLANE, &tm_at, fb, ti.i0, pr + k0);
+            else
+              tma_load_2d(st + d * i8s::A_PLANE, &tm_a, fb, k0, pr + ti.i0);
+            tma_load_2d(st + i8s::ND * i8s::A_PLANE + d * i8s::B_PLANE, &tm_b, fb,
+                        bt ? ti.j0 : k0, pr + (bt ? k0 : ti.j0));
           }
           issued_phase[s] = u & 1;
         }
@@ -199,12 +238,13 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
   } else if (warp == 1) {
     if (lane == 0) {
       // ---------------- MMA issuer ----------------
-      constexpr uint32_t idesc = make_idesc_s8(i8s::BM, i8s::BN);
+      constexpr uint32_t idesc0 = make_idesc_s8(i8s::BM, i8s::BN);
       bool ok = true;
       uint32_t g = 0, tl = 0;
       for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const I8Tile ti = i8_tile(p, t);
         if (!ti.ok) continue;
+        const int jb = ti.j0 & ~(i8s::BM - 1);
         // the accumulators are single-buffered: wait until the epilogue has read the
         // previous tile's
         if (tl >= 1 && !mbar_wait(smem_u32(&bar_tempty), (tl - 1) & 1, &s_abort)) {
@@ -219,17 +259,27 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
             break;
           }
           tc_fence_after();
+          const int k0 = kb * i8s::BK;
+          const bool at = k0 < ti.i0, bt = k0 < jb;
+          // instruction descriptor with the MN-major bits (15: A, 16: B) of this k-block
+          const uint32_t idesc = idesc0 | (at ? 1u << 15 : 0u) | (bt ? 1u << 16 : 0u);
           const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+          // descriptors of plane 0 (a one-atom-wide MN-major tile has the same fields as
+          // the K-major one of its swizzle); plane p starts p * plane bytes further, and
+          // k advances by 32: 32 bytes K-major, 32 rows MN-major (in 16-byte units)
+          const uint64_t da0 = at ? sw128_desc(st) : sw64_desc(st);
+          const uint64_t db0 = sw64_desc(st + i8s::ND * i8s::A_PLANE);
+          const uint32_t ka = at ? (32u * 128u) >> 4 : 32u >> 4;
+          const uint32_t kb16 = bt ? (32u * 64u) >> 4 : 32u >> 4;
 #pragma unroll
           for (int kk = 0; kk < i8s::BK / i8s::UK; ++kk) {
-            const uint64_t off = (uint64_t)((kk * i8s::UK) >> 4);
 #pragma unroll
             for (int q = 0; q < 13; ++q) {
               const int sa = i8_pa(q), sb = i8_pb(q);
               // the first product of each u at k = 0 starts its accumulator
-              const uint64_t da = sw128_desc(st + sa * i8s::A_PLANE) + off;
-              const uint64_t db = sw128_desc(st + i8s::ND * i8s::A_PLANE + sb * i8s::B_PLANE) + off;
-              umma_i8(tmem + (sa + sb) * i8s::BN, da, db, idesc,
+              umma_i8(tmem + (sa + sb) * i8s::BN,
+                      da0 + (uint64_t)(sa * (i8s::A_PLANE >> 4) + kk * ka),
+                      db0 + (uint64_t)(sb * (i8s::B_PLANE >> 4) + kk * kb16), idesc,
                       (kb > 0 || kk > 0 || !i8_first(q)) ? 1u : 0u);
             }
           }
@@ -250,95 +300,190 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
     const int q = warp & 3;                   // TMEM lane quarter
     const int grp = (warp - 2) >> 2;          // 16-column group of the 64-column tile
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    const int ld = p.ld;
-    const size_t plane = (size_t)R * ld;
-    const int8_t* X = (const int8_t*)p.A;
-    int8_t* O = (int8_t*)p.out;
-    uint8_t* scr = smem + i8s::SCR_OFF + (warp - 2) * i8s::SCR_WARP;
-    uint32_t tl = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      const I8Tile ti = i8_tile(p, t);
-      if (!ti.ok) continue;
-      const int rl = q * 32 + lane;             // row inside the tile
-      const int r = ti.i0 + rl;                 // row inside the part
-      const int c0 = ti.j0 + grp * 16;          // first column of this thread's 16
-      const size_t rowoff = ((size_t)ti.row0 + r) * ld + c0;
-      // X_k digits of this thread's 16 elements (read before the accumulators are ready)
-      uint4 xd[i8s::ND];
+    // One thread stages each tile's X_k in shared memory (a TMA load into the output
+    // staging buffer, one tile ahead) and writes X_{k+1} back from the same buffer.
+    const bool storer = warp == 2 && lane == 0;
+    // this thread's 16 bytes of each staged plane: row q * 32 + lane, 16-byte chunk grp
+    // under the 64-byte swizzle (chunk ^ (row >> 1) & 3)
+    const int rl = q * 32 + lane;
+    uint8_t* stg = smem + i8s::OUT_OFF + rl * 64 + ((grp ^ ((rl >> 1) & 3)) << 4);
+    const int sg = (int)sgn;
+    auto next_valid = [&](int t) {
+      while (t < ntiles && !i8_tile(p, t).ok) t += gridDim.x;
+      return t;
+    };
+    auto load_xk = [&](int t) {
+      const I8Tile tn = i8_tile(p, t);
+      const uint32_t xb = smem_u32(&bar_xk);
+      mbar_expect_tx(xb, i8s::ND * i8s::OUT_PLANE);
 #pragma unroll
       for (int d = 0; d < i8s::ND; ++d)
-        xd[d] = *reinterpret_cast<const uint4*>(X + d * plane + rowoff);
-      if (!mbar_wait_idle(smem_u32(&bar_tfull), tl & 1, &s_abort)) break;
+        tma_load_2d(sbase + i8s::OUT_OFF + d * i8s::OUT_PLANE, &tm_a, xb, tn.j0,
+                    d * R + tn.row0 + tn.i0);
+    };
+    uint32_t tl = 0;
+    bool xk_pending = false;   // a staging load in flight (phase tl & 1)
+    int t = next_valid(blockIdx.x);
+    if (storer && t < ntiles) {
+      load_xk(t);
+      xk_pending = true;
+    }
+    while (t < ntiles) {
+      const I8Tile ti = i8_tile(p, t);
+      const int r = ti.i0 + rl;                 // row inside the part
+      const int c0 = ti.j0 + grp * 16;          // first column of this thread's 16
+      bool ok = mbar_wait_idle(smem_u32(&bar_tfull), tl & 1, &s_abort) &&
+                mbar_wait(smem_u32(&bar_xk), tl & 1, &s_abort);
+      // every epilogue thread takes the same exit (the named barriers below need all 512)
+      if (!epi_all(ok)) break;
+      xk_pending = false;
       tc_fence_after();
-      long long P[16];
+      uint4 xd[i8s::ND];   // X_k digits of this thread's 16 elements
+#pragma unroll
+      for (int d = 0; d < i8s::ND; ++d) xd[d] = *reinterpret_cast<const uint4*>(stg + d * i8s::OUT_PLANE);
+      // Q = rint(2^31 X'^2) = floor((P + 2^14) / 2^15), P = sum_u A_u 2^{32 - 8u}, in 32-bit
+      // steps: with s3 = A_3 + (A_4 >> 8) and s2 = A_2 + (s3 >> 8),
+      //   P = 2^16 S + R,  S = 2^16 A_0 + 2^8 A_1 + s2,  R = 2^8 (s3 & 255) + (A_4 & 255),
+      // so Q = 2 S + floor((R + 2^14) / 2^15).  S is formed modulo 2^32; its true value
+      // fits (|Q| <= 2^29 since |X'^2| <= 1/4), so the wrapped sum is exact.  The low pair
+      // is read first and folded into e = 2 (s3 >> 8) + floor((R + 2^14) / 2^15); the
+      // other three are read together and the accumulators released before the sum.
+      int Q[16];
       {
-        uint32_t acc[16];
         const uint32_t ta = tmem + lane_base + grp * 16;
-        tmem_ld16(ta, acc);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 16; ++j) P[j] = (long long)(int)acc[j] * (1ll << 32);
-#pragma unroll
-        for (int u = 1; u < i8s::NU; ++u) {
-          tmem_ld16(ta + u * i8s::BN, acc);
+        int e[16];
+        {
+          uint32_t a4[16], a3[16];
+          tmem_ld16(ta + 4 * i8s::BN, a4);
+          tmem_ld16(ta + 3 * i8s::BN, a3);
           tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 16; ++j) P[j] += (long long)(int)acc[j] * (1ll << (32 - 8 * u));
+          for (int j = 0; j < 16; ++j) {
+            const int s3 = (int)a3[j] + ((int)a4[j] >> 8);
+            const int rr = ((s3 & 255) << 8) + (int)(a4[j] & 255u);
+            e[j] = 2 * (s3 >> 8) + ((rr + (1 << 14)) >> 15);
+          }
         }
+        uint32_t a2[16], a1[16], a0[16];
+        tmem_ld16(ta + 2 * i8s::BN, a2);
+        tmem_ld16(ta + i8s::BN, a1);
+        tmem_ld16(ta, a0);
+        tmem_wait_ld();
+        tc_fence_before();   // TMEM reads ordered before the release
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&bar_tempty));
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          Q[j] = (int)(2u * ((a0[j] << 16) + (a1[j] << 8) + a2[j]) + (uint32_t)e[j]);
       }
-      tc_fence_before();   // TMEM reads ordered before the release
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&bar_tempty));
-      ++tl;
+      const int tn = next_valid(t + gridDim.x);
 
-      uint4 nd[i8s::ND];
+      // Rows whose 16 columns all lie above the diagonal and on one side of the core
+      // boundary weigh every element the same: the residual is summed once and scaled.
+      const bool above = c0 > ti.i0 + q * 32 + 31;
+      const bool cuni = above && (ti.core <= 0 || c0 + 15 < ti.core || c0 >= ti.core);
+      const int cw_row = ti.core <= 0 ? 2 : (r < ti.core ? 1 : 0) + (c0 < ti.core ? 1 : 0);
+      float s_res = 0.f;
+      double s_tr = 0.0, s_trp = 0.0;
+      uint32_t wn[16];   // X_{k+1} of each element: its four digit bytes (plane 0 lowest)
 #pragma unroll
-      for (int d = 0; d < i8s::ND; ++d) nd[d] = make_uint4(0u, 0u, 0u, 0u);
-      double s_res = 0.0, s_tr = 0.0, s_trp = 0.0;
+      for (int g = 0; g < 4; ++g) {
+        // element-major words of X_k for elements 4g..4g+3: bytes [d3, d2, d1, d0] of
+        // each element gathered from the four planes (a 4 x 4 byte transpose)
+        const uint32_t p0 = g == 0 ? xd[0].x : g == 1 ? xd[0].y : g == 2 ? xd[0].z : xd[0].w;
+        const uint32_t p1 = g == 0 ? xd[1].x : g == 1 ? xd[1].y : g == 2 ? xd[1].z : xd[1].w;
+        const uint32_t p2 = g == 0 ? xd[2].x : g == 1 ? xd[2].y : g == 2 ? xd[2].z : xd[2].w;
+        const uint32_t p3 = g == 0 ? xd[3].x : g == 1 ? xd[3].y : g == 2 ? xd[3].z : xd[3].w;
+        const uint32_t alo = __byte_perm(p3, p2, 0x5140u), ahi = __byte_perm(p3, p2, 0x7362u);
+        const uint32_t blo = __byte_perm(p1, p0, 0x5140u), bhi = __byte_perm(p1, p0, 0x7362u);
+        uint32_t u4[4];
+        u4[0] = __byte_perm(alo, blo, 0x5410u);
+        u4[1] = __byte_perm(alo, blo, 0x7632u);
+        u4[2] = __byte_perm(ahi, bhi, 0x5410u);
+        u4[3] = __byte_perm(ahi, bhi, 0x7632u);
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int c = c0 + j;
-        const bool dg = r == c;
-        const long long m = (long long)((((i8_byte(xd[0], j) * 256 + i8_byte(xd[1], j)) * 256 +
-                                          i8_byte(xd[2], j)) * 256) + i8_byte(xd[3], j));
-        const long long qv = (P[j] + (1ll << 14)) >> 15;            // rint(2^31 X'^2)
-        const long long mn = m + sgn * qv - (dg ? sgn * (1ll << 29) : 0ll);
-        int8_t b0, b1, b2, b3;
-        i8_digits((int)mn, b0, b1, b2, b3);
-        i8_put(nd[0], j, b0);
-        i8_put(nd[1], j, b1);
-        i8_put(nd[2], j, b2);
-        i8_put(nd[3], j, b3);
-        // weight of (r, c) in the full-matrix sums: itself and its mirror above the
-        // diagonal, once on it, nothing below it (the mirror of another tile carries it)
-        const int w = r < c ? 2 : (dg ? 1 : 0);
-        const int cw = core_weight(w, r, c, ti.core);
-        const double res = (double)((dg ? (1ll << 44) : 0ll) - P[j]);   // 2^46 (X - X^2)
-        s_res = fma((double)cw * res, res, s_res);
-        if (dg) {
-          s_tr += (double)mn * 0x1p-31 + 0.5;
-          s_trp += (double)P[j] * 0x1p-46 + (double)m * 0x1p-31 + 0.25;   // Tr X^2
+        for (int e = 0; e < 4; ++e) {
+          const int j = 4 * g + e;
+          const int c = c0 + j;
+          const bool dg = r == c;
+          // M = d0 2^24 + d1 2^16 + d2 2^8 + d3 with signed digits: the bytes read as one
+          // int, less 2^8 of the next place for each negative lower digit
+          const uint32_t uv = u4[e];
+          const int m = (int)uv - (int)((uv & 0x00808080u) << 1);
+          const int mn = m + sg * Q[j] - (dg ? sg * (1 << 29) : 0);
+          // balanced base-256 digits of M_{k+1}: each digit's byte is the low byte of the
+          // running quotient
+          const int m1 = (mn + 128) >> 8;
+          const int m2 = (m1 + 128) >> 8;
+          const int d0 = max(-127, min(127, (m2 + 128) >> 8));
+          const uint32_t lo = __byte_perm((uint32_t)d0, (uint32_t)m2, 0x0040u);
+          const uint32_t hi = __byte_perm((uint32_t)m1, (uint32_t)mn, 0x0040u);
+          wn[j] = __byte_perm(lo, hi, 0x5410u);
+          // 2^31 (X - X^2) = 2^31 (I/4 - X'^2), from the rounded square
+          const float res = (float)((dg ? (1 << 29) : 0) - Q[j]);
+          if (cuni) {
+            s_res = fmaf(res, res, s_res);
+          } else {
+            // weight of (r, c) in the full-matrix sums: itself and its mirror above the
+            // diagonal, once on it, nothing below it (its mirror above carries it)
+            const int w = r < c ? 2 : (dg ? 1 : 0);
+            s_res = fmaf((float)core_weight(w, r, c, ti.core) * res, res, s_res);
+            if (dg) {
+              s_tr += (double)mn * 0x1p-31 + 0.5;
+              s_trp += (double)Q[j] * 0x1p-31 + (double)m * 0x1p-31 + 0.25;   // Tr X^2
+            }
+          }
         }
       }
       sums[1] += s_tr;
-      sums[2] = fma(s_res, 0x1p-92, sums[2]);
+      sums[2] = fma((double)(cuni ? (float)cw_row * s_res : s_res), 0x1p-62, sums[2]);
       sums[3] += s_trp;
-      // X_{k+1}: this thread's 16 bytes per plane, and the warp's 32 x 16 block mirrored
-      // (rows c0.., columns of this warp's 32 rows) through shared memory.  Mirror values
-      // that land on or above the diagonal equal the ones stored there directly (the
-      // integer products are exactly symmetric), so no element needs masking.
+      // X_{k+1}: this thread's 16 bytes of each plane, from its element-major words
+      auto planes = [](const uint32_t (&w)[16], uint4 (&pl)[i8s::ND]) {
+        uint32_t o[i8s::ND][4];
 #pragma unroll
-      for (int d = 0; d < i8s::ND; ++d) {
-        *reinterpret_cast<uint4*>(O + d * plane + rowoff) = nd[d];
+        for (int g = 0; g < 4; ++g) {
+          const uint32_t alo = __byte_perm(w[4 * g], w[4 * g + 1], 0x5140u);
+          const uint32_t ahi = __byte_perm(w[4 * g], w[4 * g + 1], 0x7362u);
+          const uint32_t blo = __byte_perm(w[4 * g + 2], w[4 * g + 3], 0x5140u);
+          const uint32_t bhi = __byte_perm(w[4 * g + 2], w[4 * g + 3], 0x7362u);
+          o[0][g] = __byte_perm(alo, blo, 0x5410u);
+          o[1][g] = __byte_perm(alo, blo, 0x7632u);
+          o[2][g] = __byte_perm(ahi, bhi, 0x5410u);
+          o[3][g] = __byte_perm(ahi, bhi, 0x7632u);
+        }
 #pragma unroll
-        for (int j = 0; j < 16; ++j) scr[j * 32 + lane] = (uint8_t)i8_byte(nd[d], j);
-        __syncwarp();
-        const int jj = lane >> 1, hf = lane & 1;
-        const uint4 v = *reinterpret_cast<const uint4*>(scr + jj * 32 + hf * 16);
-        *reinterpret_cast<uint4*>(O + d * plane + ((size_t)ti.row0 + c0 + jj) * ld + ti.i0 +
-                                  q * 32 + hf * 16) = v;
-        __syncwarp();
+        for (int d = 0; d < i8s::ND; ++d) pl[d] = make_uint4(o[d][0], o[d][1], o[d][2], o[d][3]);
+      };
+      {
+        uint4 pl[i8s::ND];
+        planes(wn, pl);
+#pragma unroll
+        for (int d = 0; d < i8s::ND; ++d) *reinterpret_cast<uint4*>(stg + d * i8s::OUT_PLANE) = pl[d];
       }
+      fence_proxy_async_smem();   // staged bytes visible to the TMA stores
+      epi_sync();
+      if (storer) {
+#pragma unroll
+        for (int d = 0; d < i8s::ND; ++d)
+          tma_store_2d(&tm_o, sbase + i8s::OUT_OFF + d * i8s::OUT_PLANE, ti.j0,
+                       d * R + ti.row0 + ti.i0);
+        bulk_commit();
+        // the next tile's X_k goes into the buffer once the stores have read it
+        if (tn < ntiles) {
+          bulk_wait_read0();
+          load_xk(tn);
+          xk_pending = true;
+        }
+      }
+      ++tl;
+      t = tn;
+    }
+    if (storer) {
+      bulk_wait0();
+      if (xk_pending)   // abandoned after an abort: let the copy land before exit (bounded)
+        for (uint32_t i = 0; i < kSpinLimit; ++i)
+          if (mbar_try(smem_u32(&bar_xk), tl & 1)) break;
     }
   }
   tc_fence_before();
@@ -350,18 +495,22 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
 }
 
 cudaError_t launch_i8_batched(const StepArgs& a, long long rows, cudaStream_t st) {
-  if (!a.tiles || a.ntiles <= 0 || a.ld % i8s::BK != 0 || rows % i8s::BM != 0 || !a.A ||
-      !a.out || 4 * rows > 0x7fffffffLL)
+  if (!a.tiles || a.ntiles <= 0 || a.ld % 128 != 0 || rows % i8s::BM != 0 || !a.A || !a.out ||
+      4 * rows > 0x7fffffffLL)
     return cudaErrorInvalidValue;
-  CUtensorMap ma, mb;
-  if (!make_tmap_box(&ma, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BM) ||
-      !make_tmap_box(&mb, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BN))
+  // operand maps over the input's 4R rows (K-major A, MN-major A^T, B and B^T) and the
+  // store map over the output's
+  CUtensorMap ma, mat, mb, mo;
+  if (!make_tmap_u8_sw64(&ma, a.A, 4 * rows, a.ld, a.ld, i8s::BM) ||
+      !make_tmap_box(&mat, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BK) ||
+      !make_tmap_u8_sw64(&mb, a.A, 4 * rows, a.ld, a.ld, i8s::BN) ||
+      !make_tmap_u8_sw64(&mo, a.out, 4 * rows, a.ld, a.ld, i8s::BM))
     return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_i8_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        i8s::SMEM_BYTES);
   if (e != cudaSuccess) return e;
   const int grid = std::min(a.ntiles, device_sms());
-  k_i8_batch<<<grid, i8s::NTHR, i8s::SMEM_BYTES, st>>>(ma, mb, a, rows, a.ntiles);
+  k_i8_batch<<<grid, i8s::NTHR, i8s::SMEM_BYTES, st>>>(ma, mat, mb, mo, a, rows, a.ntiles);
   note_launch();
   return cudaGetLastError();
 }
@@ -454,6 +603,13 @@ __global__ void k_norm_digits(const double* __restrict__ xs, const int* __restri
   }
 }
 
+// Offset of entry (r, c) of a part in the upper-band storage the step kernel keeps: row r
+// holds the columns from its 128-row block's first row on; the rest is read from the
+// mirror (c, r).
+__device__ __forceinline__ size_t i8_band_off(long long row0, int r, int c, int ld) {
+  return c >= (r & ~(i8s::BM - 1)) ? ((size_t)row0 + r) * ld + c : ((size_t)row0 + c) * ld + r;
+}
+
 // rho (core rows) = 2 X = 2^-30 M + I.
 __global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
                                  const PartDesc* __restrict__ parts, const int* __restrict__ halo,
@@ -466,7 +622,7 @@ __global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
   for (long long q = (long long)blockIdx.y * blockDim.x + threadIdx.x; q < total;
        q += (long long)gridDim.y * blockDim.x) {
     const int r = (int)(q / P.n), c = (int)(q % P.n);
-    const size_t src = ((size_t)P.row0 + r) * ld + c;
+    const size_t src = i8_band_off(P.row0, r, c, ld);
     const int m = i8_value(dig[src], dig[plane + src], dig[2 * plane + src], dig[3 * plane + src]);
     const double v = (double)m * 0x1p-30 + (r == c ? 1.0 : 0.0);
     if (core_out) core_out[P.coff + q] = v;
@@ -474,7 +630,8 @@ __global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
   }
 }
 
-// Sum over each part's core rows of (X - X^2)_ii = X_ii - sum_j X_ij^2, from the digits.
+// Sum over each part's core rows of (X - X^2)_ii = X_ii - sum_j X_ij^2, from the digits
+// (upper-band storage).
 __global__ void k_part_idem_digits(const int8_t* __restrict__ dig, long long rows,
                                    const PartDesc* __restrict__ parts, int ld,
                                    double* __restrict__ out) {
@@ -485,7 +642,15 @@ __global__ void k_part_idem_digits(const int8_t* __restrict__ dig, long long row
   double s = 0.0;
   for (int r = blockIdx.y * nw + warp; r < P.ncore; r += gridDim.y * nw) {
     const size_t row = ((size_t)P.row0 + r) * ld;
-    for (int c0 = lane * 16; c0 < P.np; c0 += 512) {
+    // columns left of the row's block from their mirrors (off the diagonal)
+    const int rb = r & ~(i8s::BM - 1);
+    for (int c = lane; c < rb; c += 32) {
+      const size_t o = ((size_t)P.row0 + c) * ld + r;
+      const double x = (double)i8_value(dig[o], dig[plane + o], dig[2 * plane + o], dig[3 * plane + o]) *
+                       0x1p-31;
+      s -= x * x;
+    }
+    for (int c0 = rb + lane * 16; c0 < P.np; c0 += 512) {
       uint4 v[4];
 #pragma unroll
       for (int d = 0; d < 4; ++d) v[d] = *reinterpret_cast<const uint4*>(dig + d * plane + row + c0);

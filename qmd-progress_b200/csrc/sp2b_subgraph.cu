@@ -215,11 +215,12 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       // a part without core rows contributes to neither rho nor vv: no tiles
       if (P[p].ncore <= 0) continue;
       if (dig) {
-        // 128 x 64 tiles that reach the diagonal or lie above it; K over the whole
-        // padded block (the padding diagonal holds X' = -1/2, not zero)
-        for (int bi = 0; bi < P[p].np / 128; ++bi)
-          for (int bj = 2 * bi; bj < P[p].np / 64; ++bj)
-            tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj, P[p].np, P[p].ncore));
+        // 128 x 64 tiles that reach the diagonal or lie above it, inside the part size
+        // rounded up to 64 (also the K extent)
+        const int n64 = (P[p].n + 63) / 64 * 64;
+        for (int bi = 0; bi * 128 < n64; ++bi)
+          for (int bj = 2 * bi; bj * 64 < n64; ++bj)
+            tiles.push_back(make_int4((int)P[p].row0, (bi << 16) | bj, n64, P[p].ncore));
         continue;
       }
       const int T = P[p].np / bt;
@@ -428,6 +429,9 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
           (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
         return e;
       if (dig) {
+        // the second buffer's entries outside the written band (columns past a part's
+        // tiles) are read as zero padding by the mirrored operand loads
+        if ((e = cudaMemsetAsync(b.dig[1], 0, 4 * packed, cap)) != cudaSuccess) return e;
         if (fused) {
           if ((e = launch_extract_digits(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey,
                                          b.sval, ld, rows, j.mineval, j.maxeval, b.dig[0], cap)) !=

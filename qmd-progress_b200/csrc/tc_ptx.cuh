@@ -124,6 +124,51 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// Warp-wide forms: every lane of the warp executes them with the same operands (so they
+// stay warp-uniform) and the instruction is issued by the lanes with `issue` set (one).
+__device__ __forceinline__ void umma_i8_if(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "setp.ne.b32 q, %5, 0;\n\t"
+      "@q tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(issue)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit_if(uint32_t mbar, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %1, 0;\n\t"
+      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(
+          mbar),
+      "r"(issue)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d_if(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
+                                               int x, int y, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %5, 0;\n\t"
+      "@q cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];\n\t}\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(mbar), "r"(x), "r"(y), "r"(issue)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx_if(uint32_t a, uint32_t bytes, uint32_t issue) {
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.ne.b32 q, %2, 0;\n\t"
+      "@q mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t}\n" ::"r"(a),
+      "r"(bytes), "r"(issue)
+      : "memory");
+}
+// Bounded wait by a whole warp: every lane polls (so the issuing lane has observed the
+// phase), and the warp proceeds only if all lanes saw it.
+__device__ __forceinline__ bool mbar_wait_warp(uint32_t a, uint32_t parity, volatile int* abort_flag) {
+  const bool ok = mbar_wait(a, parity, abort_flag);
+  return __all_sync(0xffffffffu, ok) != 0;
+}
 __device__ __forceinline__ void umma_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    mbar)
@@ -227,6 +272,16 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   d |= (uint64_t)2u << 61;
   return d;
 }
+// K-major operand tile, 64-byte swizzle: 64-byte rows, 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(512u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)4u << 61;
+  return d;
+}
 // kind::f16 instruction descriptor: FP32 accumulate, A/B K-major, M x N.
 __host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, int M, int N) {
   return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) |
@@ -283,6 +338,20 @@ static bool make_tmap_box(CUtensorMap* tm, const void* base, long long rows, lon
                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   CUresult r = fn(tm, dt, 2, const_cast<void*>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+// 8-bit map with 64-byte boxes and the 64-byte swizzle (box of box_rows rows x 64 bytes).
+static bool make_tmap_u8_sw64(CUtensorMap* tm, const void* base, long long rows, long long cols,
+                              long long ld, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld};
+  cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box,
+                  es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }

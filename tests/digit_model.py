@@ -3,7 +3,8 @@
 The GPU form holds X' = X - I/2 as M = rint(2^31 X') in four balanced base-256 digits,
 forms P = 2^46 X'^2 from the thirteen exact digit products with s + t <= 4, and applies
 M <- M + sgn rint(P / 2^15) - sgn 2^29 [i == j] (sgn = +1 for X^2, -1 for 2X - X^2).
-Every step is integer arithmetic, so this model and the GPU must agree bit for bit.
+Every step is integer arithmetic, so this model and the GPU must agree bit for bit (the
+vv sums, formed from the rounded square in FP32 on the GPU, to FP32 summation).
 X0 is formed as the GPU forms it: x = alpha h (+ beta on the diagonal), then x - 1/2 on
 the diagonal, each a separately rounded FP64 operation.
 """
@@ -44,10 +45,10 @@ def step(M, branch):
             if 0 <= t < 4:
                 A += d[s] @ d[t]
         P += A.astype(np.int64) << (32 - 8 * u)
-    res = (np.eye(npad, dtype=np.int64) << 44) - P
-    rowsq = np.sum((res.astype(np.float64) * 2.0 ** -46) ** 2, axis=1)
     sg = 1 if branch else -1
-    Q = (P + (1 << 14)) >> 15
+    Q = (P + (1 << 14)) >> 15                       # rint(2^31 X'^2)
+    res = (np.eye(npad, dtype=np.int64) << 29) - Q  # 2^31 (X - X^2) from the rounded square
+    rowsq = np.sum((res.astype(np.float64) * 2.0 ** -31) ** 2, axis=1)
     return M + sg * Q - sg * (1 << 29) * np.eye(npad, dtype=np.int64), rowsq
 
 

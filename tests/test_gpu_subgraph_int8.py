@@ -2,7 +2,7 @@
 
 * Bit for bit against the host model of its integer arithmetic (tests/digit_model.py):
   every step is exact integer work, so the packed core rows are identical and the vv
-  sums agree to FP64 summation order.
+  sums agree to FP32 summation.
 * Against the FP64 oracle (prg_subgraphSP2Loop, src/prg_subgraphloop_mod.F90:36-126):
   within 1e-7 relative Frobenius on the gapped two-band model, also for ragged parts, a
   part without core rows and zero iterations.
@@ -43,7 +43,7 @@ def test_int8_subgraph_equals_digit_model(cuda, n, per):
         _, core, vv = sp2b.subgraph_sp2_loop(n, h_csr, hp, hi, lls, pp, maxiter, emin, emax,
                                              precision=I8, dense=False, core=True, refine_tol=0.0)
         assert np.array_equal(core, core_ref)
-        assert np.allclose(vv, np.sqrt(vv_ref), rtol=1e-12, atol=0)
+        assert np.allclose(vv, np.sqrt(vv_ref), rtol=1e-5, atol=1e-9)
 
 
 def test_int8_subgraph_close_to_oracle(cuda):
