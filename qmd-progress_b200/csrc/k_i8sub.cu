@@ -47,13 +47,15 @@ constexpr int NU = 5;                           // accumulators, u = s + t = 0..
 constexpr int A_PLANE = BM * BK;                // 8 KB
 constexpr int B_PLANE = BN * BK;                // 4 KB
 constexpr int STAGE_BYTES = ND * (A_PLANE + B_PLANE);   // 48 KB
-constexpr int ST = 4;
+constexpr int ST = 3;
 constexpr int EPI_WARPS = 16;                   // 4 lane quarters x 4 groups of 16 columns
-constexpr int NWARP = 2 + EPI_WARPS;
+constexpr int STORE_WARP = 2 + EPI_WARPS;       // TMA stores and completion signals
+constexpr int NWARP = 3 + EPI_WARPS;
 constexpr int NTHR = NWARP * 32;
 constexpr int OUT_PLANE = BM * BN;              // 8 KB: one plane of the output tile
-constexpr int OUT_OFF = ST * STAGE_BYTES;       // output tile staging (64-byte swizzle)
-constexpr int SMEM_BYTES = OUT_OFF + ND * OUT_PLANE + 1024;
+constexpr int OUT_BYTES = ND * OUT_PLANE;       // 32 KB: one staged tile (X_k in, X_{k+1} out)
+constexpr int OUT_OFF = ST * STAGE_BYTES;       // two staged tiles (64-byte swizzle)
+constexpr int SMEM_BYTES = OUT_OFF + 2 * OUT_BYTES + 1024;
 constexpr int TMEM_COLS = 512;
 static_assert(NU * BN <= TMEM_COLS, "the five accumulators fit the TMEM allocation");
 }  // namespace i8s
@@ -91,8 +93,7 @@ struct I8Tile {
   bool ok;
 };
 
-__device__ __forceinline__ I8Tile i8_tile(const StepArgs& p, int t) {
-  const int4 v = p.tiles[t];
+__device__ __forceinline__ I8Tile i8_tile_v(int4 v) {
   I8Tile ti;
   ti.row0 = v.x;
   ti.i0 = (v.y >> 16) * i8s::BM;
@@ -101,6 +102,16 @@ __device__ __forceinline__ I8Tile i8_tile(const StepArgs& p, int t) {
   ti.ok = ti.i0 < v.z && ti.j0 < v.z && v.z % i8s::BK == 0;   // z: K extent, multiple of 64
   ti.kb = ti.ok ? v.z / i8s::BK : 0;
   return ti;
+}
+__device__ __forceinline__ I8Tile i8_tile(const int4* tiles, int t) { return i8_tile_v(tiles[t]); }
+// The same read by a whole warp and broadcast from lane 0 (warp-uniform fields).
+__device__ __forceinline__ I8Tile i8_tile_uniform(const int4* tiles, int t) {
+  int4 v = tiles[t];
+  v.x = warp_uniform(v.x);
+  v.y = warp_uniform(v.y);
+  v.z = warp_uniform(v.z);
+  v.w = warp_uniform(v.w);
+  return i8_tile_v(v);
 }
 
 // Balanced base-256 digits of M (|M| < 2^31): d3, d2, d1 in [-128, 127], d0 the rest.
@@ -121,52 +132,65 @@ __device__ __forceinline__ int i8_value(int8_t d0, int8_t d1, int8_t d2, int8_t 
   return (((int)d0 * 256 + (int)d1) * 256 + (int)d2) * 256 + (int)d3;
 }
 
-// Named barrier 1 over the 16 epilogue warps (512 threads), and its AND-reduction form.
-__device__ __forceinline__ void epi_sync() {
-  asm volatile("bar.sync 1, %0;" ::"n"(i8s::EPI_WARPS * 32) : "memory");
-}
-__device__ __forceinline__ bool epi_all(bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred a, b;\n\t"
-      "setp.ne.u32 a, %1, 0;\n\t"
-      "bar.red.and.pred b, 1, %2, a;\n\t"
-      "selp.u32 %0, 1, 0, b;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v), "n"(i8s::EPI_WARPS * 32)
-      : "memory");
-  return r != 0;
+// Tensor maps of the two digit buffers (index: buffer), each over its 4R rows.
+struct I8Maps {
+  CUtensorMap a[2];    // K-major operand and staged tile: 64 bytes x 128 rows, 64-byte swizzle
+  CUtensorMap at[2];   // MN-major A^T: 128 bytes x 64 rows, 128-byte swizzle
+  CUtensorMap b[2];    // B and B^T: 64 bytes x 64 rows, 64-byte swizzle
+};
+
+// Bounded wait until a counter in global memory reaches `target` (acquire).
+__device__ __forceinline__ bool wait_count(const unsigned* c, unsigned target,
+                                           volatile int* abort_flag) {
+  for (uint32_t i = 0; i < kSpinLimit; ++i) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(c) : "memory");
+    if (v >= target) return true;
+    if ((i & 63u) == 63u && *abort_flag) return false;
+    __nanosleep(64);
+  }
+  *abort_flag = 1;
+  return false;
 }
 
-// One SP2 step of every part: out = branch(in) in digit form.  A = B = E = in (4 planes),
-// out: the other buffer.  warp 0: TMA producer; warp 1: TMEM owner and MMA issuer;
-// warps 2..17: epilogue (warp w reads TMEM lane quarter w & 3, columns 16 ((w - 2) >> 2)..).
+// All SP2 steps of every part in one persistent launch: out = branch(in) in digit form,
+// step after step, the two digit buffers alternating (step k reads buffer k & 1).
+// warp 0: TMA producer (operands and each tile's X_k); warp 1: TMEM owner and MMA
+// issuer; warps 2..17: epilogue (warp w reads TMEM lane quarter w & 3, columns
+// 16 ((w - 2) >> 2)..); warp 18: TMA stores of the finished tiles and their signals.
+//
+// Work items are (step k, tile t) in step-major order; CTA c takes items c, c + G, ...
+// A part's step-k tiles read only that part's step-(k-1) result, so the producer starts an
+// item once every tile of its part has finished the previous step: done[part] counts
+// finished tiles, signalled by the store warp once a tile's stores have landed (it waits
+// on nothing but its own CTA's epilogue).  Every CTA finishes its items in increasing
+// order and all CTAs are resident (cooperative launch), so the earliest unfinished item
+// never waits on an unfinished one.
 //
 // Only the upper band of each part is stored: row r holds valid entries in the columns
 // from its 128-row block's first row, c >= (r & ~127), which are exactly the entries of
 // the tiles this kernel writes (bj >= 2 bi).  An operand block left of that (k-block
 // before the block's first row) is read from its mirror X[k, i] = X[i, k] in MN-major
 // form: A^T as a 64 x 128-byte box (128-byte swizzle), B^T as a 64 x 64-byte box.
-// The new tile is staged in shared memory and written by four TMA stores (one per plane).
+// Each tile's X_k is loaded into one of two staging buffers (alternating per tile), the
+// epilogue overwrites it in place with X_{k+1}, and four TMA stores (one per plane)
+// write it back.
+//
+// Step sums (Tr X_{k+1}, ||X_k - X_k^2||_F^2 over the core rows, Tr X_k^2) are written per
+// (step, CTA, epilogue warp) to partials and reduced in a fixed order by k_i8_step_sums.
 __global__ void __launch_bounds__(i8s::NTHR, 1)
-    k_i8_batch(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_at,
-               const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_o,
-               const StepArgs p, long long rows, int ntiles) {
+    k_i8_steps(const __grid_constant__ I8Maps maps, const I8StepsArgs p) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[i8s::ST];
   __shared__ __align__(8) uint64_t bar_empty[i8s::ST];
   __shared__ __align__(8) uint64_t bar_tfull;
   __shared__ __align__(8) uint64_t bar_tempty;
   __shared__ __align__(8) uint64_t bar_final;
-  __shared__ __align__(8) uint64_t bar_xk;    // X_k tile staged for the epilogue
+  __shared__ __align__(8) uint64_t bar_xk[2];      // X_k staged (producer's copy landed)
+  __shared__ __align__(8) uint64_t bar_staged[2];  // X_{k+1} staged (all epilogue warps)
+  __shared__ __align__(8) uint64_t bar_free[2];    // staging read by the stores
   __shared__ uint32_t tmem_holder;
-  __shared__ double red[32 * 4];
-  __shared__ int s_flag;
   __shared__ volatile int s_abort;
-
-  const int br = control_prologue(p);
-  if (br < 0) return;
-  const long long sgn = br == BR_X2 ? 1 : -1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -181,96 +205,155 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
     mbar_init(smem_u32(&bar_tfull), 1);
     mbar_init(smem_u32(&bar_tempty), i8s::EPI_WARPS);
     mbar_init(smem_u32(&bar_final), 1);
-    mbar_init(smem_u32(&bar_xk), 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&bar_xk[b]), 1);
+      mbar_init(smem_u32(&bar_staged[b]), i8s::EPI_WARPS);
+      mbar_init(smem_u32(&bar_free[b]), 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_holder), i8s::TMEM_COLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = tmem_holder;
-  double sums[4] = {0.0, 0.0, 0.0, 0.0};
-  const int R = (int)rows;
+  const uint32_t tmem = (uint32_t)warp_uniform((int)tmem_holder);
+  const int R = p.rows;
+  const long long nitems = (long long)p.nsteps * p.ntiles;
+  const int G = gridDim.x;
+  // step and tile of item i
+  auto item_of = [&](long long i, int& k, int& t) {
+    k = (int)(i / p.ntiles);
+    t = (int)(i - (long long)k * p.ntiles);
+  };
+  // staging buffer b of the output tiles
+  auto stage_of = [&](int b) { return sbase + i8s::OUT_OFF + b * i8s::OUT_BYTES; };
 
+  // The producer and MMA roles run warp-wide: tile data is broadcast from lane 0, so loop
+  // bounds, descriptors and coordinates stay warp-uniform, and one elected lane issues.
   if (warp == 0) {
-    if (lane == 0) {
-      // ---------------- TMA producer ----------------
-      int issued_phase[i8s::ST];
-      for (int s = 0; s < i8s::ST; ++s) issued_phase[s] = -1;
-      bool ok = true;
-      uint32_t g = 0;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const I8Tile ti = i8_tile(p, t);
-        const int jb = ti.j0 & ~(i8s::BM - 1);   // first row of the block holding B's rows
-        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
-          const int s = g % i8s::ST;
-          const uint32_t u = g / i8s::ST;
-          if (g >= (uint32_t)i8s::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
-            ok = false;
-            break;
-          }
-          const int k0 = kb * i8s::BK;
-          const bool at = k0 < ti.i0, bt = k0 < jb;
-          const uint32_t fb = smem_u32(&bar_full[s]);
-          const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+    // ---------------- TMA producer ----------------
+    int issued_phase[i8s::ST];
+    for (int s = 0; s < i8s::ST; ++s) issued_phase[s] = -1;
+    int xk_phase[2] = {-1, -1};
+    bool ok = true;
+    uint32_t g = 0, tl = 0;
+    for (long long i = blockIdx.x; i < nitems && ok; i += G, ++tl) {
+      int k, t;
+      item_of(i, k, t);
+      const I8Tile ti = i8_tile_uniform(p.tiles, t);
+      // an item of step k > 0 starts once its part has finished step k - 1
+      bool dep = true;
+      if (k > 0) {
+        const int part = p.tpart[t];
+        dep = wait_count(p.done + part, (unsigned)k * (unsigned)p.pnt[part], &s_abort);
+      }
+      ok = ti.ok && __all_sync(0xffffffffu, dep);
+      if (!ok) break;
+      fence_proxy_async_global();   // the other CTAs' results, then the async-proxy reads
+      const CUtensorMap* ma = &maps.a[k & 1];
+      const CUtensorMap* mat = &maps.at[k & 1];
+      const CUtensorMap* mb = &maps.b[k & 1];
+      const int jb = ti.j0 & ~(i8s::BM - 1);   // first row of the block holding B's rows
+      for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+        const int s = g % i8s::ST;
+        const uint32_t u = g / i8s::ST;
+        if (g >= (uint32_t)i8s::ST && !mbar_wait_warp(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+          ok = false;
+          break;
+        }
+        const int k0 = kb * i8s::BK;
+        const bool at = k0 < ti.i0, bt = k0 < jb;
+        const uint32_t fb = smem_u32(&bar_full[s]);
+        const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+        if (elect_one()) {
           mbar_expect_tx(fb, i8s::STAGE_BYTES);
 #pragma unroll
           for (int d = 0; d < i8s::ND; ++d) {
             const int pr = d * R + ti.row0;
             if (at)
-              tma_load_2d(st + d * i8s::A_PLANE, &tm_at, fb, ti.i0, pr + k0);
+              tma_load_2d(st + d * i8s::A_PLANE, mat, fb, ti.i0, pr + k0);
             else
-              tma_load_2d(st + d * i8s::A_PLANE, &tm_a, fb, k0, pr + ti.i0);
-            tma_load_2d(st + i8s::ND * i8s::A_PLANE + d * i8s::B_PLANE, &tm_b, fb,
+              tma_load_2d(st + d * i8s::A_PLANE, ma, fb, k0, pr + ti.i0);
+            tma_load_2d(st + i8s::ND * i8s::A_PLANE + d * i8s::B_PLANE, mb, fb,
                         bt ? ti.j0 : k0, pr + (bt ? k0 : ti.j0));
           }
-          issued_phase[s] = u & 1;
         }
+        __syncwarp();
+        issued_phase[s] = u & 1;
       }
-      if (!ok) {  // abort: wait (bounded) for this CTA's copies still in flight
+      if (!ok) break;
+      // the tile's X_k into staging buffer tl & 1, once the stores of the tile that used
+      // it two items ago have read it
+      const int b = tl & 1;
+      if (tl >= 2 && !mbar_wait_warp(smem_u32(&bar_free[b]), ((tl - 2) >> 1) & 1, &s_abort)) {
+        ok = false;
+        break;
+      }
+      const uint32_t xb = smem_u32(&bar_xk[b]);
+      if (elect_one()) {
+        mbar_expect_tx(xb, i8s::OUT_BYTES);
+#pragma unroll
+        for (int d = 0; d < i8s::ND; ++d)
+          tma_load_2d(stage_of(b) + d * i8s::OUT_PLANE, ma, xb, ti.j0, d * R + ti.row0 + ti.i0);
+      }
+      __syncwarp();
+      xk_phase[b] = (tl >> 1) & 1;
+    }
+    if (!ok) {  // abort: wait (bounded) for this CTA's copies still in flight
+      s_abort = 1;
+      if (lane == 0) {
         for (int s = 0; s < i8s::ST; ++s)
           if (issued_phase[s] >= 0)
             for (uint32_t i = 0; i < kSpinLimit; ++i)
               if (mbar_try(smem_u32(&bar_full[s]), issued_phase[s])) break;
+        for (int b = 0; b < 2; ++b)
+          if (xk_phase[b] >= 0)
+            for (uint32_t i = 0; i < kSpinLimit; ++i)
+              if (mbar_try(smem_u32(&bar_xk[b]), xk_phase[b])) break;
       }
     }
     __syncwarp();
   } else if (warp == 1) {
-    if (lane == 0) {
-      // ---------------- MMA issuer ----------------
-      constexpr uint32_t idesc0 = make_idesc_s8(i8s::BM, i8s::BN);
-      bool ok = true;
-      uint32_t g = 0, tl = 0;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const I8Tile ti = i8_tile(p, t);
-        if (!ti.ok) continue;
-        const int jb = ti.j0 & ~(i8s::BM - 1);
-        // the accumulators are single-buffered: wait until the epilogue has read the
-        // previous tile's
-        if (tl >= 1 && !mbar_wait(smem_u32(&bar_tempty), (tl - 1) & 1, &s_abort)) {
+    // ---------------- MMA issuer ----------------
+    constexpr uint32_t idesc0 = make_idesc_s8(i8s::BM, i8s::BN);
+    bool ok = true;
+    uint32_t g = 0, tl = 0;
+    for (long long i = blockIdx.x; i < nitems && ok; i += G) {
+      int k, t;
+      item_of(i, k, t);
+      const I8Tile ti = i8_tile_uniform(p.tiles, t);
+      if (!ti.ok) {
+        ok = false;
+        break;
+      }
+      const int jb = ti.j0 & ~(i8s::BM - 1);
+      // the accumulators are single-buffered: wait until the epilogue has read the
+      // previous tile's
+      if (tl >= 1 && !mbar_wait_warp(smem_u32(&bar_tempty), (tl - 1) & 1, &s_abort)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      for (int kb = 0; kb < ti.kb; ++kb, ++g) {
+        const int s = g % i8s::ST;
+        if (!mbar_wait_warp(smem_u32(&bar_full[s]), (g / i8s::ST) & 1, &s_abort)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        for (int kb = 0; kb < ti.kb; ++kb, ++g) {
-          const int s = g % i8s::ST;
-          if (!mbar_wait(smem_u32(&bar_full[s]), (g / i8s::ST) & 1, &s_abort)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const int k0 = kb * i8s::BK;
-          const bool at = k0 < ti.i0, bt = k0 < jb;
-          // instruction descriptor with the MN-major bits (15: A, 16: B) of this k-block
-          const uint32_t idesc = idesc0 | (at ? 1u << 15 : 0u) | (bt ? 1u << 16 : 0u);
-          const uint32_t st = sbase + s * i8s::STAGE_BYTES;
-          // descriptors of plane 0 (a one-atom-wide MN-major tile has the same fields as
-          // the K-major one of its swizzle); plane p starts p * plane bytes further, and
-          // k advances by 32: 32 bytes K-major, 32 rows MN-major (in 16-byte units)
-          const uint64_t da0 = at ? sw128_desc(st) : sw64_desc(st);
-          const uint64_t db0 = sw64_desc(st + i8s::ND * i8s::A_PLANE);
-          const uint32_t ka = at ? (32u * 128u) >> 4 : 32u >> 4;
-          const uint32_t kb16 = bt ? (32u * 64u) >> 4 : 32u >> 4;
+        const int k0 = kb * i8s::BK;
+        const bool at = k0 < ti.i0, bt = k0 < jb;
+        // instruction descriptor with the MN-major bits (15: A, 16: B) of this k-block
+        const uint32_t idesc = idesc0 | (at ? 1u << 15 : 0u) | (bt ? 1u << 16 : 0u);
+        const uint32_t st = sbase + s * i8s::STAGE_BYTES;
+        // descriptors of plane 0 (a one-atom-wide MN-major tile has the same fields as
+        // the K-major one of its swizzle); plane p starts p * plane bytes further, and
+        // k advances by 32: 32 bytes K-major, 32 rows MN-major (in 16-byte units)
+        const uint64_t da0 = at ? sw128_desc(st) : sw64_desc(st);
+        const uint64_t db0 = sw64_desc(st + i8s::ND * i8s::A_PLANE);
+        const uint32_t ka = at ? (32u * 128u) >> 4 : 32u >> 4;
+        const uint32_t kb16 = bt ? (32u * 64u) >> 4 : 32u >> 4;
+        if (elect_one()) {
 #pragma unroll
           for (int kk = 0; kk < i8s::BK / i8s::UK; ++kk) {
 #pragma unroll
@@ -285,84 +368,105 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
           }
           umma_commit(smem_u32(&bar_empty[s]));
         }
-        if (!ok) break;
-        umma_commit(smem_u32(&bar_tfull));
-        ++tl;
+        __syncwarp();
       }
-      umma_commit(smem_u32(&bar_final));
-      for (uint32_t i = 0; i < kSpinLimit; ++i)
-        if (mbar_try(smem_u32(&bar_final), 0)) break;
-      if (!ok) s_abort = 1;
+      if (!ok) break;
+      if (elect_one()) umma_commit(smem_u32(&bar_tfull));
+      __syncwarp();
+      ++tl;
     }
+    if (elect_one()) umma_commit(smem_u32(&bar_final));
     __syncwarp();
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+      if (mbar_try(smem_u32(&bar_final), 0)) break;
+    if (!ok) s_abort = 1;
+    __syncwarp();
+  } else if (warp == i8s::STORE_WARP) {
+    // ---------------- stores and completion signals ----------------
+    // Waits only on its own CTA's epilogue, so every finished tile is signalled.
+    uint32_t tl = 0;
+    for (long long i = blockIdx.x; i < nitems; i += G, ++tl) {
+      int k, t;
+      item_of(i, k, t);
+      const I8Tile ti = i8_tile_uniform(p.tiles, t);
+      const int b = tl & 1;
+      if (!mbar_wait_warp(smem_u32(&bar_staged[b]), (tl >> 1) & 1, &s_abort)) break;
+      if (elect_one()) {
+#pragma unroll
+        for (int d = 0; d < i8s::ND; ++d)
+          tma_store_2d(&maps.a[(k + 1) & 1], stage_of(b) + d * i8s::OUT_PLANE, ti.j0,
+                       d * R + ti.row0 + ti.i0);
+        bulk_commit();
+        bulk_wait_read0();
+        mbar_arrive(smem_u32(&bar_free[b]));   // the producer may refill the buffer
+        bulk_wait0();                          // landed in global memory
+        fence_proxy_async_global();
+        __threadfence();
+        atomicAdd(p.done + p.tpart[t], 1u);
+      }
+      __syncwarp();
+    }
   } else {
     // ---------------- epilogue (16 warps) ----------------
     const int q = warp & 3;                   // TMEM lane quarter
     const int grp = (warp - 2) >> 2;          // 16-column group of the 64-column tile
     const uint32_t lane_base = (uint32_t)(q * 32) << 16;
-    // One thread stages each tile's X_k in shared memory (a TMA load into the output
-    // staging buffer, one tile ahead) and writes X_{k+1} back from the same buffer.
-    const bool storer = warp == 2 && lane == 0;
     // this thread's 16 bytes of each staged plane: row q * 32 + lane, 16-byte chunk grp
     // under the 64-byte swizzle (chunk ^ (row >> 1) & 3)
     const int rl = q * 32 + lane;
-    uint8_t* stg = smem + i8s::OUT_OFF + rl * 64 + ((grp ^ ((rl >> 1) & 3)) << 4);
-    const int sg = (int)sgn;
-    auto next_valid = [&](int t) {
-      while (t < ntiles && !i8_tile(p, t).ok) t += gridDim.x;
-      return t;
-    };
-    auto load_xk = [&](int t) {
-      const I8Tile tn = i8_tile(p, t);
-      const uint32_t xb = smem_u32(&bar_xk);
-      mbar_expect_tx(xb, i8s::ND * i8s::OUT_PLANE);
+    const int stg_off = i8s::OUT_OFF + rl * 64 + ((grp ^ ((rl >> 1) & 3)) << 4);
+    // step sums of this warp, written once per (step, CTA, warp)
+    double acc[3] = {0.0, 0.0, 0.0};   // Tr X_{k+1}, residual^2, Tr X_k^2
+    int acc_k = -1;
+    auto flush = [&]() {
+      if (acc_k < 0) return;
 #pragma unroll
-      for (int d = 0; d < i8s::ND; ++d)
-        tma_load_2d(sbase + i8s::OUT_OFF + d * i8s::OUT_PLANE, &tm_a, xb, tn.j0,
-                    d * R + tn.row0 + tn.i0);
+      for (int v = 0; v < 3; ++v)
+        for (int o = 16; o > 0; o >>= 1) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+      if (lane == 0) {
+        double* slot = p.partials + (((size_t)acc_k * G + blockIdx.x) * i8s::EPI_WARPS + (warp - 2)) * 4;
+        slot[0] = 0.0;
+        slot[1] = acc[0];
+        slot[2] = acc[1];
+        slot[3] = acc[2];
+      }
+      acc[0] = acc[1] = acc[2] = 0.0;
     };
     uint32_t tl = 0;
-    bool xk_pending = false;   // a staging load in flight (phase tl & 1)
-    int t = next_valid(blockIdx.x);
-    if (storer && t < ntiles) {
-      load_xk(t);
-      xk_pending = true;
-    }
-    while (t < ntiles) {
-      const I8Tile ti = i8_tile(p, t);
+    for (long long i = blockIdx.x; i < nitems; i += G, ++tl) {
+      int k, t;
+      item_of(i, k, t);
+      const I8Tile ti = i8_tile(p.tiles, t);
+      if (k != acc_k) {
+        flush();
+        acc_k = k;
+      }
+      const int sg = p.pp[k] == 0 ? -1 : 1;      // X^2 branch: +1; 2X - X^2: -1
       const int r = ti.i0 + rl;                 // row inside the part
       const int c0 = ti.j0 + grp * 16;          // first column of this thread's 16
-      bool ok = mbar_wait_idle(smem_u32(&bar_tfull), tl & 1, &s_abort) &&
-                mbar_wait(smem_u32(&bar_xk), tl & 1, &s_abort);
-      // every epilogue thread takes the same exit (the named barriers below need all 512)
-      if (!epi_all(ok)) break;
-      xk_pending = false;
+      const int b = tl & 1;
+      uint8_t* stg = smem + stg_off + b * i8s::OUT_BYTES;
+      if (!mbar_wait_idle(smem_u32(&bar_tfull), tl & 1, &s_abort) ||
+          !mbar_wait(smem_u32(&bar_xk[b]), (tl >> 1) & 1, &s_abort))
+        break;
       tc_fence_after();
-      uint4 xd[i8s::ND];   // X_k digits of this thread's 16 elements
-#pragma unroll
-      for (int d = 0; d < i8s::ND; ++d) xd[d] = *reinterpret_cast<const uint4*>(stg + d * i8s::OUT_PLANE);
-      // Q = rint(2^31 X'^2) = floor((P + 2^14) / 2^15), P = sum_u A_u 2^{32 - 8u}, in 32-bit
-      // steps: with s3 = A_3 + (A_4 >> 8) and s2 = A_2 + (s3 >> 8),
-      //   P = 2^16 S + R,  S = 2^16 A_0 + 2^8 A_1 + s2,  R = 2^8 (s3 & 255) + (A_4 & 255),
-      // so Q = 2 S + floor((R + 2^14) / 2^15).  S is formed modulo 2^32; its true value
-      // fits (|Q| <= 2^29 since |X'^2| <= 1/4), so the wrapped sum is exact.  The low pair
-      // is read first and folded into e = 2 (s3 >> 8) + floor((R + 2^14) / 2^15); the
-      // other three are read together and the accumulators released before the sum.
+      // Q = rint(2^31 X'^2) = floor((P + 2^14) / 2^15) with P = sum_u A_u 2^{32 - 8u}:
+      //   Q = 2^17 A_0 + 2^9 A_1 + 2 A_2 + floor((A_3 + floor((A_4 + 2^14) / 2^8)) / 2^7),
+      // the last term by nested floor division.  The sum is formed modulo 2^32; its true
+      // value fits (|Q| <= 2^29 since |X'^2| <= 1/4), so the wrapped sum is exact.  The low
+      // pair is read and folded first, then the other three are read and the
+      // accumulators released before the rest of the sum.
       int Q[16];
       {
         const uint32_t ta = tmem + lane_base + grp * 16;
-        int e[16];
+        int ql[16];
         {
           uint32_t a4[16], a3[16];
           tmem_ld16(ta + 4 * i8s::BN, a4);
           tmem_ld16(ta + 3 * i8s::BN, a3);
           tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int s3 = (int)a3[j] + ((int)a4[j] >> 8);
-            const int rr = ((s3 & 255) << 8) + (int)(a4[j] & 255u);
-            e[j] = 2 * (s3 >> 8) + ((rr + (1 << 14)) >> 15);
-          }
+          for (int j = 0; j < 16; ++j) ql[j] = ((int)a3[j] + (((int)a4[j] + (1 << 14)) >> 8)) >> 7;
         }
         uint32_t a2[16], a1[16], a0[16];
         tmem_ld16(ta + 2 * i8s::BN, a2);
@@ -374,9 +478,11 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
         if (lane == 0) mbar_arrive(smem_u32(&bar_tempty));
 #pragma unroll
         for (int j = 0; j < 16; ++j)
-          Q[j] = (int)(2u * ((a0[j] << 16) + (a1[j] << 8) + a2[j]) + (uint32_t)e[j]);
+          Q[j] = (int)((a0[j] << 17) + (a1[j] << 9) + 2u * a2[j] + (uint32_t)ql[j]);
       }
-      const int tn = next_valid(t + gridDim.x);
+      uint4 xd[i8s::ND];   // X_k digits of this thread's 16 elements (plane 0: d0)
+#pragma unroll
+      for (int d = 0; d < i8s::ND; ++d) xd[d] = *reinterpret_cast<const uint4*>(stg + d * i8s::OUT_PLANE);
 
       // Rows whose 16 columns all lie above the diagonal and on one side of the core
       // boundary weigh every element the same: the residual is summed once and scaled.
@@ -385,11 +491,16 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       const int cw_row = ti.core <= 0 ? 2 : (r < ti.core ? 1 : 0) + (c0 < ti.core ? 1 : 0);
       float s_res = 0.f;
       double s_tr = 0.0, s_trp = 0.0;
-      uint32_t wn[16];   // X_{k+1} of each element: its four digit bytes (plane 0 lowest)
+      // Digits as bytes of a biased integer: with the balanced digits d0..d3 of M (d1..d3
+      // in [-128, 127]), M + B (B = 0x808080) has the bytes d3 + 128, d2 + 128, d1 + 128
+      // and top byte d0, so the element's word [d3, d2, d1, d0] (byte 0 first) is
+      // (M + B) ^ B, and M + B = word ^ B.  The step works on M + B directly.
+      constexpr uint32_t kB = 0x00808080u;
+      uint32_t wn[16];   // X_{k+1} of each element as the word [d3, d2, d1, d0]
 #pragma unroll
       for (int g = 0; g < 4; ++g) {
-        // element-major words of X_k for elements 4g..4g+3: bytes [d3, d2, d1, d0] of
-        // each element gathered from the four planes (a 4 x 4 byte transpose)
+        // element-major words of X_k for elements 4g..4g+3 gathered from the four planes
+        // (a 4 x 4 byte transpose)
         const uint32_t p0 = g == 0 ? xd[0].x : g == 1 ? xd[0].y : g == 2 ? xd[0].z : xd[0].w;
         const uint32_t p1 = g == 0 ? xd[1].x : g == 1 ? xd[1].y : g == 2 ? xd[1].z : xd[1].w;
         const uint32_t p2 = g == 0 ? xd[2].x : g == 1 ? xd[2].y : g == 2 ? xd[2].z : xd[2].w;
@@ -406,19 +517,9 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
           const int j = 4 * g + e;
           const int c = c0 + j;
           const bool dg = r == c;
-          // M = d0 2^24 + d1 2^16 + d2 2^8 + d3 with signed digits: the bytes read as one
-          // int, less 2^8 of the next place for each negative lower digit
-          const uint32_t uv = u4[e];
-          const int m = (int)uv - (int)((uv & 0x00808080u) << 1);
-          const int mn = m + sg * Q[j] - (dg ? sg * (1 << 29) : 0);
-          // balanced base-256 digits of M_{k+1}: each digit's byte is the low byte of the
-          // running quotient
-          const int m1 = (mn + 128) >> 8;
-          const int m2 = (m1 + 128) >> 8;
-          const int d0 = max(-127, min(127, (m2 + 128) >> 8));
-          const uint32_t lo = __byte_perm((uint32_t)d0, (uint32_t)m2, 0x0040u);
-          const uint32_t hi = __byte_perm((uint32_t)m1, (uint32_t)mn, 0x0040u);
-          wn[j] = __byte_perm(lo, hi, 0x5410u);
+          const uint32_t mb = u4[e] ^ kB;                         // M_k + B
+          const uint32_t nb = mb + (uint32_t)(sg * Q[j]) - (dg ? (uint32_t)sg << 29 : 0u);
+          wn[j] = nb ^ kB;
           // 2^31 (X - X^2) = 2^31 (I/4 - X'^2), from the rounded square
           const float res = (float)((dg ? (1 << 29) : 0) - Q[j]);
           if (cuni) {
@@ -429,88 +530,99 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
             const int w = r < c ? 2 : (dg ? 1 : 0);
             s_res = fmaf((float)core_weight(w, r, c, ti.core) * res, res, s_res);
             if (dg) {
+              const int m = (int)(mb - kB), mn = (int)(nb - kB);
               s_tr += (double)mn * 0x1p-31 + 0.5;
               s_trp += (double)Q[j] * 0x1p-31 + (double)m * 0x1p-31 + 0.25;   // Tr X^2
             }
           }
         }
       }
-      sums[1] += s_tr;
-      sums[2] = fma((double)(cuni ? (float)cw_row * s_res : s_res), 0x1p-62, sums[2]);
-      sums[3] += s_trp;
-      // X_{k+1}: this thread's 16 bytes of each plane, from its element-major words
-      auto planes = [](const uint32_t (&w)[16], uint4 (&pl)[i8s::ND]) {
+      acc[0] += s_tr;
+      acc[1] = fma((double)(cuni ? (float)cw_row * s_res : s_res), 0x1p-62, acc[1]);
+      acc[2] += s_trp;
+      // X_{k+1}: this thread's 16 bytes of each plane (the inverse 4 x 4 transposes)
+      {
         uint32_t o[i8s::ND][4];
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
-          const uint32_t alo = __byte_perm(w[4 * g], w[4 * g + 1], 0x5140u);
-          const uint32_t ahi = __byte_perm(w[4 * g], w[4 * g + 1], 0x7362u);
-          const uint32_t blo = __byte_perm(w[4 * g + 2], w[4 * g + 3], 0x5140u);
-          const uint32_t bhi = __byte_perm(w[4 * g + 2], w[4 * g + 3], 0x7362u);
-          o[0][g] = __byte_perm(alo, blo, 0x5410u);
-          o[1][g] = __byte_perm(alo, blo, 0x7632u);
-          o[2][g] = __byte_perm(ahi, bhi, 0x5410u);
-          o[3][g] = __byte_perm(ahi, bhi, 0x7632u);
+          const uint32_t x = __byte_perm(wn[4 * g], wn[4 * g + 1], 0x5140u);
+          const uint32_t xh = __byte_perm(wn[4 * g], wn[4 * g + 1], 0x7362u);
+          const uint32_t y = __byte_perm(wn[4 * g + 2], wn[4 * g + 3], 0x5140u);
+          const uint32_t yh = __byte_perm(wn[4 * g + 2], wn[4 * g + 3], 0x7362u);
+          o[3][g] = __byte_perm(x, y, 0x5410u);
+          o[2][g] = __byte_perm(x, y, 0x7632u);
+          o[1][g] = __byte_perm(xh, yh, 0x5410u);
+          o[0][g] = __byte_perm(xh, yh, 0x7632u);
         }
-#pragma unroll
-        for (int d = 0; d < i8s::ND; ++d) pl[d] = make_uint4(o[d][0], o[d][1], o[d][2], o[d][3]);
-      };
-      {
-        uint4 pl[i8s::ND];
-        planes(wn, pl);
-#pragma unroll
-        for (int d = 0; d < i8s::ND; ++d) *reinterpret_cast<uint4*>(stg + d * i8s::OUT_PLANE) = pl[d];
-      }
-      fence_proxy_async_smem();   // staged bytes visible to the TMA stores
-      epi_sync();
-      if (storer) {
 #pragma unroll
         for (int d = 0; d < i8s::ND; ++d)
-          tma_store_2d(&tm_o, sbase + i8s::OUT_OFF + d * i8s::OUT_PLANE, ti.j0,
-                       d * R + ti.row0 + ti.i0);
-        bulk_commit();
-        // the next tile's X_k goes into the buffer once the stores have read it
-        if (tn < ntiles) {
-          bulk_wait_read0();
-          load_xk(tn);
-          xk_pending = true;
-        }
+          *reinterpret_cast<uint4*>(stg + d * i8s::OUT_PLANE) = make_uint4(o[d][0], o[d][1], o[d][2], o[d][3]);
       }
-      ++tl;
-      t = tn;
+      fence_proxy_async_smem();   // staged bytes visible to the TMA stores
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&bar_staged[b]));
     }
-    if (storer) {
-      bulk_wait0();
-      if (xk_pending)   // abandoned after an abort: let the copy land before exit (bounded)
-        for (uint32_t i = 0; i < kSpinLimit; ++i)
-          if (mbar_try(smem_u32(&bar_xk), tl & 1)) break;
-    }
+    flush();
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) tmem_dealloc(tmem, i8s::TMEM_COLS);
   if (s_abort && threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
-  __threadfence();
-  publish_and_finalize(p, sums, red, &s_flag);
 }
 
-cudaError_t launch_i8_batched(const StepArgs& a, long long rows, cudaStream_t st) {
-  if (!a.tiles || a.ntiles <= 0 || a.ld % 128 != 0 || rows % i8s::BM != 0 || !a.A || !a.out ||
-      4 * rows > 0x7fffffffLL)
+// Step sums: step k's totals over every (CTA, warp) slot in a fixed order; vv[k] gets the
+// residual sum (added to the caller's accumulator).
+__global__ void k_i8_step_sums(const double* __restrict__ partials, int nslots,
+                               double* __restrict__ vv) {
+  __shared__ double red[32 * 4];
+  const int k = blockIdx.x;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < nslots; j += blockDim.x)
+    for (int q = 0; q < 4; ++q) s[q] += partials[((size_t)k * nslots + j) * 4 + q];
+  block_sum<4>(s, red);
+  if (threadIdx.x == 0) vv[k] += s[2];
+}
+
+size_t i8_steps_partials(int nsteps) {
+  return (size_t)std::max(nsteps, 1) * device_sms() * i8s::EPI_WARPS * 4;
+}
+
+cudaError_t launch_i8_steps(const I8StepsArgs& a, const void* buf0, const void* buf1, int ld,
+                            double* vv, cudaStream_t st) {
+  if (!a.tiles || !a.tpart || !a.pnt || !a.pp || !a.done || !a.partials || a.ntiles <= 0 ||
+      a.nsteps <= 0 || ld % 128 != 0 || a.rows % i8s::BM != 0 || !buf0 || !buf1 || !vv ||
+      4LL * a.rows > 0x7fffffffLL)
     return cudaErrorInvalidValue;
-  // operand maps over the input's 4R rows (K-major A, MN-major A^T, B and B^T) and the
-  // store map over the output's
-  CUtensorMap ma, mat, mb, mo;
-  if (!make_tmap_u8_sw64(&ma, a.A, 4 * rows, a.ld, a.ld, i8s::BM) ||
-      !make_tmap_box(&mat, a.A, 4 * rows, a.ld, a.ld, TMAP_U8, i8s::BK) ||
-      !make_tmap_u8_sw64(&mb, a.A, 4 * rows, a.ld, a.ld, i8s::BN) ||
-      !make_tmap_u8_sw64(&mo, a.out, 4 * rows, a.ld, a.ld, i8s::BM))
-    return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(k_i8_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // per buffer: K-major operand / staged tile, MN-major A^T, and B / B^T maps over its 4R rows
+  I8Maps m;
+  for (int b = 0; b < 2; ++b) {
+    const void* buf = b ? buf1 : buf0;
+    if (!make_tmap_u8_sw64(&m.a[b], buf, 4LL * a.rows, ld, ld, i8s::BM) ||
+        !make_tmap_box(&m.at[b], buf, 4LL * a.rows, ld, ld, TMAP_U8, i8s::BK) ||
+        !make_tmap_u8_sw64(&m.b[b], buf, 4LL * a.rows, ld, ld, i8s::BN))
+      return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaFuncSetAttribute(k_i8_steps, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        i8s::SMEM_BYTES);
   if (e != cudaSuccess) return e;
-  const int grid = std::min(a.ntiles, device_sms());
-  k_i8_batch<<<grid, i8s::NTHR, i8s::SMEM_BYTES, st>>>(ma, mat, mb, mo, a, rows, a.ntiles);
+  const long long nitems = (long long)a.ntiles * a.nsteps;
+  const int grid = (int)std::min<long long>(nitems, device_sms());
+  // one CTA per SM, all resident: the CTAs wait on each other's tiles
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(i8s::NTHR);
+  cfg.dynamicSmemBytes = i8s::SMEM_BYTES;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  e = cudaLaunchKernelEx(&cfg, k_i8_steps, m, a);
+  note_launch();
+  if (e != cudaSuccess) return e;
+  k_i8_step_sums<<<a.nsteps, 256, 0, st>>>(a.partials, grid * i8s::EPI_WARPS, vv);
   note_launch();
   return cudaGetLastError();
 }

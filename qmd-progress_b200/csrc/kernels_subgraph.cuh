@@ -47,8 +47,21 @@ cudaError_t launch_place_core(const long long* hptr, const int* halo, const int*
 // Batched INT8 digit-split form (exact INT8 precision of the sub-graph loop): the
 // iterate as four signed 8-bit planes of M = rint(2^31 (X - I/2)) in each packed buffer
 // (plane s at base + s rows ld).  Tiles {row0, bi << 16 | bj64, K extent, core} of
-// 128 x 64 over the upper part of each part's block.
-cudaError_t launch_i8_batched(const StepArgs& a, long long rows, cudaStream_t st);
+// 128 x 64 over the upper band of each part's block.  All steps run in one persistent
+// launch; vv[k] += the core-row ||X_k - X_k^2||_F^2 of step k.
+struct I8StepsArgs {
+  const int4* tiles;
+  const int* tpart;     // part of each tile
+  const int* pnt;       // tiles of each part
+  const int* pp;        // branch of each step: 0 = 2X - X^2, else X^2
+  unsigned* done;       // per part, finished tiles over all steps (zero at launch)
+  double* partials;     // step sums per (step, CTA, epilogue warp): i8_steps_partials (zero)
+  int* err;
+  int ntiles, nsteps, rows;
+};
+size_t i8_steps_partials(int nsteps);   // doubles
+cudaError_t launch_i8_steps(const I8StepsArgs& a, const void* buf0, const void* buf1, int ld,
+                            double* vv, cudaStream_t st);
 cudaError_t launch_extract_digits(const long long* rp, const int* col, const double* val,
                                   const PartDesc* parts, int nparts, const int* halo,
                                   const int* skey, const int* sval, int ld, long long rows,

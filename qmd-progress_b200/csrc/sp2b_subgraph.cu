@@ -37,6 +37,8 @@ struct SubBufs {
   __half* hi[2] = {};            size_t hi_cap[2] = {};
   __half* lo[2] = {};            size_t lo_cap[2] = {};
   int8_t* dig[2] = {};           size_t dig_cap[2] = {};   // INT8 digit planes (4 per buffer)
+  int* tpart = nullptr;          size_t tpart_cap = 0;     // INT8: part of each tile
+  double* i8part = nullptr;      size_t i8part_cap = 0;    // INT8: per-step sums
   PartDesc* parts = nullptr;     size_t parts_cap = 0;
   int4* tiles = nullptr;         size_t tiles_cap = 0;
   int* row_part = nullptr;       size_t row_part_cap = 0;
@@ -53,7 +55,8 @@ struct SubBufs {
   int* pp = nullptr;             size_t pp_cap = 0;
   double* vv = nullptr;          size_t vv_cap = 0;
   double* idem = nullptr;        size_t idem_cap = 0;   // per-part core idempotency sums
-  // 32-edge FP64 layouts: the tile list of the one-launch multi-step solve
+  // 32-edge FP64 layouts: the tile list of the one-launch multi-step solve (the INT8
+  // solve uses ms_part_tiles and ms_bar too: tiles per part, finished-tile counters)
   int4* ms_tiles = nullptr;      size_t ms_tiles_cap = 0;
   int* ms_part_tiles = nullptr;  size_t ms_part_tiles_cap = 0;
   unsigned* ms_bar = nullptr;    size_t ms_bar_cap = 0;
@@ -260,6 +263,20 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       SP2B_CUDA_TRY(cudaMemcpyAsync(b.ms_part_tiles, per.data(), nparts * sizeof(int), cudaMemcpyHostToDevice, st));
       b.ms_ntiles = (int)ms.size();
     }
+    if (dig) {
+      // the persistent INT8 solve orders a part's steps by counting its finished tiles
+      std::vector<int> tp(ntiles), per(nparts, 0);
+      for (int t = 0; t < ntiles; ++t) {
+        tp[t] = row_part[tiles[t].x];
+        ++per[tp[t]];
+      }
+      SP2B_CUDA_TRY(grow_buf(b.tpart, b.tpart_cap, (size_t)ntiles));
+      SP2B_CUDA_TRY(grow_buf(b.ms_part_tiles, b.ms_part_tiles_cap, (size_t)nparts));
+      SP2B_CUDA_TRY(grow_buf(b.ms_bar, b.ms_bar_cap, (size_t)nparts));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(b.tpart, tp.data(), ntiles * sizeof(int), cudaMemcpyHostToDevice, st));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(b.ms_part_tiles, per.data(), nparts * sizeof(int), cudaMemcpyHostToDevice, st));
+      SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     SP2B_CUDA_TRY(grow_buf(b.parts, b.parts_cap, nparts));
     SP2B_CUDA_TRY(grow_buf(b.tiles, b.tiles_cap, ntiles));
     SP2B_CUDA_TRY(grow_buf(b.row_part, b.row_part_cap, rows));
@@ -301,6 +318,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     }
   } else if (dig) {
     for (int i = 0; i < 2; ++i) SP2B_CUDA_TRY(grow_buf(b.dig[i], b.dig_cap[i], 4 * packed));
+    SP2B_CUDA_TRY(grow_buf(b.i8part, b.i8part_cap, i8_steps_partials(maxiter)));
   } else {
     SP2B_CUDA_TRY(grow_buf(b.x2, b.x2_cap, packed));
   }
@@ -388,16 +406,17 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   // The captured graph bakes in every pointer, size and scalar it launches with;
   // reuse it when all of them are unchanged.
   struct Key {
-    const void* p[22];
+    const void* p[25];
     long long q[10];
     double d[2];
   } key;
   memset(&key, 0, sizeof(key));
-  const void* ptrs[22] = {j.rp, j.col, j.val, core_d, dense_d, b.xs, b.x2,
+  const void* ptrs[25] = {j.rp, j.col, j.val, core_d, dense_d, b.xs, b.x2,
                           dig ? (const void*)b.dig[0] : b.hi[0], dig ? (const void*)b.dig[1] : b.hi[1],
                           b.lo[0], b.lo[1], b.parts, b.tiles, b.row_part, b.halo, b.skey,
                           b.sval, b.partials, b.rec, b.pp, (const void*)cap,
-                          idem ? b.idem : nullptr};
+                          idem ? b.idem : nullptr, dig ? b.tpart : nullptr,
+                          dig ? b.ms_bar : nullptr, dig ? b.i8part : nullptr};
   memcpy(key.p, ptrs, sizeof(ptrs));
   const long long qs[10] = {n, nparts, rows, ld, maxiter, prec, ntiles, (long long)(size_t)b.vv,
                             j.clear_dense ? 1 : 0, bt};
@@ -460,14 +479,30 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
                                    split ? (void*)b.lo[0] : nullptr, cap)) != cudaSuccess)
           return e;
       }
-      for (int k = 0; k < maxiter; ++k) {
+      if (dig && maxiter > 0) {
+        // every step in one persistent launch
+        if ((e = cudaMemsetAsync(b.ms_bar, 0, nparts * sizeof(unsigned), cap)) != cudaSuccess)
+          return e;
+        if ((e = cudaMemsetAsync(b.i8part, 0, i8_steps_partials(maxiter) * sizeof(double), cap)) !=
+            cudaSuccess)
+          return e;
+        I8StepsArgs ia;
+        ia.tiles = b.tiles;
+        ia.tpart = b.tpart;
+        ia.pnt = b.ms_part_tiles;
+        ia.pp = b.pp;
+        ia.done = b.ms_bar;
+        ia.partials = b.i8part;
+        ia.err = c->err;
+        ia.ntiles = ntiles;
+        ia.nsteps = maxiter;
+        ia.rows = (int)rows;
+        if ((e = launch_i8_steps(ia, b.dig[0], b.dig[1], ld, b.vv, cap)) != cudaSuccess) return e;
+      }
+      for (int k = 0; k < maxiter && !dig; ++k) {
         a.k = k;
         const int bin = k & 1, bout = (k + 1) & 1;
-        if (dig) {
-          a.A = a.B = a.E = b.dig[bin];
-          a.out = b.dig[bout];
-          e = launch_i8_batched(a, rows, cap);
-        } else if (split) {
+        if (split) {
           a.A = a.B = a.E = b.hi[bin];
           a.A_lo = a.B_lo = a.E_lo = b.lo[bin];
           a.out = b.hi[bout];
@@ -518,7 +553,8 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   }
   cudaError_t le = cudaGraphLaunch(exec, st);
   if (le == cudaSuccess) le = cudaStreamSynchronize(st);
-  note_launch(maxiter + 3 + (idem ? 1 : 0));  // extract, normalise, maxiter steps, scatter
+  // extract, normalise, the steps (INT8: one persistent launch and its sums), scatter
+  note_launch((dig ? (fused ? 1 : 2) + (maxiter > 0 ? 2 : 0) + 1 : maxiter + 3) + (idem ? 1 : 0));
   if (le != cudaSuccess) {
     set_last_error("graph launch failed: %s", cudaGetErrorString(le));
     return SP2B_CUDA_ERROR;

@@ -90,6 +90,10 @@ __device__ __forceinline__ void bulk_wait0() {
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// orders this thread's generic-proxy accesses to global memory with its async-proxy ones
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -124,47 +128,20 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
-// Warp-wide forms: every lane of the warp executes them with the same operands (so they
-// stay warp-uniform) and the instruction is issued by the lanes with `issue` set (one).
-__device__ __forceinline__ void umma_i8_if(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                           uint32_t idesc, uint32_t accumulate, uint32_t issue) {
+// One lane of the (fully active) warp: true in exactly one of them.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t r;
   asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "setp.ne.b32 q, %5, 0;\n\t"
-      "@q tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(issue)
-      : "memory");
+      "{\n\t.reg .pred P;\n\t"
+      "elect.sync _|P, 0xffffffff;\n\t"
+      "selp.u32 %0, 1, 0, P;\n\t}\n"
+      : "=r"(r));
+  return r != 0;
 }
-__device__ __forceinline__ void umma_commit_if(uint32_t mbar, uint32_t issue) {
-  asm volatile(
-      "{\n\t.reg .pred q;\n\t"
-      "setp.ne.b32 q, %1, 0;\n\t"
-      "@q tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(
-          mbar),
-      "r"(issue)
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_2d_if(uint32_t dst, const CUtensorMap* tm, uint32_t mbar,
-                                               int x, int y, uint32_t issue) {
-  asm volatile(
-      "{\n\t.reg .pred q;\n\t"
-      "setp.ne.b32 q, %5, 0;\n\t"
-      "@q cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];\n\t}\n" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(mbar), "r"(x), "r"(y), "r"(issue)
-      : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx_if(uint32_t a, uint32_t bytes, uint32_t issue) {
-  asm volatile(
-      "{\n\t.reg .pred q;\n\t"
-      "setp.ne.b32 q, %2, 0;\n\t"
-      "@q mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t}\n" ::"r"(a),
-      "r"(bytes), "r"(issue)
-      : "memory");
-}
-// Bounded wait by a whole warp: every lane polls (so the issuing lane has observed the
-// phase), and the warp proceeds only if all lanes saw it.
+// Broadcast of lane 0's value: marks it warp-uniform for the compiler, so that what is
+// derived from it (descriptors, coordinates, loop bounds) stays in uniform registers.
+__device__ __forceinline__ int warp_uniform(int v) { return __shfl_sync(0xffffffffu, v, 0); }
+// Bounded wait by a whole warp: every lane polls, the warp proceeds only if all saw it.
 __device__ __forceinline__ bool mbar_wait_warp(uint32_t a, uint32_t parity, volatile int* abort_flag) {
   const bool ok = mbar_wait(a, parity, abort_flag);
   return __all_sync(0xffffffffu, ok) != 0;
