@@ -64,7 +64,7 @@ def parse():
                          "cubic_dense: the 32^3 lattice solved densely (N=32768)")
     ap.add_argument("--L", type=int, default=32, help="subgraph: lattice edge")
     ap.add_argument("--parts", type=int, default=256, help="subgraph: number of parts")
-    ap.add_argument("--subgraph-precision", default="mixed_fp16",
+    ap.add_argument("--subgraph-precision", default="exact_int8",
                     choices=["mixed_fp16", "mixed_bf16", "exact_int8", "fp64"],
                     help="precision of the sub-graph solve nested in the default line")
     ap.add_argument("--no-subgraph", action="store_true",
@@ -770,15 +770,38 @@ def measure_subgraph(args, rank, world, local, dist, precision):
         if ent:
             # captured on the 20^3 / 64-part case; DRAM bytes scale with the tiles' work
             traffic = ent["bytes_per_launch"] * flops_launch / ent["flops_per_launch"]
-    achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
     peak_key, peak = roofline_peak(peaks, clk.summary())
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "frac_of_sustained": achieved / peaks.get("bf16_tflops_sustained", peak),
-                "peak_source": f"{psrc} {peak_key}",
-                "kernel": "k_tc_persist<T,0,1> (batched SP2 step, all parts)",
-                "avg_launch_ms": step_avg_ms, "flops_per_launch": flops_launch,
-                "timing": "(solve - solve with no steps) / maxIter, FP64 re-solve off"}
+    if prec == _lib.PREC_EXACT_INT8:
+        # the persistent INT8 kernel: 13 digit products of 128 x 64 x n64 per tile (tiles
+        # on or above each part's diagonal, K to the part size rounded up to 64); int8
+        # tensor rate = 2x the bf16 dense rate on B200
+        ops = 0.0
+        for nn in ls:
+            n64 = -(-int(nn) // 64) * 64
+            ntile = sum(n64 // 64 - 2 * bi for bi in range(-(-n64 // 128)))
+            ops += ntile * 2.0 * 13 * 128 * 64 * n64
+        achieved = ops / (step_avg_ms / 1e3) / 1e12
+        peak = 2.0 * peak
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": f"{psrc} {peak_key} x 2 (int8 : bf16 dense rate)",
+                    "kernel": "k_i8_steps (persistent: every step of every part, one launch)",
+                    "avg_step_ms": step_avg_ms, "int8_ops_per_step": ops,
+                    "sp2_flops_per_step": flops_launch,
+                    "sp2_tflops": flops_launch / (step_avg_ms / 1e3) / 1e12,
+                    "timing": "(solve - solve with no steps) / maxIter, FP64 re-solve off"}
+    else:
+        achieved = flops_launch / (step_avg_ms / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "frac_of_sustained": achieved / peaks.get("bf16_tflops_sustained", peak),
+                    "peak_source": f"{psrc} {peak_key}",
+                    "kernel": ("k_tc_persist<T,0,1> (batched SP2 step, all parts)"
+                               if prec != _lib.PREC_FP64 else "batched FP64 step (all parts)"),
+                    "avg_launch_ms": step_avg_ms, "flops_per_launch": flops_launch,
+                    "timing": "(solve - solve with no steps) / maxIter, FP64 re-solve off"}
+    roofline["ms_solve_without_fp64_resolve"] = t_steps
+    roofline["ms_solve_without_steps"] = t_none
 
     # ---- end to end through the C ABI with host buffers ----
     e2e = None

@@ -1,9 +1,9 @@
 """Generate tests/golden/poly512.npz from the reference's own test fixture.
 
 Input: ``tests/tests_data/poly.512.mtx`` of lanl/qmd-progress (6144 x 6144, 98,304
-nonzeros), read from the reference checkout given on the command line (default
-/root/reference).  This script only runs where that checkout exists; the fixture it
-writes is what the tests read on any machine.
+nonzeros), read from the reference checkout given on the command line or in
+SP2B_REFERENCE (default /root/reference).  This script only runs where that checkout
+exists; the fixture it writes is what the tests read on any machine.
 
 It runs the CPU oracle (oracle/sp2_oracle.py) with the parameters of the reference
 tests that use this file (tests/src/main.F90):
@@ -83,4 +83,4 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SP2B_REFERENCE", "/root/reference"))
