@@ -60,19 +60,19 @@ constexpr int TMEM_COLS = 512;
 static_assert(NU * BN <= TMEM_COLS, "the five accumulators fit the TMEM allocation");
 }  // namespace i8s
 
-// The thirteen plane products (s, t) with s + t <= 4, grouped by u = s + t; product q
-// multiplies A plane pa(q) by B plane pb(q), and starts its accumulator if first(q).
+// The thirteen plane products (s, t) with s + t <= 4, issued as seven MMAs: B planes t
+// and t + 1 lie back to back in shared memory, so one N = 128 product of A plane s with
+// them writes A_s B_t^T and A_s B_{t+1}^T into the adjacent accumulators u = s + t and
+// u + 1.  MMA q multiplies A plane pa(q) by B planes pb(q).. (two if wide(q)); the first
+// three, in this order, start the five accumulators at k = 0 (0-1, 2-3, 4).
 __device__ __forceinline__ constexpr int i8_pa(int q) {
-  return q == 0 ? 0 : q == 1 ? 0 : q == 2 ? 1 : q == 3 ? 0 : q == 4 ? 1 : q == 5 ? 2
-       : q == 6 ? 0 : q == 7 ? 1 : q == 8 ? 2 : q == 9 ? 3 : q == 10 ? 1 : q == 11 ? 2 : 3;
+  return q == 0 ? 0 : q == 1 ? 0 : q == 2 ? 2 : q == 3 ? 1 : q == 4 ? 1 : q == 5 ? 2 : 3;
 }
 __device__ __forceinline__ constexpr int i8_pb(int q) {
-  return q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 0 : q == 3 ? 2 : q == 4 ? 1 : q == 5 ? 0
-       : q == 6 ? 3 : q == 7 ? 2 : q == 8 ? 1 : q == 9 ? 0 : q == 10 ? 3 : q == 11 ? 2 : 1;
+  return q == 0 ? 0 : q == 1 ? 2 : q == 2 ? 2 : q == 3 ? 0 : q == 4 ? 2 : 0;
 }
-__device__ __forceinline__ constexpr bool i8_first(int q) {
-  return q == 0 || q == 1 || q == 3 || q == 6 || q == 10;
-}
+__device__ __forceinline__ constexpr bool i8_wide(int q) { return q != 2; }
+__device__ __forceinline__ constexpr bool i8_first(int q) { return q <= 2; }
 
 // Byte j (0..15) of a 16-byte register vector, sign-extended (j is a constant after
 // unrolling, so this folds to one shift pair).
@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     constexpr uint32_t idesc0 = make_idesc_s8(i8s::BM, i8s::BN);
+    constexpr uint32_t idesc128 = make_idesc_s8(i8s::BM, 2 * i8s::BN);
     bool ok = true;
     uint32_t g = 0, tl = 0;
     for (long long i = blockIdx.x; i < nitems && ok; i += G) {
@@ -344,26 +345,30 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
         const int k0 = kb * i8s::BK;
         const bool at = k0 < ti.i0, bt = k0 < jb;
         // instruction descriptor with the MN-major bits (15: A, 16: B) of this k-block
-        const uint32_t idesc = idesc0 | (at ? 1u << 15 : 0u) | (bt ? 1u << 16 : 0u);
+        const uint32_t mn = (at ? 1u << 15 : 0u) | (bt ? 1u << 16 : 0u);
+        const uint32_t id64 = idesc0 | mn, id128 = idesc128 | mn;
         const uint32_t st = sbase + s * i8s::STAGE_BYTES;
         // descriptors of plane 0 (a one-atom-wide MN-major tile has the same fields as
         // the K-major one of its swizzle); plane p starts p * plane bytes further, and
         // k advances by 32: 32 bytes K-major, 32 rows MN-major (in 16-byte units)
+        // B as two planes of N = 64: K-major, plane t + 1's rows follow plane t's at the
+        // same 8-row group stride; MN-major, the second 64-byte atom along N sits one plane
+        // further (leading byte offset = one plane)
         const uint64_t da0 = at ? sw128_desc(st) : sw64_desc(st);
-        const uint64_t db0 = sw64_desc(st + i8s::ND * i8s::A_PLANE);
+        const uint64_t db0 = sw64_desc_lbo(st + i8s::ND * i8s::A_PLANE, bt ? i8s::B_PLANE : 16);
         const uint32_t ka = at ? (32u * 128u) >> 4 : 32u >> 4;
         const uint32_t kb16 = bt ? (32u * 64u) >> 4 : 32u >> 4;
         if (elect_one()) {
 #pragma unroll
           for (int kk = 0; kk < i8s::BK / i8s::UK; ++kk) {
 #pragma unroll
-            for (int q = 0; q < 13; ++q) {
+            for (int q = 0; q < 7; ++q) {
               const int sa = i8_pa(q), sb = i8_pb(q);
-              // the first product of each u at k = 0 starts its accumulator
+              // the first three MMAs at k = 0 start the accumulators
               umma_i8(tmem + (sa + sb) * i8s::BN,
                       da0 + (uint64_t)(sa * (i8s::A_PLANE >> 4) + kk * ka),
-                      db0 + (uint64_t)(sb * (i8s::B_PLANE >> 4) + kk * kb16), idesc,
-                      (kb > 0 || kk > 0 || !i8_first(q)) ? 1u : 0u);
+                      db0 + (uint64_t)(sb * (i8s::B_PLANE >> 4) + kk * kb16),
+                      i8_wide(q) ? id128 : id64, (kb > 0 || kk > 0 || !i8_first(q)) ? 1u : 0u);
             }
           }
           umma_commit(smem_u32(&bar_empty[s]));

@@ -259,6 +259,17 @@ __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   d |= (uint64_t)4u << 61;
   return d;
 }
+// The same with a leading byte offset (a multiple of 16): for an MN-major operand wider
+// than one 64-byte atom, the stride from one atom to the next along MN.
+__device__ __forceinline__ uint64_t sw64_desc_lbo(uint32_t saddr, uint32_t lbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)(512u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)4u << 61;
+  return d;
+}
 // kind::f16 instruction descriptor: FP32 accumulate, A/B K-major, M x N.
 __host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, int M, int N) {
   return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) |
