@@ -69,6 +69,8 @@ def parse():
                     help="precision of the sub-graph solve nested in the default line")
     ap.add_argument("--no-subgraph", action="store_true",
                     help="default workload: leave out the nested sub-graph measurement")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="default workload: leave out the nested adjoint (config 3) measurement")
     return ap.parse_args()
 
 
@@ -567,6 +569,9 @@ def main():
             it64, _ = oracle_solve(n)
         cpu = cpu_baseline_sample(n, it64, max_seconds=20.0)
         cpu["sp2_iters"] = it64
+    adj = None
+    if args.workload == "two_band" and not args.no_adjoint and rank == 0 and world == 1:
+        adj = measure_adjoint()
     sub = None
     if args.workload == "two_band" and not args.no_subgraph:
         del h_dev, rho_dev, rho_mixed
@@ -584,7 +589,7 @@ def main():
                "tflops": value * (2.0 * n ** 3 * iters + (4.0 * n ** 3 if prec != _lib.PREC_FP64 else 0.0)) / 1e12,
                "fp64": fp64, "e2e": e2e, "roofline": roofline, "refinement": refinement,
                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
-               "tuning": _tuning(), "subgraph": sub}
+               "tuning": _tuning(), "subgraph": sub, "adjoint": adj}
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
@@ -607,6 +612,55 @@ def run_subgraph(args, rank, world, local):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def measure_adjoint(n=2048, reps=5):
+    """Config 3: the differentiable SP2 (sp2b.autograd.SP2Density) on the two-band model,
+    N = 2048, loss Tr(D A) with a random symmetric A; forward (replay of the genseq branch
+    sequence, FP32 storage, split-precision squarings, X kept every 4 steps) and backward
+    (segments recomputed from the checkpoints, one product M = G X and M + M^T per step)
+    timed with CUDA events on the current stream.  Algorithmic flops: 2 n^3 per forward
+    step; backward 2 n^3 per adjoint step plus the recomputed steps."""
+    import torch
+    import sp2b
+    from sp2b import modelham as M
+    from sp2b.autograd import sequence_and_bounds, sp2_density
+    h = torch.tensor(M.two_band_1d(n, seed=0), device="cuda", dtype=torch.float32)
+    a = torch.tensor(M.random_symmetric(n, seed=1), device="cuda", dtype=torch.float32)
+    pp, lo, hi = sequence_and_bounds(h, 0.5)
+    K, ck = len(pp), 4
+    stream = torch.cuda.current_stream()
+
+    def one():
+        hv = h.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        d = sp2_density(hv, pp, lo, hi, ck)
+        loss = (d * a).sum()
+        e1.record(stream)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2), hv.grad
+    for _ in range(2):
+        one()
+    fw, bw = [], []
+    for _ in range(reps):
+        f, b, g = one()
+        fw.append(f)
+        bw.append(b)
+    f, b = statistics.median(fw), statistics.median(bw)
+    nseg = (K + ck - 1) // ck
+    recomputed = K - nseg                      # steps replayed from the checkpoints
+    flops_f = 2.0 * n ** 3 * K
+    flops_b = 2.0 * n ** 3 * (K + recomputed)
+    return {"workload": f"two_band_1d_n{n}_adjoint_trDA", "n": n, "sp2_steps": K,
+            "checkpoint": ck, "forward_ms": f, "backward_ms": b,
+            "forward_tflops": flops_f / (f / 1e3) / 1e12,
+            "backward_tflops": flops_b / (b / 1e3) / 1e12,
+            "grad_finite": bool(torch.isfinite(g).all().item()),
+            "kernels": "k_tc (split FP16 products), k_adjoint_combine (M + M^T)",
+            "timing": f"median of {reps}, CUDA events"}
 
 
 def measure_subgraph(args, rank, world, local, dist, precision):
