@@ -349,6 +349,14 @@ int sp2b_place_core_rows(long long n, int nparts, const long long* halo_ptr, con
  * computed as hi/lo FP16 tcgen05 products with FP32 accumulation. */
 int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* c, int n, void* stream);
 
+/* Row panel of a product with a symmetric right operand, for the row-block distributed
+ * dense SP2 (each rank forms its rows of X^2; the reference's DO_MPI_BLOCK loop,
+ * src/prg_sp2_mod.F90:263-380 with :312-317 and :365-370): C (m x n, row pitch n) =
+ * A_rows (m x n, row pitch n) * B (n x n, symmetric), m <= n, device FP32 arrays on
+ * `stream`, hi/lo FP16 tcgen05 products with FP32 accumulation. */
+int sp2b_dev_panel_gemm_f32(const float* a_rows, int m, const float* b, int n, float* c,
+                            void* stream);
+
 /* Differentiable SP2 (the autograd path), device FP32 n x n arrays on `stream`.  These
  * have no single counterpart in the reference: they are the pieces of a reverse-mode
  * derivative of the SP2 recursion whose forward-mode form is prg_compute_response_SP2

@@ -204,7 +204,8 @@ __global__ void __launch_bounds__(128, 1)
       tmem_wait_ld();
       const int c0 = j0 + cc * 32;
       if (!SYM) {
-        if (r < plain_n) {
+        // rows bounded by n_out when set (a row panel of the product), else by plain_n
+        if (r < (p.n_out > 0 ? p.n_out : plain_n)) {
           for (int j = 0; j < 32; ++j) {
             const int c = c0 + j;
             if (c < plain_n)
@@ -1196,6 +1197,21 @@ __global__ void k_f32_to_split(const float* __restrict__ a, int n, int np, __hal
   }
 }
 
+// An m x n FP32 row panel into the padded mp x np hi/lo split (zeros outside).
+__global__ void k_f32_rows_to_split(const float* __restrict__ a, int m, int n, int mp, int np,
+                                    __half* __restrict__ hi, __half* __restrict__ lo) {
+  using TR = SplitTraits<__half>;
+  const size_t total = (size_t)mp * np;
+  for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / np), c = (int)(idx % np);
+    const double v = (r < m && c < n) ? (double)a[(size_t)r * n + c] : 0.0;
+    const __half h = TR::from_d(v);
+    hi[idx] = h;
+    lo[idx] = TR::from_d((v - TR::to_d(h)) * TR::kScale);
+  }
+}
+
 // ---------------------------------------------------------------------------------
 // Host side: tensor maps and launches
 // ---------------------------------------------------------------------------------
@@ -1464,6 +1480,33 @@ cudaError_t launch_tc_plain(const __half* ahi, const __half* alo, const __half* 
   return launch_tc<__half, false>(a, np, grid, c, n, st);
 }
 
+// Row panel C (m x n, row pitch n) = A_rows B^T from split operands: A over mp rows, B over
+// np rows (both with row pitch np, K = np); one CTA per 128 x 128 tile of the panel.
+cudaError_t launch_tc_panel(const __half* ahi, const __half* alo, int mp, const __half* bhi,
+                            const __half* blo, int np, float* c, int m, int n, cudaStream_t st,
+                            int* err) {
+  if (mp % tc::BM != 0 || np % tc::BN != 0 || m > mp || n > np || m <= 0 || n <= 0)
+    return cudaErrorInvalidValue;
+  StepArgs a;
+  memset(&a, 0, sizeof(a));
+  a.np = np;
+  a.ld = np;
+  a.n_out = m;
+  a.err = err;
+  CUtensorMap mm[4];
+  if (!make_tmap(&mm[0], ahi, mp, np, np, false) || !make_tmap(&mm[1], alo, mp, np, np, false) ||
+      !make_tmap(&mm[2], bhi, np, np, np, false) || !make_tmap(&mm[3], blo, np, np, np, false))
+    return cudaErrorInvalidValue;
+  auto kern = k_tc_gemm<__half, false>;
+  cudaError_t e =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  kern<<<dim3(np / tc::BN, mp / tc::BM), 128, tc::SMEM_BYTES, st>>>(mm[0], mm[1], mm[2], mm[3], a,
+                                                                    c, n);
+  note_launch();
+  return cudaGetLastError();
+}
+
 static int ew_grid(size_t total) {
   size_t g = (total + 255) / 256;
   if (g > 148 * 8) g = 148 * 8;
@@ -1494,6 +1537,13 @@ cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int 
         (const __nv_bfloat16*)hi, (const __nv_bfloat16*)lo, total, x);
   else
     k_split_to_f64<__half><<<ew_grid(total), 256, 0, st>>>(hi, lo, total, x);
+  note_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_f32_rows_to_split(const float* a, int m, int n, int mp, int np, __half* hi,
+                                     __half* lo, cudaStream_t st) {
+  k_f32_rows_to_split<<<ew_grid((size_t)mp * np), 256, 0, st>>>(a, m, n, mp, np, hi, lo);
   note_launch();
   return cudaGetLastError();
 }

@@ -112,6 +112,11 @@ cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf
 cudaError_t launch_split_to_f64(const __half* hi, const __half* lo, int np, int bf16,
                                 double* x, cudaStream_t st);
 cudaError_t launch_wait_selftest(uint32_t limit, int* err, cudaStream_t st);
+cudaError_t launch_f32_rows_to_split(const float* a, int m, int n, int mp, int np, __half* hi,
+                                     __half* lo, cudaStream_t st);
+cudaError_t launch_tc_panel(const __half* ahi, const __half* alo, int mp, const __half* bhi,
+                            const __half* blo, int np, float* c, int m, int n, cudaStream_t st,
+                            int* err);
 cudaError_t launch_f32_to_split(const float* a, int n, int np, __half* hi, __half* lo,
                                 cudaStream_t st);
 cudaError_t launch_mcweeny_tc(const __half* xhi, const __half* xlo, const __half* rhi,

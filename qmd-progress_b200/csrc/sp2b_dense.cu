@@ -1034,6 +1034,27 @@ int sp2b_last_solve_info(int* launches, int* nupd, int* iter, int* status, doubl
   return SP2B_OK;
 }
 
+int sp2b_dev_panel_gemm_f32(const float* a_rows, int m, const float* b, int n, float* cout,
+                            void* stream) {
+  if (m <= 0 || n <= 0 || m > n || !a_rows || !b || !cout) {
+    set_last_error("sp2b_dev_panel_gemm_f32: bad argument");
+    return SP2B_BAD_ARG;
+  }
+  int status = SP2B_OK;
+  Ctx* c = get_ctx(&status);
+  if (!c) return status;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaStream_t st = (cudaStream_t)stream;  // device arrays: NULL = the default stream
+  const int np = padded(n), mp = padded(m);
+  SP2B_CUDA_TRY(c->ensure_split(np));      // mp x np <= np x np
+  SP2B_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(int), st));
+  SP2B_CUDA_TRY(launch_f32_rows_to_split(a_rows, m, n, mp, np, c->hi[0], c->lo[0], st));
+  SP2B_CUDA_TRY(launch_f32_to_split(b, n, np, c->hi[1], c->lo[1], st));
+  SP2B_CUDA_TRY(launch_tc_panel(c->hi[0], c->lo[0], mp, c->hi[1], c->lo[1], np, cout, m, n, st,
+                                c->err));
+  return SP2B_OK;
+}
+
 int sp2b_dev_sym_gemm_f32(const float* a, const float* b, float* cout, int n, void* stream) {
   if (n <= 0 || !a || !b || !cout) {
     set_last_error("bad argument");

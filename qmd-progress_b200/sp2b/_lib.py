@@ -80,6 +80,7 @@ _SIGS = {
     "sp2b_subgraph_sp2_loop": (_i, [_i, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp, _i, _d, _d, _vp, _vp,
                                     _vp, C.POINTER(Opts)]),
     "sp2b_dev_sym_gemm_f32": (_i, [_vp, _vp, _vp, _i, _vp]),
+    "sp2b_dev_panel_gemm_f32": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "sp2b_dev_normalize_f32": (_i, [_vp, _vp, _i, _d, _d, _vp]),
     "sp2b_dev_sp2_step_f32": (_i, [_vp, _vp, _i, _i, _vp]),
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
