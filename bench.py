@@ -669,11 +669,12 @@ def measure_subgraph(args, rank, world, local, dist, precision):
     Setup (untimed), as the reference's sub-graph test does
     (tests/src/test_subgraphloop.F90:59-152): a dense genseq of the full H gives
     vv and pp, prg_homolumogap and prg_sp2sequence give the shared branch sequence;
-    the graph is |H^2| > 0.6 (the H^2 graph of
-    benchmarks/dmconstruction_graphBased/dmconstruction_graphBased.F90:63-65); parts
-    come from recursive coordinate bisection with split fractions U[0.4, 0.6]; halos
-    are one jump in the graph.  A step is one whole sub-graph solve (one graph launch):
-    extraction from CSR, normalisation, maxIter batched SP2 steps, core-row scatter.
+    the graph is the pattern of |D^2| > 0.3 for the density D of that genseq (the test
+    thresholds the density of a previous solve; the configuration partitions the graph
+    of D^2); parts come from recursive coordinate bisection with split fractions
+    U[0.4, 0.6]; halos are one jump in the graph.  A step is one whole sub-graph solve
+    (one graph launch): extraction from CSR, normalisation, the SP2 steps, core-row
+    scatter.
     """
     import numpy as np
     import torch
@@ -682,7 +683,8 @@ def measure_subgraph(args, rank, world, local, dist, precision):
     L = args.L
     n = L ** 3
     Lb = _lib.lib()
-    rp, col, val = M.cubic_3d_csr(L, seed=rank, threshold=1e-5)
+    # one system (the sharded solve splits its parts over the ranks)
+    rp, col, val = M.cubic_3d_csr(L, seed=0, threshold=1e-5)
     # Gershgorin bounds from the CSR rows
     diag = np.zeros(n)
     rows = np.repeat(np.arange(n), np.diff(rp))
@@ -705,7 +707,14 @@ def measure_subgraph(args, rank, world, local, dist, precision):
     _lib.check(Lb.sp2b_sp2_alg2_genseq(hd.data_ptr(), rd.data_ptr(), n, 0.0, 0.5, 0, 100, b"None",
                                        1e-10, pp.ctypes.data, C.byref(ic), vv.ctypes.data, 0,
                                        C.byref(o)), "genseq")
-    del hd, rd
+    del hd
+    torch.cuda.empty_cache()
+    # the graph of D^2 (the full system's density from the same genseq), thresholded at
+    # 0.3: core+halo sizes 96..462 with 256 parts (configuration: 64..512)
+    tg = time.time()
+    g_csr = G.density_square_graph(rd, 0.3)
+    graph_s = time.time() - tg
+    del rd
     torch.cuda.empty_cache()
     full_iters = ic.value
     eh, el, egap = sp2b.homolumogap(vv[:full_iters], full_iters, pp[:full_iters], emin, emax)
@@ -719,9 +728,6 @@ def measure_subgraph(args, rank, world, local, dist, precision):
         seq, maxiter = [int(x) for x in pp[:full_iters]], full_iters
         seq_source = "full-system exact-INT8 genseq pp"
 
-    tg = time.time()
-    g_csr = G.square_graph_gpu((rp, col, val), n, 0.6)   # |H^2| > 0.6 on the GPU
-    graph_s = time.time() - tg
     parts = G.rcb_partition(G.lattice_coords(L), args.parts, seed=0, lo=0.4, hi=0.6)
     hp, hidx, ls, lls = sp2b.subgraph_halos(n, g_csr, parts, None, double_jump=False)
     nparts_all = len(parts)
@@ -929,7 +935,7 @@ def measure_subgraph(args, rank, world, local, dist, precision):
                           "lsize_max": int(ls.max()), "lsize_mean": float(ls.mean()),
                           "maxiter": maxiter, "full_genseq_iters": full_iters,
                           "homo": eh, "lumo": el, "sequence": seq_source,
-                          "graph": "|H^2| > 0.6", "halo": "one jump",
+                          "graph": "|D^2| > 0.3 (D: the full system's genseq density)", "halo": "one jump",
                           "partition": "RCB U[0.4,0.6]", "setup_s": setup_s,
                           "l2": "CSR H 13 MB fits in L2: 256 MiB written between timed solves",
                           "graph_s": graph_s,

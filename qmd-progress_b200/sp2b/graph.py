@@ -80,6 +80,31 @@ def square_graph_gpu(h_csr, n: int, gthreshold: float):
     return grp, gcol[:need.value]
 
 
+def density_square_graph(d, gthreshold: float):
+    """Graph of D^2 on the GPU: the pattern of |D^2| > gthreshold (no diagonal test: every
+    node of an occupied or empty state has |(D^2)_ii| far above it) from a dense symmetric
+    CUDA tensor D, the product as the library's split-precision tcgen05 product
+    (sp2b_dev_sym_gemm_f32, FP32 accumulation; the threshold decides against entries
+    of order 0.1, far above its rounding).  Returns CSR (row_ptr int64, col int32),
+    columns ascending."""
+    import ctypes as C
+    import torch
+    from . import _lib
+    n = d.shape[0]
+    d32 = d.float().contiguous()
+    d2 = torch.empty_like(d32)
+    _lib.check(_lib.lib().sp2b_dev_sym_gemm_f32(
+        d32.data_ptr(), d32.data_ptr(), d2.data_ptr(), n,
+        C.c_void_p(torch.cuda.current_stream(d.device).cuda_stream)), "sym_gemm_f32")
+    del d32
+    idx = (d2.abs() > gthreshold).nonzero()
+    del d2
+    counts = torch.bincount(idx[:, 0], minlength=n)
+    rp = np.zeros(n + 1, dtype=np.int64)
+    rp[1:] = np.cumsum(counts.cpu().numpy())
+    return rp, idx[:, 1].to(torch.int32).cpu().numpy()
+
+
 def thresholded_graph(dense: np.ndarray, gthreshold: float):
     """Pattern of |A| > gthreshold of a dense matrix as CSR (bml_threshold, then the
     nonzero pattern, as tests/src/test_subgraphloop.F90:100 does with the density)."""

@@ -70,3 +70,26 @@ def test_capacity_and_overflow(cuda):
     # the library stays usable
     g = G.square_graph_gpu((rp, col, val), n, 0.6)
     assert np.array_equal(g[1], G.thresholded_square_graph((rp, col, val), n, 0.6)[1])
+
+
+def test_density_square_graph_matches_host(cuda):
+    """The graph of D^2 (sp2b.graph.density_square_graph, the bench's sub-graph
+    construction) against the FP64 host product on a 10^3 lattice's density: equal
+    patterns except for entries within 1e-5 of the threshold (FP32-accumulated product)."""
+    torch = cuda
+    import sp2_oracle as O
+    n = 1000
+    rp, col, val = M.cubic_3d_csr(10, seed=0, threshold=1e-5)
+    h = M.csr_to_dense(rp, col, val, n)
+    d = O.sp2_alg2(h, 0.5, 25, 100, "Rel", 1e-10).rho
+    d2 = d @ d
+    for thr in (0.3, 0.1):
+        grp, gcol = G.density_square_graph(torch.tensor(d, device="cuda"), thr)
+        got = np.zeros((n, n), dtype=bool)
+        got[np.repeat(np.arange(n), np.diff(grp)), gcol] = True
+        ref = np.abs(d2) > thr
+        near = np.abs(np.abs(d2) - thr) < 1e-5
+        assert np.array_equal(got[~near], ref[~near])
+        for r in range(0, n, 97):                     # columns ascending in every row
+            c = gcol[grp[r]:grp[r + 1]]
+            assert np.all(np.diff(c) > 0)
