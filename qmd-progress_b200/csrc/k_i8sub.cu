@@ -7,7 +7,8 @@
 // as four balanced base-256 digits,
 //     M = d0 2^24 + d1 2^16 + d2 2^8 + d3,   d1, d2, d3 in [-128, 127], |d0| <= 65,
 // in four signed 8-bit planes.  Then 2^62 X'^2 = sum_{s,t} (D_s D_t) 2^{48 - 8(s+t)}, and
-// every plane product D_s D_t is exact in the 32-bit accumulators (|d| <= 128, K <= 512).
+// every plane product D_s D_t is exact in the 32-bit accumulators (|d| <= 128 and at most
+// four products per accumulator: |A_u| < 2^16 K <= 2^31 for any part size K <= 32768).
 // Products are grouped by u = s + t into five accumulators A_u (u = 0..4: thirteen
 // products); the three terms with u >= 5 lie below 2^-36 (typical) and are dropped.  The
 // epilogue forms P = 2^46 X'^2 = sum_u A_u 2^{32 - 8u} exactly in 64-bit integers and
