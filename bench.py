@@ -631,11 +631,11 @@ def measure_adjoint(n=2048, reps=5):
     K, ck = len(pp), 4
     stream = torch.cuda.current_stream()
 
-    def one():
+    def one(graphs=True):
         hv = h.clone().requires_grad_(True)
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         e0.record(stream)
-        d = sp2_density(hv, pp, lo, hi, ck)
+        d = sp2_density(hv, pp, lo, hi, ck, graphs)
         loss = (d * a).sum()
         e1.record(stream)
         loss.backward()
@@ -650,6 +650,12 @@ def measure_adjoint(n=2048, reps=5):
         fw.append(f)
         bw.append(b)
     f, b = statistics.median(fw), statistics.median(bw)
+    one(False)
+    fe, be = [], []
+    for _ in range(reps):
+        fx, bx, _ = one(False)
+        fe.append(fx)
+        be.append(bx)
     nseg = (K + ck - 1) // ck
     recomputed = K - nseg                      # steps replayed from the checkpoints
     flops_f = 2.0 * n ** 3 * K
@@ -659,7 +665,9 @@ def measure_adjoint(n=2048, reps=5):
             "forward_tflops": flops_f / (f / 1e3) / 1e12,
             "backward_tflops": flops_b / (b / 1e3) / 1e12,
             "grad_finite": bool(torch.isfinite(g).all().item()),
-            "kernels": "k_tc (split FP16 products), k_adjoint_combine (M + M^T)",
+            "eager_forward_ms": statistics.median(fe), "eager_backward_ms": statistics.median(be),
+            "kernels": "k_tc (split FP16 products), k_adjoint_combine (M + M^T); forward "
+                       "steps and backward replayed as CUDA graphs",
             "timing": f"median of {reps}, CUDA events"}
 
 

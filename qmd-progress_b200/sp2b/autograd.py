@@ -45,55 +45,112 @@ def _check_input(h: torch.Tensor):
     return h.contiguous()
 
 
+def _forward_steps(x, pp, checkpoint):
+    """X_K from X_0 (consumed), keeping X_k every `checkpoint` steps: (X_K, checkpoints)."""
+    ckpts = [x.clone()]
+    y = torch.empty_like(x)
+    for k, b in enumerate(pp):
+        _step(x, y, b)
+        x, y = y, x
+        if (k + 1) % checkpoint == 0 and k + 1 < len(pp):
+            ckpts.append(x.clone())
+    return x, ckpts
+
+
+def _backward_steps(g, ckpts, pp, c):
+    """G_0 from G_K and the checkpoints (g is overwritten)."""
+    K = len(pp)
+    work = torch.empty_like(g)
+    gout = torch.empty_like(g)
+    nseg = (K + c - 1) // c
+    for s in range(nseg - 1, -1, -1):
+        k0, k1 = s * c, min((s + 1) * c, K)
+        xs = [ckpts[s]]
+        for k in range(k0, k1 - 1):                # X_{k0+1} .. X_{k1-1} from the checkpoint
+            y = torch.empty_like(g)
+            _step(xs[-1], y, pp[k])
+            xs.append(y)
+        for k in range(k1 - 1, k0 - 1, -1):
+            _adjoint(g, xs[k - k0], gout, work, pp[k])
+            g, gout = gout, g
+    return g
+
+
+class _Replay:
+    """A CUDA graph of the forward steps or of the backward pass for one (device, n,
+    branch sequence, checkpoint spacing), captured after one eager run (which sizes the
+    library's buffers and makes its launch choices) and replayed with the inputs copied
+    into its static buffers.  The library's kernels go to the capturing stream, and the
+    tensors made during capture come from the graph's private pool."""
+    _cache = {}
+
+    def __init__(self, fn, inputs):
+        self.inputs = [t.clone() for t in inputs]
+        fn(*[t.clone() for t in self.inputs])      # eager warm-up outside the capture
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.outputs = fn(*self.inputs)
+
+    def run(self, inputs):
+        for dst, src in zip(self.inputs, inputs):
+            dst.copy_(src)
+        self.graph.replay()
+        return self.outputs
+
+    @classmethod
+    def get(cls, key, fn, inputs):
+        r = cls._cache.get(key)
+        if r is None:
+            r = cls._cache[key] = cls(fn, inputs)
+        return r
+
+
 class SP2Density(torch.autograd.Function):
     """D = SP2(H) with a fixed branch sequence and fixed bounds; see the module docstring."""
 
     @staticmethod
-    def forward(ctx, h, pp, mineval, maxeval, checkpoint=4):
+    def forward(ctx, h, pp, mineval, maxeval, checkpoint=4, use_graphs=True):
         h = _check_input(h)
         n = h.shape[0]
         pp = [int(b) for b in pp]
         x = torch.empty_like(h)
         _lib.check(_lib.lib().sp2b_dev_normalize_f32(h.data_ptr(), x.data_ptr(), n, float(mineval),
                                                      float(maxeval), _stream()), "normalize_f32")
-        ckpts = [x.clone()]
-        y = torch.empty_like(h)
-        for k, b in enumerate(pp):
-            _step(x, y, b)
-            x, y = y, x
-            if (k + 1) % checkpoint == 0 and k + 1 < len(pp):
-                ckpts.append(x.clone())
+        if use_graphs:
+            key = ("fwd", h.device.index, n, tuple(pp), checkpoint)
+            xk, ck = _Replay.get(key, lambda x0: _forward_steps(x0, pp, checkpoint), [x]).run([x])
+            xk, ckpts = xk.clone(), [t.clone() for t in ck]
+        else:
+            xk, ckpts = _forward_steps(x, pp, checkpoint)
         ctx.save_for_backward(*ckpts)
         ctx.pp = pp
         ctx.scale = -1.0 / (float(maxeval) - float(mineval))
         ctx.checkpoint = checkpoint
-        return 2.0 * x
+        ctx.use_graphs = use_graphs
+        return 2.0 * xk
 
     @staticmethod
     def backward(ctx, grad_d):
-        ckpts = ctx.saved_tensors
+        ckpts = list(ctx.saved_tensors)
         pp, c = ctx.pp, ctx.checkpoint
-        K = len(pp)
         g = (grad_d + grad_d.transpose(0, 1)).contiguous().float()   # dL/dX_K = 2 sym(dL/dD)
-        work = torch.empty_like(g)
-        gout = torch.empty_like(g)
-        nseg = (K + c - 1) // c
-        for s in range(nseg - 1, -1, -1):
-            k0, k1 = s * c, min((s + 1) * c, K)
-            xs = [ckpts[s]]
-            for k in range(k0, k1 - 1):            # X_{k0+1} .. X_{k1-1} from the checkpoint
-                y = torch.empty_like(g)
-                _step(xs[-1], y, pp[k])
-                xs.append(y)
-            for k in range(k1 - 1, k0 - 1, -1):
-                _adjoint(g, xs[k - k0], gout, work, pp[k])
-                g, gout = gout, g
-        return ctx.scale * g, None, None, None, None
+        if ctx.use_graphs:
+            key = ("bwd", g.device.index, g.shape[0], tuple(pp), c)
+            g0 = _Replay.get(key, lambda gk, *cs: _backward_steps(gk, list(cs), pp, c),
+                             [g] + ckpts).run([g] + ckpts).clone()
+        else:
+            g0 = _backward_steps(g, ckpts, pp, c)
+        return ctx.scale * g0, None, None, None, None, None
 
 
-def sp2_density(h: torch.Tensor, pp, mineval: float, maxeval: float, checkpoint: int = 4):
-    """Differentiable D(H) for a given branch sequence and bounds."""
-    return SP2Density.apply(h, pp, mineval, maxeval, checkpoint)
+def sp2_density(h: torch.Tensor, pp, mineval: float, maxeval: float, checkpoint: int = 4,
+                use_graphs: bool = True):
+    """Differentiable D(H) for a given branch sequence and bounds.  With use_graphs the
+    forward steps and the backward pass are replayed as CUDA graphs (captured on the first
+    call for this size, sequence and checkpoint spacing), which removes the per-step host
+    launch overhead; the results are the same."""
+    return SP2Density.apply(h, pp, mineval, maxeval, checkpoint, use_graphs)
 
 
 def sequence_and_bounds(h: torch.Tensor, bndfil: float, maxsp2iter: int = 100,

@@ -80,3 +80,25 @@ def test_adjoint_n2048_finite_differences_and_response(cuda):
     lhs = float(np.sum(g * h1))
     rhs = float(np.sum(rho1 * a))
     assert abs(lhs - rhs) <= 1e-5 * max(1.0, abs(rhs)), (lhs, rhs)
+
+
+def test_adjoint_graph_replay_equals_eager(cuda):
+    """The CUDA-graph replay of the forward steps and the backward pass gives the eager
+    path's D and gradient bit for bit, for a second H too (new inputs into the same
+    captured graphs)."""
+    torch = cuda
+    from sp2b.autograd import sequence_and_bounds, sp2_density
+    n = 256
+    a = torch.tensor(M.random_symmetric(n, seed=5), dtype=torch.float32, device="cuda")
+    h0 = M.two_band_1d(n, seed=21)
+    pp, lo, hi = sequence_and_bounds(torch.tensor(h0, device="cuda"), 0.5)
+    for seed in (21, 22):
+        h_np = M.two_band_1d(n, seed=seed)
+        out = []
+        for graphs in (True, False):
+            h = torch.tensor(h_np, dtype=torch.float32, device="cuda", requires_grad=True)
+            d = sp2_density(h, pp, lo, hi, 3, graphs)
+            (d * a).sum().backward()
+            out.append((d.detach().cpu().numpy(), h.grad.cpu().numpy()))
+        assert np.array_equal(out[0][0], out[1][0])
+        assert np.array_equal(out[0][1], out[1][1])

@@ -134,3 +134,17 @@ def test_int8_lattice_within_1e6_of_fp64_batch(cuda):
         assert rel <= 1e-6, (tol, rel)
         assert np.linalg.norm(c8 - c64) / n <= 1e-7
         assert np.allclose(vv8, vv64, rtol=1e-4, atol=2e-5)
+
+
+def test_int8_subgraph_parts_above_512(cuda):
+    """Parts larger than 512 (core+halo ~610): the digit planes come from the FP64
+    extraction (k_norm_digits) instead of straight from CSR; within 1e-7 of the oracle."""
+    n = 1400
+    h, g, parts, emin, emax, pp, maxiter = _setup(n, 600)
+    rho_ref, vv_ref, _ = O.subgraph_sp2_loop(h, g, parts, pp, maxiter, emin, emax)
+    hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
+    assert np.diff(hp).max() > 512
+    rho, _, vv = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin,
+                                        emax, precision=I8)
+    assert np.linalg.norm(rho - rho_ref) / np.linalg.norm(rho_ref) <= 1e-7
+    assert np.allclose(vv, O.fnorm_graph(vv_ref, maxiter), rtol=1e-5, atol=2e-6)
