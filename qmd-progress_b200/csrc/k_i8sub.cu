@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       for (int kb = 0; kb < ti.kb; ++kb, ++g) {
         const int s = g % i8s::ST;
         const uint32_t u = g / i8s::ST;
-        if (g >= (uint32_t)i8s::ST && !mbar_wait_warp(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+        if (g >= (uint32_t)i8s::ST && !mbar_wait_warp_idle(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
           ok = false;
           break;
         }
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       // the tile's X_k into staging buffer tl & 1, once the stores of the tile that used
       // it two items ago have read it
       const int b = tl & 1;
-      if (tl >= 2 && !mbar_wait_warp(smem_u32(&bar_free[b]), ((tl - 2) >> 1) & 1, &s_abort)) {
+      if (tl >= 2 && !mbar_wait_warp_idle(smem_u32(&bar_free[b]), ((tl - 2) >> 1) & 1, &s_abort)) {
         ok = false;
         break;
       }
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       item_of(i, k, t);
       const I8Tile ti = i8_tile_uniform(p.tiles, t);
       const int b = tl & 1;
-      if (!mbar_wait_warp(smem_u32(&bar_staged[b]), (tl >> 1) & 1, &s_abort)) break;
+      if (!mbar_wait_warp_idle(smem_u32(&bar_staged[b]), (tl >> 1) & 1, &s_abort)) break;
       if (elect_one()) {
 #pragma unroll
         for (int d = 0; d < i8s::ND; ++d)
@@ -518,6 +518,17 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
         u4[1] = __byte_perm(alo, blo, 0x7632u);
         u4[2] = __byte_perm(ahi, bhi, 0x5410u);
         u4[3] = __byte_perm(ahi, bhi, 0x7632u);
+        if (cuni) {
+          // off the diagonal, one weight: X'_{k+1} = X' +- X'^2, residual^2 = Q^2
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int j = 4 * g + e;
+            wn[j] = ((u4[e] ^ kB) + (uint32_t)(sg * Q[j])) ^ kB;
+            const float qf = (float)Q[j];
+            s_res = fmaf(qf, qf, s_res);
+          }
+          continue;
+        }
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int j = 4 * g + e;
@@ -528,9 +539,7 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
           wn[j] = nb ^ kB;
           // 2^31 (X - X^2) = 2^31 (I/4 - X'^2), from the rounded square
           const float res = (float)((dg ? (1 << 29) : 0) - Q[j]);
-          if (cuni) {
-            s_res = fmaf(res, res, s_res);
-          } else {
+          {
             // weight of (r, c) in the full-matrix sums: itself and its mirror above the
             // diagonal, once on it, nothing below it (its mirror above carries it)
             const int w = r < c ? 2 : (dg ? 1 : 0);

@@ -146,6 +146,13 @@ __device__ __forceinline__ bool mbar_wait_warp(uint32_t a, uint32_t parity, vola
   const bool ok = mbar_wait(a, parity, abort_flag);
   return __all_sync(0xffffffffu, ok) != 0;
 }
+// The same with sleeps between polls, for warps whose wait is not on the critical path
+// (their polls would take issue slots from the warps they share a scheduler with).
+__device__ __forceinline__ bool mbar_wait_warp_idle(uint32_t a, uint32_t parity,
+                                                    volatile int* abort_flag) {
+  const bool ok = mbar_wait_idle(a, parity, abort_flag);
+  return __all_sync(0xffffffffu, ok) != 0;
+}
 __device__ __forceinline__ void umma_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    mbar)
