@@ -1,5 +1,5 @@
-// Batched sub-graph SP2 step on the INT8 tensor cores with exact integer products
-// ("INT8 digit split").
+// Batched sub-graph SP2 on the INT8 tensor cores with exact integer products ("INT8
+// digit split"): every step of every part in one persistent launch (k_i8_steps).
 //
 // The iterate is held in fixed point, shifted so that every entry fits the same range:
 // X' = X - I/2 has its spectrum in [-1/2, 1/2] (Gershgorin-normalised X has it in [0, 1]),
@@ -11,8 +11,8 @@
 // four products per accumulator: |A_u| < 2^16 K <= 2^31 for any part size K <= 32768).
 // Products are grouped by u = s + t into five accumulators A_u (u = 0..4: thirteen
 // products); the three terms with u >= 5 lie below 2^-36 (typical) and are dropped.  The
-// epilogue forms P = 2^46 X'^2 = sum_u A_u 2^{32 - 8u} exactly in 64-bit integers and
-// applies the SP2 branch in the shifted variable,
+// epilogue rounds P = 2^46 X'^2 = sum_u A_u 2^{32 - 8u} to Q = rint(2^31 X'^2) exactly
+// with 32-bit integer steps and applies the SP2 branch in the shifted variable,
 //     X^2 branch:      X'_{k+1} = X'^2 + X' - I/4,
 //     2X - X^2 branch: X'_{k+1} = X' - X'^2 + I/4,
 // as M_{k+1} = M_k +- rint(2^31 X'^2) -+ 2^29 [i == j].  The only rounding per step is

@@ -141,10 +141,11 @@ def test_distributed_path_single_rank_gpu_solver(cuda, tmp_path):
     assert np.allclose(vv, vv_loc, rtol=1e-12, atol=0)
 
 
-def test_distributed_path_nccl_device_exchange(cuda, tmp_path):
+@pytest.mark.parametrize("prec", [sp2b.PREC_FP64, sp2b.PREC_EXACT_INT8])
+def test_distributed_path_nccl_device_exchange(cuda, tmp_path, prec):
     """The sharded loop with NCCL on device tensors (one rank): the all-gathered core
     rows placed into the dense density on the device (sp2b_place_core_rows) equal the
-    local call's density."""
+    local call's density, for the FP64 batch and for the persistent INT8 form."""
     import torch.distributed as dist
     from sp2b import dist as D
     torch = cuda
@@ -152,13 +153,13 @@ def test_distributed_path_nccl_device_exchange(cuda, tmp_path):
     h, g, parts, emin, emax, pp, maxiter = _setup(n)
     hp, hi, ls, lls = sp2b.subgraph_halos(n, sp2b.dense_to_csr(g), parts, sp2b.dense_to_csr(h))
     rho_loc, _, vv_loc = sp2b.subgraph_sp2_loop(n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter,
-                                                emin, emax, precision=sp2b.PREC_FP64)
+                                                emin, emax, precision=prec)
     dist.init_process_group("nccl", init_method=f"file://{tmp_path}/pg", rank=0, world_size=1,
                             device_id=torch.device("cuda", 0))
     try:
         rho, vv, owner = D.subgraph_sp2_loop_distributed(
             n, sp2b.dense_to_csr(h), hp, hi, lls, pp, maxiter, emin, emax,
-            D.gpu_solver(sp2b.PREC_FP64), device=torch.device("cuda", 0))
+            D.gpu_solver(prec), device=torch.device("cuda", 0))
         torch.cuda.synchronize()
     finally:
         dist.destroy_process_group()
