@@ -59,9 +59,11 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="two_band", choices=["two_band", "subgraph", "cubic_dense"],
+    ap.add_argument("--workload", default="two_band",
+                    choices=["two_band", "subgraph", "cubic_dense", "adjoint"],
                     help="two_band: dense config (default); subgraph: 32^3 lattice, 256 parts; "
-                         "cubic_dense: the 32^3 lattice solved densely (N=32768)")
+                         "cubic_dense: the 32^3 lattice solved densely (N=32768); adjoint: the "
+                         "differentiable SP2's forward and backward at N=2048")
     ap.add_argument("--L", type=int, default=32, help="subgraph: lattice edge")
     ap.add_argument("--parts", type=int, default=256, help="subgraph: number of parts")
     ap.add_argument("--subgraph-precision", default="exact_int8",
@@ -374,6 +376,8 @@ def main():
         return run_subgraph(args, rank, world, local)
     if args.workload == "cubic_dense":
         return run_cubic_dense(args, rank, local)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, local)
 
     import numpy as np
     import torch
@@ -596,6 +600,24 @@ def main():
         dist.destroy_process_group()
 
 
+def run_adjoint(args, rank, local):
+    """bench.py --workload adjoint: the differentiable SP2's forward and backward
+    (measure_adjoint) as its own line; value = gradients (forward + backward) per second.
+    Under torchrun every rank runs an independent replica and rank 0 prints."""
+    import torch
+    torch.cuda.set_device(local)
+    adj = measure_adjoint(reps=max(args.steps, 1))
+    if rank == 0:
+        ms = adj["forward_ms"] + adj["backward_ms"]
+        print(json.dumps({"metric": "sp2_gradients_per_s", "value": 1e3 / ms, "unit": "gradients/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": 2, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f16", "data": "synthetic",
+                          "config": {"workload": adj["workload"], "n": adj["n"],
+                                     "sp2_steps": adj["sp2_steps"]},
+                          "adjoint": adj}), flush=True)
+
+
 def run_subgraph(args, rank, world, local):
     """bench.py --workload subgraph: the batched sub-graph measurement as its own line."""
     import torch
@@ -617,10 +639,11 @@ def run_subgraph(args, rank, world, local):
 def measure_adjoint(n=2048, reps=5):
     """Config 3: the differentiable SP2 (sp2b.autograd.SP2Density) on the two-band model,
     N = 2048, loss Tr(D A) with a random symmetric A; forward (replay of the genseq branch
-    sequence, FP32 storage, split-precision squarings, X kept every 4 steps) and backward
-    (segments recomputed from the checkpoints, one product M = G X and M + M^T per step)
-    timed with CUDA events on the current stream.  Algorithmic flops: 2 n^3 per forward
-    step; backward 2 n^3 per adjoint step plus the recomputed steps."""
+    sequence, iterates kept in the FP16 hi/lo split form, one symmetric split product per
+    step, X kept every 4 steps) and backward (segments recomputed from the checkpoints,
+    one symmetric product over the concatenated K range [G | X][X | G]^T per reverse
+    step) timed with CUDA events on the current stream.  Algorithmic flops: 2 n^3 per
+    forward step; backward 2 n^3 per reverse step plus the recomputed steps."""
     import torch
     import sp2b
     from sp2b import modelham as M
@@ -666,8 +689,9 @@ def measure_adjoint(n=2048, reps=5):
             "backward_tflops": flops_b / (b / 1e3) / 1e12,
             "grad_finite": bool(torch.isfinite(g).all().item()),
             "eager_forward_ms": statistics.median(fe), "eager_backward_ms": statistics.median(be),
-            "kernels": "k_tc (split FP16 products), k_adjoint_combine (M + M^T); forward "
-                       "steps and backward replayed as CUDA graphs",
+            "kernels": "k_tc_pair (split FP16 symmetric products: X^2, and {G, X} over the "
+                       "concatenated K range); forward steps and backward replayed as CUDA "
+                       "graphs",
             "timing": f"median of {reps}, CUDA events"}
 
 

@@ -371,6 +371,31 @@ int sp2b_dev_sp2_step_f32(const float* x, float* y, int n, int branch, void* str
 int sp2b_dev_adjoint_step_f32(const float* g, const float* x, float* g_out, float* work, int n,
                               int branch, void* stream);
 
+/* The same steps with X and G kept in the FP16 hi + lo split form between steps (lo
+ * scaled by 2^11; x = hi + 2^-11 lo), so no conversion runs between products.  Each
+ * split matrix is two np x np half arrays (hi, lo), np = sp2b_split_dim(n), row pitch
+ * np, zeros outside the n x n block (every entry below writes the padding).
+ *   normalize_split:    split X_0 = (maxeval I - h)/(maxeval - mineval) from FP32 h
+ *   f32_to_split / split_to_f32: conversions; split_to_f32 writes y = scale x (n x n)
+ *   sp2_step_split:     y = x^2 (branch 1) or 2x - x^2 (branch 0); one symmetric
+ *                       product whose epilogue writes the split y (y must not alias x)
+ *   adjoint_step_split: o = {g, x} (branch 1) or 2g - {g, x} (branch 0), g and x
+ *                       symmetric, formed as one symmetric product over the
+ *                       concatenated K range [g | x][x | g]^T with the branch in its
+ *                       epilogue when np is a multiple of 256 (else g x in FP32 and a
+ *                       combine pass); o must not alias g or x. */
+int sp2b_split_dim(int n);
+int sp2b_dev_normalize_split(const float* h, int n, double mineval, double maxeval, void* x_hi,
+                             void* x_lo, void* stream);
+int sp2b_dev_f32_to_split(const float* a, int n, void* hi, void* lo, void* stream);
+int sp2b_dev_split_to_f32(const void* hi, const void* lo, int n, double scale, float* y,
+                          void* stream);
+int sp2b_dev_sp2_step_split(const void* x_hi, const void* x_lo, void* y_hi, void* y_lo, int n,
+                            int branch, void* stream);
+int sp2b_dev_adjoint_step_split(const void* g_hi, const void* g_lo, const void* x_hi,
+                                const void* x_lo, void* o_hi, void* o_lo, int n, int branch,
+                                void* stream);
+
 /* ---- diagnostics ------------------------------------------------------------------ */
 
 /* State of the last dense solve on the current device: SP2 step launches issued by

@@ -906,6 +906,10 @@ __global__ void __launch_bounds__(ESM ? tcp::NTHR_E : tcp::NTHR, 1)
 // epilogue as the single-CTA kernel on its own 128 x 128 block (TMEM double-buffered).
 // Work item w = {bi2, bj}: rows 256 bi2 .. +255, columns 128 bj .. +127, bj >= 2 bi2; the
 // block of CTA 1 is skipped by its epilogue when it lies below the diagonal.
+// ANTI: the anticommutator {G, X} = G X + X G of two symmetric matrices as one symmetric
+// product over the concatenated K range, [G | X] [X | G]^T: the K loop runs twice over
+// the columns, the second time with the operands' roles swapped (tm_a2* holds X in the
+// A role, tm_b2* G in the B role), so the one accumulator sums both products.
 // ---------------------------------------------------------------------------------
 namespace tcq {
 constexpr int BH = 64;                                  // B rows staged per CTA (N / 2)
@@ -917,10 +921,12 @@ constexpr int SCR_OFF = ST * STAGE_BYTES;
 constexpr int SMEM_BYTES = SCR_OFF + tcp::EPI_WARPS * tcp::SCR_WARP + 1024;
 }  // namespace tcq
 
-template <typename T, int EPI>
+template <typename T, int EPI, bool ANTI = false>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
     k_tc_pair(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
               const __grid_constant__ CUtensorMap tm_bhi, const __grid_constant__ CUtensorMap tm_blo,
+              const __grid_constant__ CUtensorMap tm_a2hi, const __grid_constant__ CUtensorMap tm_a2lo,
+              const __grid_constant__ CUtensorMap tm_b2hi, const __grid_constant__ CUtensorMap tm_b2lo,
               const StepArgs p, const int2* __restrict__ ptiles, int ntiles) {
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_full[tcq::ST];
@@ -966,6 +972,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
   tc_fence_after();
   const uint32_t tmem = tmem_holder;
   const int KB = p.np / tc::BK;
+  const int KBT = ANTI ? 2 * KB : KB;   // K-blocks per tile
   double sums[4] = {0.0, 0.0, 0.0, 0.0};
 
   if (warp == 0) {
@@ -977,7 +984,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
         const int2 tile = ptiles[w];
         const int ra = tile.x * 2 * tc::BM + (int)rank * tc::BM;
         const int rb = tile.y * tc::BN + (int)rank * tcq::BH;
-        for (int kb = 0; kb < KB; ++kb, ++g) {
+        for (int kb = 0; kb < KBT; ++kb, ++g) {
           const int s = g % tcq::ST;
           const uint32_t u = g / tcq::ST;
           if (g >= (uint32_t)tcq::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
@@ -987,10 +994,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
           const uint32_t fb0 = map_to_rank(smem_u32(&bar_full[s]), 0);
           if (rank == 0) mbar_expect_tx(smem_u32(&bar_full[s]), 2 * tcq::STAGE_BYTES);
           const uint32_t st = sbase + s * tcq::STAGE_BYTES;
-          tma_load_2d_pair(st, &tm_ahi, fb0, kb * tc::BK, ra);
-          tma_load_2d_pair(st + tcq::A_BYTES, &tm_alo, fb0, kb * tc::BK, ra);
-          tma_load_2d_pair(st + 2 * tcq::A_BYTES, &tm_bhi, fb0, kb * tc::BK, rb);
-          tma_load_2d_pair(st + 2 * tcq::A_BYTES + tcq::BH_BYTES, &tm_blo, fb0, kb * tc::BK, rb);
+          const bool sw = ANTI && kb >= KB;    // second pass: roles swapped
+          const int kc = (sw ? kb - KB : kb) * tc::BK;
+          tma_load_2d_pair(st, sw ? &tm_a2hi : &tm_ahi, fb0, kc, ra);
+          tma_load_2d_pair(st + tcq::A_BYTES, sw ? &tm_a2lo : &tm_alo, fb0, kc, ra);
+          tma_load_2d_pair(st + 2 * tcq::A_BYTES, sw ? &tm_b2hi : &tm_bhi, fb0, kc, rb);
+          tma_load_2d_pair(st + 2 * tcq::A_BYTES + tcq::BH_BYTES, sw ? &tm_b2lo : &tm_blo, fb0, kc,
+                           rb);
         }
       }
       if (!ok) s_abort = 1;
@@ -1011,7 +1021,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
         }
         tc_fence_after();
         const uint32_t acc_hh = tmem + a * 256, acc_x = tmem + a * 256 + tc::BN;
-        for (int kb = 0; kb < KB; ++kb, ++g) {
+        for (int kb = 0; kb < KBT; ++kb, ++g) {
           const int s = g % tcq::ST;
           if (!mbar_wait(smem_u32(&bar_full[s]), (g / tcq::ST) & 1, &s_abort)) {
             ok = false;
@@ -1296,9 +1306,6 @@ void panel_tile_order(int nb, int panel, std::vector<int2>& out) {
 }
 
 static const int4* dense_tiles(int np, cudaStream_t st) {
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
-    return nullptr;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   static std::mutex mu;
@@ -1306,6 +1313,10 @@ static const int4* dense_tiles(int np, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(mu);
   auto it = cache.find({dev, np});
   if (it != cache.end()) return it->second;
+  // a new list needs an allocation and a copy, neither of which a stream capture allows
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return nullptr;
   std::vector<int2> order;
   panel_tile_order(np / tc::BM, kPanel, order);
   std::vector<int4> t(order.size());
@@ -1333,9 +1344,6 @@ void pair_tile_order(int nb, int panel, std::vector<int2>& out) {
 }
 
 static const int2* pair_tiles(int np, cudaStream_t st, int* count) {
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
-    return nullptr;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   static std::mutex mu;
@@ -1346,6 +1354,10 @@ static const int2* pair_tiles(int np, cudaStream_t st, int* count) {
     *count = it->second.second;
     return it->second.first;
   }
+  // a new list needs an allocation and a copy, neither of which a stream capture allows
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return nullptr;
   std::vector<int2> t;
   pair_tile_order(np / tc::BM, kPanel, t);
   int2* d = nullptr;
@@ -1360,7 +1372,7 @@ static const int2* pair_tiles(int np, cudaStream_t st, int* count) {
 }
 
 // Clusters of the paired kernel that can be resident at once (one CTA per SM).
-template <typename T, int EPI>
+template <typename T, int EPI, bool ANTI = false>
 static int pair_clusters() {
   static int per_dev[64] = {0};
   int dev = 0;
@@ -1378,7 +1390,8 @@ static int pair_clusters() {
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, (void*)k_tc_pair<T, EPI>, &cfg) != cudaSuccess || n <= 0) {
+  if (cudaOccupancyMaxActiveClusters(&n, (void*)k_tc_pair<T, EPI, ANTI>, &cfg) != cudaSuccess ||
+      n <= 0) {
     cudaGetLastError();
     n = num_sms() / 2;
   }
@@ -1387,26 +1400,36 @@ static int pair_clusters() {
 }
 
 // Paired-CTA launch for np a multiple of 256; returns cudaErrorNotSupported when the
-// caller should use the single-CTA kernel instead.
-template <typename T, int EPI>
+// caller should use the single-CTA kernel instead.  ANTI: A = G, B = X (see k_tc_pair).
+template <typename T, int EPI, bool ANTI = false>
 static cudaError_t launch_pair(const StepArgs& a, cudaStream_t st) {
   if (a.np % (2 * tc::BM) != 0 || a.ld != a.np) return cudaErrorNotSupported;
   int ntiles = 0;
   const int2* tl = pair_tiles(a.np, st, &ntiles);
   if (!tl || ntiles <= 0) return cudaErrorNotSupported;
   const int type = std::is_same<T, __nv_bfloat16>::value ? TMAP_BF16 : TMAP_F16;
-  CUtensorMap m[4];
+  CUtensorMap m[8];
   if (!make_tmap_box(&m[0], a.A, a.np, a.np, a.np, type, tc::BM) ||
       !make_tmap_box(&m[1], a.A_lo, a.np, a.np, a.np, type, tc::BM) ||
       !make_tmap_box(&m[2], a.B, a.np, a.np, a.np, type, tcq::BH) ||
       !make_tmap_box(&m[3], a.B_lo, a.np, a.np, a.np, type, tcq::BH))
     return cudaErrorInvalidValue;
-  auto kern = k_tc_pair<T, EPI>;
+  if (ANTI) {
+    if (!make_tmap_box(&m[4], a.B, a.np, a.np, a.np, type, tc::BM) ||
+        !make_tmap_box(&m[5], a.B_lo, a.np, a.np, a.np, type, tc::BM) ||
+        !make_tmap_box(&m[6], a.A, a.np, a.np, a.np, type, tcq::BH) ||
+        !make_tmap_box(&m[7], a.A_lo, a.np, a.np, a.np, type, tcq::BH))
+      return cudaErrorInvalidValue;
+  } else {
+    for (int i = 0; i < 4; ++i) m[4 + i] = m[i];   // unused
+  }
+  auto kern = k_tc_pair<T, EPI, ANTI>;
   cudaError_t e =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tcq::SMEM_BYTES);
   if (e != cudaSuccess) return e;
-  const int clusters = std::min(ntiles, pair_clusters<T, EPI>());
-  kern<<<2 * clusters, tcp::NTHR, tcq::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], a, tl, ntiles);
+  const int clusters = std::min(ntiles, pair_clusters<T, EPI, ANTI>());
+  kern<<<2 * clusters, tcp::NTHR, tcq::SMEM_BYTES, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6],
+                                                         m[7], a, tl, ntiles);
   note_launch();
   return cudaGetLastError();
 }
@@ -1423,6 +1446,17 @@ cudaError_t launch_sym_gemm_tc(const StepArgs& a0, int bf16, cudaStream_t st) {
   const int nt = tc_ntiles(a.np);
   return bf16 ? launch_persist<__nv_bfloat16, 0>(a, a.np, nt, st)
               : launch_persist<__half, 0>(a, a.np, nt, st);
+}
+
+// {G, X} on the upper tiles, out = alpha {G, X} + beta E (E = G for the adjoint step):
+// a.A / a.A_lo = G, a.B / a.B_lo = X.  cudaErrorNotSupported when np is not a multiple
+// of 256 (the caller forms G X with launch_tc_plain and combines).
+cudaError_t launch_anti_tc(const StepArgs& a0, cudaStream_t st) {
+  if (a0.np % tc::BM != 0) return cudaErrorInvalidValue;
+  StepArgs a = a0;
+  a.tiles = nullptr;
+  a.ld = a.np;
+  return launch_pair<__half, 0, true>(a, st);
 }
 
 cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,

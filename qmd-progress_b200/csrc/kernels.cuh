@@ -106,6 +106,10 @@ cudaError_t launch_normalize_split(const double* h, int n, int ld, int np,
                                    double* partials, unsigned* counter, SP2Rec* rec0,
                                    double* norm_out, cudaStream_t st);
 cudaError_t launch_sym_gemm_tc(const StepArgs& a, int bf16, cudaStream_t st);
+// {G, X} = G X + X G of symmetric split matrices (A = G, B = X) on the upper tiles in one
+// pass over the concatenated K range; out = alpha {G, X} + beta E.  FP16 split only;
+// cudaErrorNotSupported unless np is a multiple of 256.
+cudaError_t launch_anti_tc(const StepArgs& a, cudaStream_t st);
 // batched parts: A/B tensors are rows x ld packed buffers
 cudaError_t launch_sym_gemm_tc_batched(const StepArgs& a, long long rows, int bf16,
                                        cudaStream_t st);

@@ -84,6 +84,12 @@ _SIGS = {
     "sp2b_dev_normalize_f32": (_i, [_vp, _vp, _i, _d, _d, _vp]),
     "sp2b_dev_sp2_step_f32": (_i, [_vp, _vp, _i, _i, _vp]),
     "sp2b_dev_adjoint_step_f32": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
+    "sp2b_split_dim": (_i, [_i]),
+    "sp2b_dev_normalize_split": (_i, [_vp, _i, _d, _d, _vp, _vp, _vp]),
+    "sp2b_dev_f32_to_split": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "sp2b_dev_split_to_f32": (_i, [_vp, _vp, _i, _d, _vp, _vp]),
+    "sp2b_dev_sp2_step_split": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
+    "sp2b_dev_adjoint_step_split": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "sp2b_last_solve_info": (_i, [_ip, _ip, _ip, _ip, _vp, _i]),
     "sp2b_last_subgraph_refined": (_i, [_ip, _vp, _i, _vp, _i]),
     "sp2b_graph_square_threshold": (_i, [_i, _vp, _vp, _vp, _d, _vp, _vp, C.c_longlong, _vp,

@@ -4,11 +4,15 @@ torch.autograd.Function, giving d(Tr D A)/dH for response and force workloads.
 Forward (replaying a branch sequence pp with fixed bounds, like prg_sp2_alg2_seq,
 src/prg_sp2_mod.F90:543-627):  X_0 = (e_max I - H)/(e_max - e_min),
 X_{k+1} = X_k^2 (pp_k = 1) or 2 X_k - X_k^2 (pp_k = 0), D = 2 X_K.
-FP32 storage, squarings as FP16 hi+lo split products on the tensor cores.
+The iterates stay in the FP16 hi + lo split form between steps (a (2, np, np) half
+tensor: hi, lo); each step is one symmetric split product on the tensor cores (FP32
+accumulation) whose epilogue writes the next split iterate.  H and D are FP32.
 
 Backward: G_K = dL/dX_K = 2 sym(dL/dD); G_k = {G_{k+1}, X_k} or 2 G_{k+1} - {G_{k+1}, X_k};
-dL/dH = -G_0/(e_max - e_min).  The forward keeps X_k every `checkpoint` steps; the
-backward recomputes each segment from its checkpoint.  The Gershgorin bounds and the
+dL/dH = -G_0/(e_max - e_min).  Each reverse step is one symmetric split product over
+the concatenated K range, [G | X_k][X_k | G]^T = G X_k + X_k G, with the branch applied
+in its epilogue.  The forward keeps X_k every `checkpoint` steps; the backward
+recomputes each segment from its checkpoint.  The Gershgorin bounds and the
 branch sequence are held fixed (they are piecewise constant in H), which is what the
 reference's density-matrix perturbation theory does (prg_compute_response_SP2,
 src/prg_response_mod.F90:653-782, propagates a perturbation through the same
@@ -28,15 +32,30 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
-def _step(x: torch.Tensor, y: torch.Tensor, branch: int):
-    _lib.check(_lib.lib().sp2b_dev_sp2_step_f32(x.data_ptr(), y.data_ptr(), x.shape[0], int(branch),
-                                                _stream()), "sp2_step_f32")
+def _split(n: int, device) -> torch.Tensor:
+    """An uninitialised split matrix: (2, np, np) halves, [0] = hi, [1] = lo."""
+    np_ = int(_lib.lib().sp2b_split_dim(n))
+    return torch.empty(2, np_, np_, dtype=torch.float16, device=device)
 
 
-def _adjoint(g: torch.Tensor, x: torch.Tensor, out: torch.Tensor, work: torch.Tensor, branch: int):
-    _lib.check(_lib.lib().sp2b_dev_adjoint_step_f32(g.data_ptr(), x.data_ptr(), out.data_ptr(),
-                                                    work.data_ptr(), x.shape[0], int(branch),
-                                                    _stream()), "adjoint_step_f32")
+def _step(x: torch.Tensor, y: torch.Tensor, branch: int, n: int):
+    _lib.check(_lib.lib().sp2b_dev_sp2_step_split(x[0].data_ptr(), x[1].data_ptr(), y[0].data_ptr(),
+                                                  y[1].data_ptr(), n, int(branch), _stream()),
+               "sp2_step_split")
+
+
+def _adjoint(g: torch.Tensor, x: torch.Tensor, out: torch.Tensor, branch: int, n: int):
+    _lib.check(_lib.lib().sp2b_dev_adjoint_step_split(g[0].data_ptr(), g[1].data_ptr(),
+                                                      x[0].data_ptr(), x[1].data_ptr(),
+                                                      out[0].data_ptr(), out[1].data_ptr(), n,
+                                                      int(branch), _stream()), "adjoint_step_split")
+
+
+def _to_f32(x: torch.Tensor, n: int, scale: float) -> torch.Tensor:
+    y = torch.empty(n, n, dtype=torch.float32, device=x.device)
+    _lib.check(_lib.lib().sp2b_dev_split_to_f32(x[0].data_ptr(), x[1].data_ptr(), n, float(scale),
+                                                y.data_ptr(), _stream()), "split_to_f32")
+    return y
 
 
 def _check_input(h: torch.Tensor):
@@ -45,22 +64,22 @@ def _check_input(h: torch.Tensor):
     return h.contiguous()
 
 
-def _forward_steps(x, pp, checkpoint):
-    """X_K from X_0 (consumed), keeping X_k every `checkpoint` steps: (X_K, checkpoints)."""
+def _forward_steps(x, pp, checkpoint, n):
+    """Split X_K from split X_0 (consumed), keeping X_k every `checkpoint` steps:
+    (X_K, checkpoints)."""
     ckpts = [x.clone()]
     y = torch.empty_like(x)
     for k, b in enumerate(pp):
-        _step(x, y, b)
+        _step(x, y, b, n)
         x, y = y, x
         if (k + 1) % checkpoint == 0 and k + 1 < len(pp):
             ckpts.append(x.clone())
     return x, ckpts
 
 
-def _backward_steps(g, ckpts, pp, c):
-    """G_0 from G_K and the checkpoints (g is overwritten)."""
+def _backward_steps(g, ckpts, pp, c, n):
+    """Split G_0 from split G_K and the split checkpoints (g is overwritten)."""
     K = len(pp)
-    work = torch.empty_like(g)
     gout = torch.empty_like(g)
     nseg = (K + c - 1) // c
     for s in range(nseg - 1, -1, -1):
@@ -68,10 +87,10 @@ def _backward_steps(g, ckpts, pp, c):
         xs = [ckpts[s]]
         for k in range(k0, k1 - 1):                # X_{k0+1} .. X_{k1-1} from the checkpoint
             y = torch.empty_like(g)
-            _step(xs[-1], y, pp[k])
+            _step(xs[-1], y, pp[k], n)
             xs.append(y)
         for k in range(k1 - 1, k0 - 1, -1):
-            _adjoint(g, xs[k - k0], gout, work, pp[k])
+            _adjoint(g, xs[k - k0], gout, pp[k], n)
             g, gout = gout, g
     return g
 
@@ -114,34 +133,39 @@ class SP2Density(torch.autograd.Function):
         h = _check_input(h)
         n = h.shape[0]
         pp = [int(b) for b in pp]
-        x = torch.empty_like(h)
-        _lib.check(_lib.lib().sp2b_dev_normalize_f32(h.data_ptr(), x.data_ptr(), n, float(mineval),
-                                                     float(maxeval), _stream()), "normalize_f32")
+        x = _split(n, h.device)
+        _lib.check(_lib.lib().sp2b_dev_normalize_split(h.data_ptr(), n, float(mineval),
+                                                       float(maxeval), x[0].data_ptr(),
+                                                       x[1].data_ptr(), _stream()), "normalize_split")
         if use_graphs:
             key = ("fwd", h.device.index, n, tuple(pp), checkpoint)
-            xk, ck = _Replay.get(key, lambda x0: _forward_steps(x0, pp, checkpoint), [x]).run([x])
-            xk, ckpts = xk.clone(), [t.clone() for t in ck]
+            xk, ck = _Replay.get(key, lambda x0: _forward_steps(x0, pp, checkpoint, n), [x]).run([x])
+            ckpts = [t.clone() for t in ck]
         else:
-            xk, ckpts = _forward_steps(x, pp, checkpoint)
+            xk, ckpts = _forward_steps(x, pp, checkpoint, n)
         ctx.save_for_backward(*ckpts)
         ctx.pp = pp
+        ctx.n = n
         ctx.scale = -1.0 / (float(maxeval) - float(mineval))
         ctx.checkpoint = checkpoint
         ctx.use_graphs = use_graphs
-        return 2.0 * xk
+        return _to_f32(xk, n, 2.0)
 
     @staticmethod
     def backward(ctx, grad_d):
         ckpts = list(ctx.saved_tensors)
-        pp, c = ctx.pp, ctx.checkpoint
-        g = (grad_d + grad_d.transpose(0, 1)).contiguous().float()   # dL/dX_K = 2 sym(dL/dD)
+        pp, c, n = ctx.pp, ctx.checkpoint, ctx.n
+        gf = (grad_d + grad_d.transpose(0, 1)).contiguous().float()  # dL/dX_K = 2 sym(dL/dD)
+        g = _split(n, gf.device)
+        _lib.check(_lib.lib().sp2b_dev_f32_to_split(gf.data_ptr(), n, g[0].data_ptr(),
+                                                    g[1].data_ptr(), _stream()), "f32_to_split")
         if ctx.use_graphs:
-            key = ("bwd", g.device.index, g.shape[0], tuple(pp), c)
-            g0 = _Replay.get(key, lambda gk, *cs: _backward_steps(gk, list(cs), pp, c),
-                             [g] + ckpts).run([g] + ckpts).clone()
+            key = ("bwd", g.device.index, n, tuple(pp), c)
+            g0 = _Replay.get(key, lambda gk, *cs: _backward_steps(gk, list(cs), pp, c, n),
+                             [g] + ckpts).run([g] + ckpts)
         else:
-            g0 = _backward_steps(g, ckpts, pp, c)
-        return ctx.scale * g0, None, None, None, None, None
+            g0 = _backward_steps(g, ckpts, pp, c, n)
+        return _to_f32(g0, n, ctx.scale), None, None, None, None, None
 
 
 def sp2_density(h: torch.Tensor, pp, mineval: float, maxeval: float, checkpoint: int = 4,

@@ -102,3 +102,68 @@ def test_adjoint_graph_replay_equals_eager(cuda):
             out.append((d.detach().cpu().numpy(), h.grad.cpu().numpy()))
         assert np.array_equal(out[0][0], out[1][0])
         assert np.array_equal(out[0][1], out[1][1])
+
+
+def _to_split(torch, a):
+    """(2, np, np) half split of an FP32 n x n tensor through the library."""
+    import ctypes as C
+    from sp2b import _lib
+    n = a.shape[0]
+    np_ = _lib.lib().sp2b_split_dim(n)
+    s = torch.empty(2, np_, np_, dtype=torch.float16, device="cuda")
+    _lib.check(_lib.lib().sp2b_dev_f32_to_split(a.data_ptr(), n, s[0].data_ptr(), s[1].data_ptr(),
+                                                C.c_void_p(0)), "f32_to_split")
+    return s
+
+
+def _from_split(torch, s, n):
+    import ctypes as C
+    from sp2b import _lib
+    y = torch.empty(n, n, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib().sp2b_dev_split_to_f32(s[0].data_ptr(), s[1].data_ptr(), n, 1.0,
+                                                y.data_ptr(), C.c_void_p(0)), "split_to_f32")
+    torch.cuda.synchronize()
+    return y.double().cpu().numpy()
+
+
+@pytest.mark.parametrize("n", [300, 512, 1000])
+@pytest.mark.parametrize("branch", [0, 1])
+def test_split_step_and_anticommutator_match_fp64(cuda, n, branch):
+    """The split-form entries of the autograd path: one SP2 step and one reverse step
+    ({G, X} as one product over the concatenated K range when np is a multiple of 256,
+    n = 512 / 1000; G X and a combine pass otherwise, n = 300) against FP64 on the
+    FP32-rounded inputs.  The bound is relative to the product of the absolute values
+    (|X||X|, |G||X| + |X||G|): random signs cancel in the product itself, and the split
+    products' error (22-bit operands, FP32 accumulation) scales with the absolute terms."""
+    torch = cuda
+    import ctypes as C
+    from sp2b import _lib
+    x = M.random_symmetric(n, seed=n)
+    x /= np.abs(x).sum(axis=1).max()                 # spectral radius <= 1, like X_k
+    g = M.random_symmetric(n, seed=n + 1)
+    xs = _to_split(torch, torch.tensor(x, dtype=torch.float32, device="cuda"))
+    gs = _to_split(torch, torch.tensor(g, dtype=torch.float32, device="cuda"))
+    x32 = _from_split(torch, xs, n)
+    g32 = _from_split(torch, gs, n)
+    ys, os_ = torch.empty_like(xs), torch.empty_like(xs)
+    L = _lib.lib()
+    _lib.check(L.sp2b_dev_sp2_step_split(xs[0].data_ptr(), xs[1].data_ptr(), ys[0].data_ptr(),
+                                         ys[1].data_ptr(), n, branch, C.c_void_p(0)), "step")
+    _lib.check(L.sp2b_dev_adjoint_step_split(gs[0].data_ptr(), gs[1].data_ptr(), xs[0].data_ptr(),
+                                             xs[1].data_ptr(), os_[0].data_ptr(),
+                                             os_[1].data_ptr(), n, branch, C.c_void_p(0)), "adj")
+    torch.cuda.synchronize()
+    x2 = x32 @ x32
+    y_ref = x2 if branch else 2 * x32 - x2
+    anti = g32 @ x32 + x32 @ g32
+    o_ref = anti if branch else 2 * g32 - anti
+    y = _from_split(torch, ys, n)
+    o = _from_split(torch, os_, n)
+    ax, ag = np.abs(x32), np.abs(g32)
+    assert np.linalg.norm(y - y_ref) <= 1e-6 * np.linalg.norm(ax @ ax)
+    assert np.linalg.norm(o - o_ref) <= 1e-6 * np.linalg.norm(ag @ ax + ax @ ag)
+    assert np.array_equal(o, o.T)                    # symmetric by construction
+    np_ = xs.shape[1]                                # the padding stays zero
+    assert not ys[:, n:, :].any() and not ys[:, :, n:].any()
+    assert not os_[:, n:, :].any() and not os_[:, :, n:].any()
+    assert np_ % 128 == 0
