@@ -656,13 +656,15 @@ __device__ __forceinline__ void i8_store_x(int8_t* base, size_t plane, size_t id
 }
 
 // CSR rows of each part straight to X0' = X0 - I/2 in digits (parts up to 512), with the
-// same row construction as the split extraction: one warp per row in shared memory.
+// same row construction as the split extraction: one warp per row in shared memory.  The
+// row's digits are collected by plane in shared memory and leave as 16-byte stores.
 __global__ void __launch_bounds__(256) k_extract_digits(
     const long long* __restrict__ rp, const int* __restrict__ col, const double* __restrict__ val,
     const PartDesc* __restrict__ parts, const int* __restrict__ halo, const int* __restrict__ skey,
     const int* __restrict__ sval, int ld, long long rows, double emin, double emax,
     int8_t* __restrict__ dig) {
   __shared__ double rowbuf[8][512];
+  __shared__ __align__(16) int8_t dbuf[8][4][512];
   const PartDesc P = parts[blockIdx.x];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double mm = emax - emin;
@@ -693,7 +695,7 @@ __global__ void __launch_bounds__(256) k_extract_digits(
       }
     }
     __syncwarp();
-    const size_t ro = ((size_t)P.row0 + r) * ld;
+    int8_t(*db)[512] = dbuf[warp];
     for (int c = lane; c < P.np; c += 32) {
       // separate roundings (no contraction), so a host model forms the same X0'
       double x = 0.0;
@@ -701,8 +703,16 @@ __global__ void __launch_bounds__(256) k_extract_digits(
         x = __dmul_rn(alpha, buf[c]);
         if (r == c) x = __dadd_rn(x, beta);
       }
-      i8_store_x(dig, plane, ro + c, r == c ? __dadd_rn(x, -0.5) : x);
+      const int m = (int)llrint((r == c ? __dadd_rn(x, -0.5) : x) * 0x1p31);
+      i8_digits(m, db[0][c], db[1][c], db[2][c], db[3][c]);
     }
+    __syncwarp();
+    const size_t ro = ((size_t)P.row0 + r) * ld;   // ld, np: multiples of 128
+    for (int c0 = lane * 16; c0 < P.np; c0 += 512)
+#pragma unroll
+      for (int d = 0; d < 4; ++d)
+        *reinterpret_cast<uint4*>(dig + d * plane + ro + c0) =
+            *reinterpret_cast<const uint4*>(&db[d][c0]);
     __syncwarp();
   }
 }
@@ -737,7 +747,7 @@ __device__ __forceinline__ size_t i8_band_off(long long row0, int r, int c, int 
   return c >= (r & ~(i8s::BM - 1)) ? ((size_t)row0 + r) * ld + c : ((size_t)row0 + c) * ld + r;
 }
 
-// rho (core rows) = 2 X = 2^-30 M + I.
+// rho (core rows) = 2 X = 2^-30 M + I; one warp per core row, the lanes along it.
 __global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
                                  const PartDesc* __restrict__ parts, const int* __restrict__ halo,
                                  int ld, double* __restrict__ core_out, double* __restrict__ dense,
@@ -745,20 +755,23 @@ __global__ void k_scatter_digits(const int8_t* __restrict__ dig, long long rows,
   const PartDesc P = parts[blockIdx.x];
   const int* hl = halo + P.hoff;
   const size_t plane = (size_t)rows * ld;
-  const long long total = (long long)P.ncore * P.n;
-  for (long long q = (long long)blockIdx.y * blockDim.x + threadIdx.x; q < total;
-       q += (long long)gridDim.y * blockDim.x) {
-    const int r = (int)(q / P.n), c = (int)(q % P.n);
-    const size_t src = i8_band_off(P.row0, r, c, ld);
-    const int m = i8_value(dig[src], dig[plane + src], dig[2 * plane + src], dig[3 * plane + src]);
-    const double v = (double)m * 0x1p-30 + (r == c ? 1.0 : 0.0);
-    if (core_out) core_out[P.coff + q] = v;
-    if (dense) dense[(size_t)hl[r] + (size_t)hl[c] * n] = v;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = blockIdx.y * nw + warp; r < P.ncore; r += gridDim.y * nw) {
+    double* co = core_out ? core_out + P.coff + (size_t)r * P.n : nullptr;
+    for (int c = lane; c < P.n; c += 32) {
+      const size_t src = i8_band_off(P.row0, r, c, ld);
+      const int m = i8_value(dig[src], dig[plane + src], dig[2 * plane + src], dig[3 * plane + src]);
+      const double v = (double)m * 0x1p-30 + (r == c ? 1.0 : 0.0);
+      if (co) co[c] = v;
+      if (dense) dense[(size_t)hl[r] + (size_t)hl[c] * n] = v;
+    }
   }
 }
 
 // Sum over each part's core rows of (X - X^2)_ii = X_ii - sum_j X_ij^2, from the digits
-// (upper-band storage).
+// (upper-band storage).  Columns j < n only: past the part size X is zero off the
+// diagonal, and past the tiles' columns (the part size rounded up to 64) the iterated
+// buffer holds entries no step writes.
 __global__ void k_part_idem_digits(const int8_t* __restrict__ dig, long long rows,
                                    const PartDesc* __restrict__ parts, int ld,
                                    double* __restrict__ out) {
@@ -777,7 +790,7 @@ __global__ void k_part_idem_digits(const int8_t* __restrict__ dig, long long row
                        0x1p-31;
       s -= x * x;
     }
-    for (int c0 = rb + lane * 16; c0 < P.np; c0 += 512) {
+    for (int c0 = rb + lane * 16; c0 < P.n; c0 += 512) {
       uint4 v[4];
 #pragma unroll
       for (int d = 0; d < 4; ++d) v[d] = *reinterpret_cast<const uint4*>(dig + d * plane + row + c0);

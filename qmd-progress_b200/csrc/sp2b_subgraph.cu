@@ -31,6 +31,40 @@ static cudaError_t grow_buf(T*& p, size_t& cap, size_t need) {
   return e;
 }
 
+// Page-locked host staging (the per-call readbacks leave in one copy batch and one wait).
+template <typename T>
+static cudaError_t grow_pinned(T*& p, size_t& cap, size_t need) {
+  if (need <= cap && p) return cudaSuccess;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMallocHost((void**)&p, std::max<size_t>(need, 1) * sizeof(T));
+  if (e == cudaSuccess) cap = std::max<size_t>(need, 1);
+  return e;
+}
+
+// 1 in *flag when the caller's part lists (halo_ptr, llsize) differ from the cached
+// layout's (node-list offsets and core sizes per part, the total node count).
+__global__ void k_cmp_parts(const long long* __restrict__ hp, const int* __restrict__ lls,
+                            const PartDesc* __restrict__ parts, int nparts, long long nhalo,
+                            int* flag) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= nparts; p += gridDim.x * blockDim.x) {
+    const bool diff = p == nparts ? hp[p] != nhalo
+                                  : (hp[p] != parts[p].hoff || lls[p] != parts[p].ncore);
+    if (diff) *flag = 1;
+  }
+}
+
+// ... and when the node lists differ; runs after k_cmp_parts and reads nothing of the
+// caller's node list unless the counts agreed (it then has nhalo entries).
+__global__ void k_cmp_halo(const int* __restrict__ hidx, const int* __restrict__ cached,
+                           long long nhalo, int* flag) {
+  if (*(volatile int*)flag) return;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nhalo;
+       q += (long long)gridDim.x * blockDim.x)
+    if (hidx[q] != cached[q]) *flag = 1;
+}
+
 struct SubBufs {
   double* xs = nullptr;          size_t xs_cap = 0;     // FP64 packed (H_sub / FP64 iterate)
   double* x2 = nullptr;          size_t x2_cap = 0;     // FP64 ping-pong partner
@@ -61,9 +95,12 @@ struct SubBufs {
   int* ms_part_tiles = nullptr;  size_t ms_part_tiles_cap = 0;
   unsigned* ms_bar = nullptr;    size_t ms_bar_cap = 0;
   int ms_ntiles = 0;
+  double* hback = nullptr;       size_t hback_cap = 0;  // pinned: vv, part sums, status
+  int* dflag = nullptr;          size_t dflag_cap = 0;  // device: part-list comparison
   // layout of the last call (reused when the part lists are unchanged)
-  std::vector<long long> last_hp;
-  std::vector<int> last_lls, last_hidx;
+  std::vector<long long> last_hp, last_coff;
+  std::vector<int> last_lls, last_hidx, last_pp;
+  const int* last_pp_dev = nullptr;
   std::vector<PartDesc> P;
   int ld = 0, ntiles = 0, layout_bt = 0, layout_order = 0, layout_dig = 0;
   long long rows = 0, coff = 0;
@@ -125,6 +162,10 @@ struct SubJob {
   // measured launch configuration (-1: the built-in rule).  FP64: the tile edge (32 or 64);
   // split: the order of the tile list (0 largest parts first, 1 balanced over the CTAs)
   int variant = -1;
+  // per part, the offset of its ncore x n block in `core` (null: packed in part order)
+  const std::vector<long long>* coff_at = nullptr;
+  // part_idem: receives the per-part sums (nparts x kPartIdemGroups) with the vv readback
+  std::vector<double>* idem_out = nullptr;
 };
 
 // Builds (or reuses) the layout, buffers and CUDA graph of `j` in `b`, launches the
@@ -157,9 +198,13 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     if (!j.multistep && (j.variant == 32 || j.variant == 64)) bt = j.variant;
   }
   const int tile_order = (split && j.variant == 1) ? 1 : 0;
+  // (the caller may pass the cached lists themselves, which then need no comparison)
+  static const std::vector<long long> no_coff;
+  const std::vector<long long>& coff_at = j.coff_at ? *j.coff_at : no_coff;
   const bool same_layout = b.layout_valid && b.layout_bt == bt && b.layout_order == tile_order &&
-                           b.layout_dig == (dig ? 1 : 0) && b.last_hp == hp && b.last_lls == lls &&
-                           b.last_hidx == hidx;
+                           b.layout_dig == (dig ? 1 : 0) && (&b.last_hp == &hp || b.last_hp == hp) &&
+                           (&b.last_lls == &lls || b.last_lls == lls) &&
+                           (&b.last_hidx == &hidx || b.last_hidx == hidx) && b.last_coff == coff_at;
   if (!same_layout) {
     b.layout_valid = false;
     std::vector<PartDesc>& P = b.P;
@@ -178,7 +223,7 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
       d.ncore = lls[p];
       d.hoff = hp[p];
       d.row0 = rows;
-      d.coff = coff;
+      d.coff = j.coff_at ? coff_at[p] : coff;
       d.pad_ = 0;
       rows += d.np;
       coff += (long long)d.ncore * d.n;
@@ -294,9 +339,10 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     b.rows = rows;
     b.coff = coff;
     b.ntiles = ntiles;
-    b.last_hp = hp;
-    b.last_lls = lls;
-    b.last_hidx = hidx;
+    if (&b.last_hp != &hp) b.last_hp = hp;
+    if (&b.last_lls != &lls) b.last_lls = lls;
+    if (&b.last_hidx != &hidx) b.last_hidx = hidx;
+    b.last_coff = coff_at;
     b.layout_bt = bt;
     b.layout_order = tile_order;
     b.layout_dig = dig ? 1 : 0;
@@ -328,8 +374,13 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
   SP2B_CUDA_TRY(grow_buf(b.rec, b.rec_cap, (size_t)maxiter + 2));
   SP2B_CUDA_TRY(grow_buf(b.pp, b.pp_cap, (size_t)maxiter + 1));
   SP2B_CUDA_TRY(grow_buf(b.vv, b.vv_cap, (size_t)maxiter + 1));
-  if (maxiter > 0)  // pp is a host array in every mode
+  // pp is a host array in every mode; uploaded when it changed (or its buffer did)
+  if (maxiter > 0 && (b.pp != b.last_pp_dev || (int)b.last_pp.size() != maxiter ||
+                      !std::equal(b.last_pp.begin(), b.last_pp.end(), j.pp))) {
     SP2B_CUDA_TRY(cudaMemcpyAsync(b.pp, j.pp, maxiter * sizeof(int), cudaMemcpyHostToDevice, st));
+    b.last_pp.assign(j.pp, j.pp + maxiter);
+    b.last_pp_dev = b.pp;
+  }
   double* core_d = j.core;
   double* dense_d = j.dense;
 
@@ -365,9 +416,11 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     if (me == cudaSuccess) {
       SP2B_CUDA_TRY(launch_scatter_parts((maxiter & 1) ? b.x2 : b.xs, nullptr, nullptr, prec,
                                          b.parts, nparts, b.halo, ld, core_d, dense_d, n, st));
+      SP2B_CUDA_TRY(grow_pinned(b.hback, b.hback_cap, 1));
+      SP2B_CUDA_TRY(cudaMemcpyAsync(b.hback, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
       SP2B_CUDA_TRY(cudaStreamSynchronize(st));
       int herr = 0;
-      SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+      memcpy(&herr, b.hback, sizeof(int));
       if (herr) {
         set_last_error("a device-side wait timed out");
         return SP2B_TIMEOUT;
@@ -448,9 +501,11 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
           (e = cudaMemsetAsync(dense_d, 0, (size_t)n * n * sizeof(double), cap)) != cudaSuccess)
         return e;
       if (dig) {
-        // the second buffer's entries outside the written band (columns past a part's
-        // tiles) are read as zero padding by the mirrored operand loads
-        if ((e = cudaMemsetAsync(b.dig[1], 0, 4 * packed, cap)) != cudaSuccess) return e;
+        // The steps write each part's tiles (rows to the 128-row block, columns to the part
+        // size rounded up to 64).  The second buffer's other entries are not cleared: the
+        // mirrored operand loads reach columns past the tiles only for rows past them, so
+        // stale values there feed padding rows alone, which no core row, sum or scatter
+        // reads.
         if (fused) {
           if ((e = launch_extract_digits(j.rp, j.col, j.val, b.parts, nparts, b.halo, b.skey,
                                          b.sval, ld, rows, j.mineval, j.maxeval, b.dig[0], cap)) !=
@@ -552,18 +607,26 @@ static int batched_solve(Ctx* c, SubBufs& b, const SubJob& j, cudaStream_t st,
     b.exec_key = kbytes;
   }
   cudaError_t le = cudaGraphLaunch(exec, st);
-  if (le == cudaSuccess) le = cudaStreamSynchronize(st);
   // extract, normalise, the steps (INT8: one persistent launch and its sums), scatter
   note_launch((dig ? (fused ? 1 : 2) + (maxiter > 0 ? 2 : 0) + 1 : maxiter + 3) + (idem ? 1 : 0));
   if (le != cudaSuccess) {
     set_last_error("graph launch failed: %s", cudaGetErrorString(le));
     return SP2B_CUDA_ERROR;
   }
+  // the sums, the part sums and the status leave together, then one wait
+  const size_t nv = (size_t)maxiter;
+  const size_t ni = (idem && j.idem_out) ? (size_t)nparts * kPartIdemGroups : 0;
+  SP2B_CUDA_TRY(grow_pinned(b.hback, b.hback_cap, nv + ni + 1));
+  if (nv) SP2B_CUDA_TRY(cudaMemcpyAsync(b.hback, b.vv, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (ni)
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.hback + nv, b.idem, ni * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaMemcpyAsync(b.hback + nv + ni, c->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SP2B_CUDA_TRY(cudaStreamSynchronize(st));
   vvh.assign(maxiter + 1, 0.0);
-  if (maxiter > 0)
-    SP2B_CUDA_TRY(cudaMemcpy(vvh.data(), b.vv, maxiter * sizeof(double), cudaMemcpyDeviceToHost));
+  std::copy(b.hback, b.hback + nv, vvh.begin());
+  if (ni) j.idem_out->assign(b.hback + nv, b.hback + nv + ni);
   int herr = 0;
-  SP2B_CUDA_TRY(cudaMemcpy(&herr, c->err, sizeof(int), cudaMemcpyDeviceToHost));
+  memcpy(&herr, b.hback + nv + ni, sizeof(int));
   if (herr) {
     set_last_error("a device-side wait timed out");
     return SP2B_TIMEOUT;
@@ -648,35 +711,71 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   // stream); the CUDA graph is captured on the library stream and launched on `st`
   cudaStream_t st = opts->stream ? (cudaStream_t)opts->stream : (dev ? (cudaStream_t)0 : c->stream);
 
-  // ---- host-side layout (index lists are small; device inputs are fetched) ----
-  std::vector<long long> hp(nparts + 1);
-  std::vector<int> lls(nparts);
-  if (dev) {
-    SP2B_CUDA_TRY(cudaMemcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long), cudaMemcpyDeviceToHost));
-    SP2B_CUDA_TRY(cudaMemcpy(lls.data(), llsize, nparts * sizeof(int), cudaMemcpyDeviceToHost));
+  // ---- host-side layout (index lists are small) ----
+  // Device inputs: when a layout is cached, the caller's lists are compared with it on the
+  // device (two small kernels and one 4-byte readback, in stream order) and the cached host
+  // copies are used when they agree; otherwise the lists are fetched.
+  std::vector<long long> hp_own;
+  std::vector<int> lls_own, hidx_own;
+  const std::vector<long long>* php = &hp_own;
+  const std::vector<int>* plls = &lls_own;
+  const std::vector<int>* phidx = &hidx_own;
+  bool cached = false;
+  if (dev && b.layout_valid && (int)b.P.size() == nparts &&
+      b.last_hp.size() == (size_t)nparts + 1) {
+    SP2B_CUDA_TRY(grow_buf(b.dflag, b.dflag_cap, 1));
+    SP2B_CUDA_TRY(grow_pinned(b.hback, b.hback_cap, 1));
+    SP2B_CUDA_TRY(cudaMemsetAsync(b.dflag, 0, sizeof(int), st));
+    const long long nh = b.last_hp[nparts];
+    k_cmp_parts<<<nparts / 256 + 1, 256, 0, st>>>(halo_ptr, llsize, b.parts, nparts, nh, b.dflag);
+    k_cmp_halo<<<(int)std::min<long long>(nh / 256 + 1, 4 * 148), 256, 0, st>>>(halo_idx, b.halo,
+                                                                                nh, b.dflag);
+    note_launch(2);
+    SP2B_CUDA_TRY(cudaGetLastError());
+    SP2B_CUDA_TRY(cudaMemcpyAsync(b.hback, b.dflag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SP2B_CUDA_TRY(cudaStreamSynchronize(st));
+    int diff = 1;
+    memcpy(&diff, b.hback, sizeof(int));
+    cached = diff == 0;
+  }
+  if (cached) {
+    php = &b.last_hp;
+    plls = &b.last_lls;
+    phidx = &b.last_hidx;
   } else {
-    std::memcpy(hp.data(), halo_ptr, (nparts + 1) * sizeof(long long));
-    std::memcpy(lls.data(), llsize, nparts * sizeof(int));
+    hp_own.resize(nparts + 1);
+    lls_own.resize(nparts);
+    if (dev) {
+      SP2B_CUDA_TRY(cudaMemcpy(hp_own.data(), halo_ptr, (nparts + 1) * sizeof(long long),
+                               cudaMemcpyDeviceToHost));
+      SP2B_CUDA_TRY(cudaMemcpy(lls_own.data(), llsize, nparts * sizeof(int), cudaMemcpyDeviceToHost));
+    } else {
+      std::memcpy(hp_own.data(), halo_ptr, (nparts + 1) * sizeof(long long));
+      std::memcpy(lls_own.data(), llsize, nparts * sizeof(int));
+    }
+    if (hp_own[nparts] < 0) {
+      set_last_error("sp2b_subgraph_sp2_loop: bad halo_ptr");
+      return SP2B_BAD_ARG;
+    }
+    hidx_own.resize(hp_own[nparts]);
+    if (dev)
+      SP2B_CUDA_TRY(cudaMemcpy(hidx_own.data(), halo_idx, hidx_own.size() * sizeof(int),
+                               cudaMemcpyDeviceToHost));
+    else
+      std::memcpy(hidx_own.data(), halo_idx, hidx_own.size() * sizeof(int));
   }
-  const long long nhalo = hp[nparts];
-  if (nhalo < 0) {
-    set_last_error("sp2b_subgraph_sp2_loop: bad halo_ptr");
-    return SP2B_BAD_ARG;
-  }
-  std::vector<int> hidx(nhalo);
-  if (dev) SP2B_CUDA_TRY(cudaMemcpy(hidx.data(), halo_idx, nhalo * sizeof(int), cudaMemcpyDeviceToHost));
-  else std::memcpy(hidx.data(), halo_idx, nhalo * sizeof(int));
+  const std::vector<long long>& hp = *php;
+  const std::vector<int>& lls = *plls;
+  const std::vector<int>& hidx = *phidx;
   long long coff = 0;
   for (int p = 0; p < nparts; ++p) coff += (long long)lls[p] * (hp[p + 1] - hp[p]);
 
   // ---- H and the outputs on the device ----
-  long long nnz;
-  if (dev) SP2B_CUDA_TRY(cudaMemcpy(&nnz, h_row_ptr + n, sizeof(long long), cudaMemcpyDeviceToHost));
-  else nnz = h_row_ptr[n];
   const long long* rp_d = h_row_ptr;
   const int* col_d = h_col;
   const double* val_d = h_val;
   if (!dev) {
+    const long long nnz = h_row_ptr[n];
     SP2B_CUDA_TRY(grow_buf(b.rp, b.rp_cap, (size_t)n + 1));
     SP2B_CUDA_TRY(grow_buf(b.col, b.col_cap, (size_t)nnz));
     SP2B_CUDA_TRY(grow_buf(b.val, b.val_cap, (size_t)nnz));
@@ -704,17 +803,19 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
   bool core_out_done = false;   // the core rows already reached rho_core (host calls)
   SubJob j{n, rp_d, col_d, val_d, &hp, &lls, &hidx, pp, maxiter, mineval, maxeval, prec,
            core_d, dense_d, true, refine, false};
-  std::vector<double> vvh;
+  std::vector<double> vvh, part;
   int rc = tune_subgraph(c, b, j, st);
   if (rc != SP2B_OK) return rc;
+  j.idem_out = refine ? &part : nullptr;   // the part sums come back with vv
   rc = batched_solve(c, b, j, st, vvh);
   if (rc != SP2B_OK) return rc;
 
   // ---- FP64 re-solve of the parts left with a half-occupied state ----
   if (refine) {
-    std::vector<double> part((size_t)nparts * kPartIdemGroups);
-    SP2B_CUDA_TRY(cudaMemcpy(part.data(), b.idem, part.size() * sizeof(double),
-                             cudaMemcpyDeviceToHost));
+    if (part.size() != (size_t)nparts * kPartIdemGroups) {
+      set_last_error("sp2b_subgraph_sp2_loop: part sums missing");
+      return SP2B_CUDA_ERROR;
+    }
     t_idem.assign(nparts, 0.0);
     for (int p = 0; p < nparts; ++p)
       for (int g = 0; g < kPartIdemGroups; ++g) t_idem[p] += part[(size_t)p * kPartIdemGroups + g];
@@ -729,13 +830,6 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
     }
     if (!t_refined.empty()) {
       SubBufs& rb = g_sub_ref[c->dev];
-      long long rcoff = 0;
-      for (size_t q = 0; q < rlls.size(); ++q) rcoff += (long long)rlls[q] * (rhp[q + 1] - rhp[q]);
-      double* rcore = nullptr;
-      if (core_d) {
-        SP2B_CUDA_TRY(grow_buf(rb.core, rb.core_cap, (size_t)std::max(rcoff, 1LL)));
-        rcore = rb.core;
-      }
       // A host-pointer call whose core output is page-locked: the split solve's core rows
       // (final but for the re-solved parts' blocks) leave on a second stream while the
       // re-solve runs, and the re-solved blocks follow from its output once they are out.
@@ -745,8 +839,25 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         SP2B_CUDA_TRY(cudaMemcpyAsync(rho_core, b.core, coff * sizeof(double),
                                       cudaMemcpyDeviceToHost, cs));
       }
+      // Otherwise the re-solve writes each part's block in place in the core output (part
+      // p's block sits at sum_{q<p} llsize[q] * lsize[q]); with the copy stream it writes
+      // them packed into its own buffer, from which they follow the copy.
+      std::vector<long long> rcoffs;
+      double* rcore = nullptr;
+      if (core_d && cs) {
+        long long rcoff = 0;
+        for (size_t q = 0; q < rlls.size(); ++q) rcoff += (long long)rlls[q] * (rhp[q + 1] - rhp[q]);
+        SP2B_CUDA_TRY(grow_buf(rb.core, rb.core_cap, (size_t)std::max(rcoff, 1LL)));
+        rcore = rb.core;
+      } else if (core_d) {
+        std::vector<long long> start(nparts + 1, 0);
+        for (int p = 0; p < nparts; ++p) start[p + 1] = start[p] + (long long)lls[p] * (hp[p + 1] - hp[p]);
+        for (const int p : t_refined) rcoffs.push_back(start[p]);
+        rcore = core_d;
+      }
       SubJob rj{n, rp_d, col_d, val_d, &rhp, &rlls, &ridx, pp, maxiter, mineval, maxeval,
                 SP2B_PREC_FP64, rcore, dense_d, false, false, true};
+      if (core_d && !cs) rj.coff_at = &rcoffs;
       std::vector<double> rvv;
       rc = batched_solve(c, rb, rj, st, rvv);
       if (cs) {
@@ -757,20 +868,15 @@ extern "C" int sp2b_subgraph_sp2_loop(int n, const long long* h_row_ptr, const i
         }
       }
       if (rc != SP2B_OK) return rc;
-      if (core_d) {
-        // part p's block sits at sum_{q<p} llsize[q]*lsize[q] in both packings
+      if (core_d && cs) {
         long long src = 0;
         for (size_t q = 0; q < t_refined.size(); ++q) {
           const int p = t_refined[q];
           long long dst = 0;
           for (int r = 0; r < p; ++r) dst += (long long)lls[r] * (hp[r + 1] - hp[r]);
           const long long m = (long long)lls[p] * (hp[p + 1] - hp[p]);
-          if (cs)
-            SP2B_CUDA_TRY(cudaMemcpyAsync(rho_core + dst, rcore + src, m * sizeof(double),
-                                          cudaMemcpyDeviceToHost, st));
-          else
-            SP2B_CUDA_TRY(cudaMemcpyAsync(core_d + dst, rcore + src, m * sizeof(double),
-                                          cudaMemcpyDeviceToDevice, st));
+          SP2B_CUDA_TRY(cudaMemcpyAsync(rho_core + dst, rcore + src, m * sizeof(double),
+                                        cudaMemcpyDeviceToHost, st));
           src += m;
         }
         SP2B_CUDA_TRY(cudaStreamSynchronize(st));
