@@ -459,22 +459,15 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
       // Q = rint(2^31 X'^2) = floor((P + 2^14) / 2^15) with P = sum_u A_u 2^{32 - 8u}:
       //   Q = 2^17 A_0 + 2^9 A_1 + 2 A_2 + floor((A_3 + floor((A_4 + 2^14) / 2^8)) / 2^7),
       // the last term by nested floor division.  The sum is formed modulo 2^32; its true
-      // value fits (|Q| <= 2^29 since |X'^2| <= 1/4), so the wrapped sum is exact.  The low
-      // pair is read and folded first, then the other three are read and the
-      // accumulators released before the rest of the sum.
+      // value fits (|Q| <= 2^29 since |X'^2| <= 1/4), so the wrapped sum is exact.  All five
+      // accumulators are read behind one wait and released before the sum (the next
+      // tile's products wait for the release).
       int Q[16];
       {
         const uint32_t ta = tmem + lane_base + grp * 16;
-        int ql[16];
-        {
-          uint32_t a4[16], a3[16];
-          tmem_ld16(ta + 4 * i8s::BN, a4);
-          tmem_ld16(ta + 3 * i8s::BN, a3);
-          tmem_wait_ld();
-#pragma unroll
-          for (int j = 0; j < 16; ++j) ql[j] = ((int)a3[j] + (((int)a4[j] + (1 << 14)) >> 8)) >> 7;
-        }
-        uint32_t a2[16], a1[16], a0[16];
+        uint32_t a4[16], a3[16], a2[16], a1[16], a0[16];
+        tmem_ld16(ta + 4 * i8s::BN, a4);
+        tmem_ld16(ta + 3 * i8s::BN, a3);
         tmem_ld16(ta + 2 * i8s::BN, a2);
         tmem_ld16(ta + i8s::BN, a1);
         tmem_ld16(ta, a0);
@@ -483,8 +476,10 @@ __global__ void __launch_bounds__(i8s::NTHR, 1)
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&bar_tempty));
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          Q[j] = (int)((a0[j] << 17) + (a1[j] << 9) + 2u * a2[j] + (uint32_t)ql[j]);
+        for (int j = 0; j < 16; ++j) {
+          const int ql = ((int)a3[j] + (((int)a4[j] + (1 << 14)) >> 8)) >> 7;
+          Q[j] = (int)((a0[j] << 17) + (a1[j] << 9) + 2u * a2[j] + (uint32_t)ql);
+        }
       }
       uint4 xd[i8s::ND];   // X_k digits of this thread's 16 elements (plane 0: d0)
 #pragma unroll

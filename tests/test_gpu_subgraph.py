@@ -246,3 +246,63 @@ def test_subgraph_refinement_into_pinned_host_output(cuda):
         core_pinned.data_ptr(), None, vv.ctypes.data, C.byref(o)), "subgraph_sp2_loop")
     assert sp2b.last_subgraph_refined(len(lls))[0] == flagged
     assert np.array_equal(core_pinned.numpy(), core_pageable)
+
+
+def _dev_loop(torch, n, h_csr, hp, hi, lls, pp, maxiter, emin, emax, precision):
+    """prg_subgraphSP2Loop through the C ABI with every input and the core rows on the
+    device (the calls whose part lists the library compares on the device with the
+    layout it has cached)."""
+    import ctypes as C
+    from sp2b import _lib
+    dev = lambda a, t: torch.from_numpy(np.ascontiguousarray(a, t)).cuda()
+    rp, col, val = dev(h_csr[0], np.int64), dev(h_csr[1], np.int32), dev(h_csr[2], np.float64)
+    hp_d, hi_d, lls_d = dev(hp, np.int64), dev(hi, np.int32), dev(lls, np.int32)
+    ncore = int(np.sum(np.asarray(lls, np.int64) * np.diff(np.asarray(hp, np.int64))))
+    core = torch.full((ncore,), np.nan, dtype=torch.float64, device="cuda")
+    pp_a = np.ascontiguousarray(pp, np.int32)
+    vv = np.zeros(max(maxiter, 1))
+    st = torch.cuda.current_stream()
+    o = _lib.make_opts(precision=precision, device_ptrs=True, stream=st.cuda_stream)
+    _lib.check(_lib.lib().sp2b_subgraph_sp2_loop(
+        n, rp.data_ptr(), col.data_ptr(), val.data_ptr(), len(lls), hp_d.data_ptr(),
+        hi_d.data_ptr(), lls_d.data_ptr(), pp_a.ctypes.data, maxiter, emin, emax,
+        core.data_ptr(), None, vv.ctypes.data, C.byref(o)), "subgraph_sp2_loop")
+    torch.cuda.synchronize()
+    return core.cpu().numpy(), vv[:maxiter].copy()
+
+
+@pytest.mark.parametrize("precision", [sp2b.PREC_FP64, sp2b.PREC_EXACT_INT8])
+def test_subgraph_device_lists_changed_between_calls(cuda, precision):
+    """Device-pointer calls reuse the cached layout only while the caller's part lists
+    equal it.  Lists that differ only in the halo order, only in a core size, or in the
+    part sizes (the same number of parts each time) give what host-pointer calls with
+    the same lists give, bit for bit, and so do repeated calls with unchanged lists."""
+    torch = cuda
+    n = 240
+    h, g, parts, emin, emax, pp, maxiter = _setup(n)
+    h_csr, g_csr = sp2b.dense_to_csr(h), sp2b.dense_to_csr(g)
+    L1 = sp2b.subgraph_halos(n, g_csr, parts, h_csr)
+    hp, hi, ls, lls = L1
+    hi2 = hi.copy()                                    # halo entries reversed in each part
+    for p in range(len(lls)):
+        a, b = hp[p] + lls[p], hp[p + 1]
+        hi2[a:b] = hi2[a:b][::-1].copy()
+    L2 = (hp, hi2, ls, lls)
+    lls4 = lls.copy()
+    lls4[0] -= 1                                       # a core size alone
+    L4 = (hp, hi, ls, lls4)
+    sizes = [30, 50, 40, 40, 40, 40]                   # the same count of parts, other sizes
+    cuts = np.cumsum([0] + sizes)
+    L3 = sp2b.subgraph_halos(n, g_csr, [np.arange(cuts[i], cuts[i + 1]) for i in range(6)], h_csr)
+    lists = {"L1": L1, "L2": L2, "L3": L3, "L4": L4}
+    ref = {}
+    for k, (a, b, _, d) in lists.items():
+        _, core, vv = sp2b.subgraph_sp2_loop(n, h_csr, a, b, d, pp, maxiter, emin, emax,
+                                             precision=precision, dense=False, core=True)
+        ref[k] = (core, vv)
+    assert not np.array_equal(ref["L1"][0], ref["L2"][0])
+    for k in ["L1", "L2", "L4", "L3", "L1", "L1", "L2", "L2"]:
+        a, b, _, d = lists[k]
+        core, vv = _dev_loop(torch, n, h_csr, a, b, d, pp, maxiter, emin, emax, precision)
+        assert np.array_equal(core, ref[k][0]), k
+        assert np.array_equal(vv, ref[k][1]), k
