@@ -335,7 +335,9 @@ __device__ __forceinline__ TileInfo persist_tile(const StepArgs& p, int t) {
 // there, and X_{k+1} is written back in place for a TMA store of the whole tile; only the
 // mirror of an off-diagonal tile is stored from the registers.  Otherwise each lane reads
 // its row of X_k from global memory and stores the block and its mirror itself.
-template <typename T, int EPI, bool ESM>
+// ES: the tile's X_k block is staged in shared memory like ESM's (estage: this half's hi
+// box, then its lo box, 128-byte swizzle), the results leave by the direct stores.
+template <typename T, int EPI, bool ESM, bool ES = false>
 __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, uint32_t tacc,
                                          int q, int half, int lane, double alpha, double beta,
                                          double (&sums)[4], uint8_t* scr, uint8_t* estage,
@@ -368,7 +370,7 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       pf[2] = sl[0];
       pf[3] = sl[1];
     };
-    if (!ESM && first < cc_hi) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
+    if (!ESM && !ES && first < cc_hi) fetch_e(ti.j0 + half * 64 + first * tcp::CHUNK);
     const int rl = q * 32 + lane;   // row inside the tile
 #pragma unroll 1
     for (int cc = first; cc < cc_hi; ++cc) {
@@ -380,12 +382,12 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
       alignas(16) T ehi[16], elo[16], nhi[16], nlo[16];
       // 16-byte chunk k of row rl of a staged box sits at chunk k ^ (rl & 7) (128-byte
       // swizzle); estage is this half's stage: the hi box, then the lo box
-      uint8_t* eb = ESM ? estage + rl * 128 : nullptr;
+      uint8_t* eb = (ESM || ES) ? estage + rl * 128 : nullptr;
       const int k0 = ((2 * cc) ^ (rl & 7)) * 16, k1 = ((2 * cc + 1) ^ (rl & 7)) * 16;
       {
         uint4* dh = reinterpret_cast<uint4*>(ehi);
         uint4* dl = reinterpret_cast<uint4*>(elo);
-        if (ESM) {
+        if (ESM || ES) {
           dh[0] = *reinterpret_cast<const uint4*>(eb + k0);
           dh[1] = *reinterpret_cast<const uint4*>(eb + k1);
           dl[0] = *reinterpret_cast<const uint4*>(eb + tc::TILE_BYTES + k0);
@@ -397,7 +399,7 @@ __device__ __forceinline__ void epi_tile(const StepArgs& p, const TileInfo& ti, 
           dl[1] = pf[3];
         }
       }
-      if (!ESM && cc + 1 < cc_hi) fetch_e(c0 + tcp::CHUNK);
+      if (!ESM && !ES && cc + 1 < cc_hi) fetch_e(c0 + tcp::CHUNK);
       tmem_wait_ld();
       // Element math in FP32: x = hi + 2^-s lo is exact in FP32, P carries the
       // FP32 accumulators' precision, and X_{k+1} is re-split to the same 2 x 11
@@ -910,6 +912,11 @@ __global__ void __launch_bounds__(ESM ? tcp::NTHR_E : tcp::NTHR, 1)
 // product over the concatenated K range, [G | X] [X | G]^T: the K loop runs twice over
 // the columns, the second time with the operands' roles swapped (tm_a2* holds X in the
 // A role, tm_b2* G in the B role), so the one accumulator sums both products.
+// ES (SP2 epilogue, E = A: launches of at most one tile per pair): the producer also
+// brings the CTA's 128 x 128 block of E = X_k (or G) into shared memory by TMA while the
+// K loop runs, in place of the fourth operand stage, and the epilogue reads it there
+// instead of from global memory (with one tile per CTA the epilogue is not hidden behind
+// a next tile's products, and its per-row reads from L2 were its latency).
 // ---------------------------------------------------------------------------------
 namespace tcq {
 constexpr int BH = 64;                                  // B rows staged per CTA (N / 2)
@@ -919,9 +926,16 @@ constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * BH_BYTES; // 48 KB
 constexpr int ST = 4;
 constexpr int SCR_OFF = ST * STAGE_BYTES;
 constexpr int SMEM_BYTES = SCR_OFF + tcp::EPI_WARPS * tcp::SCR_WARP + 1024;
+// single-wave form with the X_k block staged: three operand stages, the epilogue scratch,
+// then the CTA's 128 x 128 block of X_k (hi and lo, two 64-column halves)
+constexpr int ST_ES = 3;
+constexpr int SCR_OFF_ES = ST_ES * STAGE_BYTES;
+constexpr int E_OFF_ES = SCR_OFF_ES + tcp::EPI_WARPS * tcp::SCR_WARP;
+constexpr int E_BYTES_ES = 4 * tc::TILE_BYTES;
+constexpr int SMEM_BYTES_ES = E_OFF_ES + E_BYTES_ES + 1024;
 }  // namespace tcq
 
-template <typename T, int EPI, bool ANTI = false>
+template <typename T, int EPI, bool ANTI = false, bool ES = false>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
     k_tc_pair(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
               const __grid_constant__ CUtensorMap tm_bhi, const __grid_constant__ CUtensorMap tm_blo,
@@ -934,10 +948,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
   __shared__ __align__(8) uint64_t bar_tfull[2];
   __shared__ __align__(8) uint64_t bar_tempty[2];
   __shared__ __align__(8) uint64_t bar_final;
+  __shared__ __align__(8) uint64_t bar_e;
   __shared__ uint32_t tmem_holder;
   __shared__ double red[32 * 4];
   __shared__ int s_flag;
   __shared__ volatile int s_abort;
+  constexpr int ST = ES ? tcq::ST_ES : tcq::ST;   // operand stages
+  if (ES && ntiles > (int)(gridDim.x >> 1)) {        // one tile per pair (uniform exit)
+    if (threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
+    return;
+  }
 
   double alpha = p.alpha, beta = p.beta;
   if (EPI == 0 && p.control) {
@@ -955,10 +975,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
   const uint32_t sbase = smem_u32(smem);
   if (threadIdx.x == 0) {
     s_abort = 0;
-    for (int s = 0; s < tcq::ST; ++s) {
+    for (int s = 0; s < ST; ++s) {
       mbar_init(smem_u32(&bar_full[s]), 1);
       mbar_init(smem_u32(&bar_empty[s]), 1);
     }
+    mbar_init(smem_u32(&bar_e), 1);
     for (int a = 0; a < 2; ++a) {
       mbar_init(smem_u32(&bar_tfull[a]), 1);
       mbar_init(smem_u32(&bar_tempty[a]), 2 * tcp::EPI_WARPS);
@@ -978,16 +999,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
   if (warp == 0) {
     if (lane == 0) {
       // ---------------- TMA producer (both CTAs) ----------------
-      bool ok = true;
+      bool ok = true, e_issued = false;
       uint32_t g = 0;
       for (int w = pair; w < ntiles && ok; w += npairs) {
         const int2 tile = ptiles[w];
         const int ra = tile.x * 2 * tc::BM + (int)rank * tc::BM;
         const int rb = tile.y * tc::BN + (int)rank * tcq::BH;
         for (int kb = 0; kb < KBT; ++kb, ++g) {
-          const int s = g % tcq::ST;
-          const uint32_t u = g / tcq::ST;
-          if (g >= (uint32_t)tcq::ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
+          const int s = g % ST;
+          const uint32_t u = g / ST;
+          if (g >= (uint32_t)ST && !mbar_wait(smem_u32(&bar_empty[s]), (u - 1) & 1, &s_abort)) {
             ok = false;
             break;
           }
@@ -1001,9 +1022,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
           tma_load_2d_pair(st + 2 * tcq::A_BYTES, sw ? &tm_b2hi : &tm_bhi, fb0, kc, rb);
           tma_load_2d_pair(st + 2 * tcq::A_BYTES + tcq::BH_BYTES, sw ? &tm_b2lo : &tm_blo, fb0, kc,
                            rb);
+          if (ES && kb == 0 && !e_issued) {
+            // this CTA's block of E (= A): rows ra.., columns 128 bj.., two 64-column halves
+            e_issued = true;
+            const uint32_t eb = smem_u32(&bar_e);
+            const uint32_t es = sbase + tcq::E_OFF_ES;
+            mbar_expect_tx(eb, tcq::E_BYTES_ES);
+            for (int h = 0; h < 2; ++h) {
+              tma_load_2d(es + h * 2 * tc::TILE_BYTES, &tm_ahi, eb, tile.y * tc::BN + h * 64, ra);
+              tma_load_2d(es + h * 2 * tc::TILE_BYTES + tc::TILE_BYTES, &tm_alo, eb,
+                          tile.y * tc::BN + h * 64, ra);
+            }
+          }
         }
       }
       if (!ok) s_abort = 1;
+      if (ES && e_issued)   // the block copy lands before this CTA can leave
+        for (uint32_t i = 0; i < kSpinLimit; ++i)
+          if (mbar_try(smem_u32(&bar_e), 0)) break;
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -1022,8 +1058,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
         tc_fence_after();
         const uint32_t acc_hh = tmem + a * 256, acc_x = tmem + a * 256 + tc::BN;
         for (int kb = 0; kb < KBT; ++kb, ++g) {
-          const int s = g % tcq::ST;
-          if (!mbar_wait(smem_u32(&bar_full[s]), (g / tcq::ST) & 1, &s_abort)) {
+          const int s = g % ST;
+          if (!mbar_wait(smem_u32(&bar_full[s]), (g / ST) & 1, &s_abort)) {
             ok = false;
             break;
           }
@@ -1074,8 +1110,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tcp::NTHR, 1)
       ti.core = p.core;
       ti.ok = brow <= tile.y;        // CTA 1's block of a diagonal pair lies below it
       ti.diag = brow == tile.y;
-      epi_tile<T, EPI, false>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta, sums,
-                              smem + tcq::SCR_OFF + (warp - 2) * tcp::SCR_WARP, nullptr);
+      if (ES && !mbar_wait_idle(smem_u32(&bar_e), 0, &s_abort)) break;
+      epi_tile<T, EPI, false, ES>(p, ti, tmem + lane_base + a * 256, q, half, lane, alpha, beta,
+                                  sums,
+                                  smem + (ES ? tcq::SCR_OFF_ES : tcq::SCR_OFF) +
+                                      (warp - 2) * tcp::SCR_WARP,
+                                  ES ? smem + tcq::E_OFF_ES + half * 2 * tc::TILE_BYTES : nullptr);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(tempty0[a]);
@@ -1372,7 +1412,7 @@ static const int2* pair_tiles(int np, cudaStream_t st, int* count) {
 }
 
 // Clusters of the paired kernel that can be resident at once (one CTA per SM).
-template <typename T, int EPI, bool ANTI = false>
+template <typename T, int EPI, bool ANTI = false, bool ES = false>
 static int pair_clusters() {
   static int per_dev[64] = {0};
   int dev = 0;
@@ -1381,7 +1421,7 @@ static int pair_clusters() {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(num_sms() & ~1, 1, 1);
   cfg.blockDim = dim3(tcp::NTHR, 1, 1);
-  cfg.dynamicSmemBytes = tcq::SMEM_BYTES;
+  cfg.dynamicSmemBytes = ES ? tcq::SMEM_BYTES_ES : tcq::SMEM_BYTES;
   cudaLaunchAttribute attr;
   attr.id = cudaLaunchAttributeClusterDimension;
   attr.val.clusterDim.x = 2;
@@ -1390,10 +1430,11 @@ static int pair_clusters() {
   cfg.attrs = &attr;
   cfg.numAttrs = 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, (void*)k_tc_pair<T, EPI, ANTI>, &cfg) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveClusters(&n, (void*)k_tc_pair<T, EPI, ANTI, ES>, &cfg) !=
+          cudaSuccess ||
       n <= 0) {
     cudaGetLastError();
-    n = num_sms() / 2;
+    n = ES ? 0 : num_sms() / 2;   // the staged form is used only where it is known to fit
   }
   per_dev[dev] = n;
   return n;
@@ -1422,6 +1463,20 @@ static cudaError_t launch_pair(const StepArgs& a, cudaStream_t st) {
       return cudaErrorInvalidValue;
   } else {
     for (int i = 0; i < 4; ++i) m[4 + i] = m[i];   // unused
+  }
+  // one tile per pair (a single wave): the X_k block staged for the epilogue (the
+  // shared-memory limit is raised before the residency query counts the clusters)
+  if (EPI == 0 && a.E == a.A && a.E_lo == a.A_lo && ntiles <= num_sms() / 2) {
+    auto kes = k_tc_pair<T, EPI, ANTI, true>;
+    if (cudaFuncSetAttribute(kes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tcq::SMEM_BYTES_ES) == cudaSuccess &&
+        ntiles <= pair_clusters<T, EPI, ANTI, true>()) {
+      kes<<<2 * ntiles, tcp::NTHR, tcq::SMEM_BYTES_ES, st>>>(m[0], m[1], m[2], m[3], m[4], m[5],
+                                                             m[6], m[7], a, tl, ntiles);
+      note_launch();
+      return cudaGetLastError();
+    }
+    (void)cudaGetLastError();
   }
   auto kern = k_tc_pair<T, EPI, ANTI>;
   cudaError_t e =

@@ -271,10 +271,7 @@ int sp2b_dev_sp2_step_split(const void* x_hi, const void* x_lo, void* y_hi, void
   a.out_lo = y_lo;
   a.alpha = branch ? 1.0 : -1.0;
   a.beta = branch ? 0.0 : 2.0;
-  a.partials = c->partials;
-  a.counter = c->counter;
-  a.sums_out = c->small + 24;
-  a.err = c->err;
+  a.err = c->err;   // no partials: the step's traces are not formed
   SP2B_CUDA_TRY(launch_sym_gemm_tc(a, 0, st));
   return SP2B_OK;
 }
@@ -306,10 +303,7 @@ int sp2b_dev_adjoint_step_split(const void* g_hi, const void* g_lo, const void* 
   a.out_lo = o_lo;
   a.alpha = branch ? 1.0 : -1.0;   // {G, X} or 2 G - {G, X}
   a.beta = branch ? 0.0 : 2.0;
-  a.partials = c->partials;
-  a.counter = c->counter;
-  a.sums_out = c->small + 24;
-  a.err = c->err;
+  a.err = c->err;   // no partials: the product's sums are not formed
   cudaError_t e = launch_anti_tc(a, st);
   if (e != cudaErrorNotSupported) {
     SP2B_CUDA_TRY(e);
