@@ -2,7 +2,7 @@
 
 Input: ``tests/tests_data/poly.512.mtx`` of lanl/qmd-progress (6144 x 6144, 98,304
 nonzeros), read from the reference checkout given on the command line or in
-SP2B_REFERENCE (default /root/reference).  This script only runs where that checkout
+SP2B_REFERENCE (one of the two is required).  This script only runs where that checkout
 exists; the fixture it writes is what the tests read on any machine.
 
 It runs the CPU oracle (oracle/sp2_oracle.py) with the parameters of the reference
@@ -83,4 +83,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SP2B_REFERENCE", "/root/reference"))
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SP2B_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_CHECKOUT (or set SP2B_REFERENCE)")
+    main(ref)
