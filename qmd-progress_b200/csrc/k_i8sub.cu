@@ -57,6 +57,7 @@ constexpr int OUT_PLANE = BM * BN;              // 8 KB: one plane of the output
 constexpr int OUT_BYTES = ND * OUT_PLANE;       // 32 KB: one staged tile (X_k in, X_{k+1} out)
 constexpr int OUT_OFF = ST * STAGE_BYTES;       // two staged tiles (64-byte swizzle)
 constexpr int SMEM_BYTES = OUT_OFF + 2 * OUT_BYTES + 1024;
+static_assert(SMEM_BYTES <= 232448 - 1536, "INT8 steps: shared memory beyond the per-block limit");
 constexpr int TMEM_COLS = 512;
 static_assert(NU * BN <= TMEM_COLS, "the five accumulators fit the TMEM allocation");
 }  // namespace i8s

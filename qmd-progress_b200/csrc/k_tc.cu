@@ -933,6 +933,10 @@ constexpr int SCR_OFF_ES = ST_ES * STAGE_BYTES;
 constexpr int E_OFF_ES = SCR_OFF_ES + tcp::EPI_WARPS * tcp::SCR_WARP;
 constexpr int E_BYTES_ES = 4 * tc::TILE_BYTES;
 constexpr int SMEM_BYTES_ES = E_OFF_ES + E_BYTES_ES + 1024;
+// 227 KB of shared memory per block on sm_100, less the kernel's ~1.2 KB of static
+// shared memory (barriers, the reduction array)
+static_assert(SMEM_BYTES <= 232448 - 1536 && SMEM_BYTES_ES <= 232448 - 1536,
+              "paired kernel: shared memory beyond the per-block limit");
 }  // namespace tcq
 
 template <typename T, int EPI, bool ANTI = false, bool ES = false>
